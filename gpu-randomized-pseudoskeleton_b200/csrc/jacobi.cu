@@ -1,0 +1,408 @@
+// Batched one-sided (Hestenes) Jacobi SVD in complex FP64, and the truncated pseudo-inverse.
+//
+// Replaces cusolverDnZgesvd + kernel_Sinv + cublasZdgmm + cublasZgemm of the reference CUR
+// round (codes/GPU_implementation/seed/user_impedance_for_julia_cuda.cu:1873-1924, and the
+// cur_external_cuda.cu:217-367 helpers): pinv(A) = V diag(s >= thr ? 1/s : 0) U^H.
+//
+// Algorithm: for every column pair (i, j) with alpha = |a_i|^2, beta = |a_j|^2,
+// gamma = a_i^H a_j = |gamma| e^{i phi}, zeta = (beta - alpha) / (2 |gamma|),
+// t = sign(zeta) / (|zeta| + sqrt(1 + zeta^2)), c = 1/sqrt(1 + t^2), s = c t:
+//     a_i <- c a_i - s e^{-i phi} a_j,   a_j <- s a_i + c e^{-i phi} a_j
+// (the same unitary applied to V). Pairs are visited in the round-robin (circle) order so
+// that the n/2 pairs of a round are disjoint and run in parallel, one lane team per pair with
+// shuffle reductions for the three inner products. A sweep with no rotation
+// (|gamma| <= n eps sqrt(alpha beta) for every pair) ends the iteration; the sweep cap turns
+// into PSKEL_ERR_NOCONV in the job's status.
+//
+// Two kernels:
+//  * resident: the whole m x n matrix and V live in shared memory of one CTA (small n, the
+//    sample counts the rank predictor produces);
+//  * blocked: one CTA per matrix keeps 2b columns of A and V in shared memory at a time and
+//    sweeps over all block pairs, the matrix itself staying in global memory (L2-resident);
+//    used for the large sample counts of the reference's doubling rule.
+#include <cfloat>
+#include <cmath>
+
+#include "pskel_internal.cuh"
+
+namespace pskel {
+
+static constexpr int kSvdThreads = 512;
+static constexpr size_t kSmemBudget = 200 * 1024;
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// circle-method player at position pos in round rho for nn (even) players
+__device__ __forceinline__ int circle_player(int pos, int rho, int nn) {
+    return pos == 0 ? 0 : ((pos - 1 + rho) % (nn - 1)) + 1;
+}
+
+// One round-robin sweep over the w columns held in shared memory (column-major, lds rows for
+// A-part and ldv rows for V-part). Returns (via *rotated) whether any rotation happened.
+// All threads of the CTA must call it.
+__device__ void inner_sweep(double2 *sA, int m, double2 *sV, int nv, int w, int team,
+                            double tol, int *s_rot) {
+    const int tid = threadIdx.x;
+    const int nteams = blockDim.x / team;
+    const int t = tid / team;
+    const int g = tid % team;
+    const int ww = w + (w & 1);
+    const int npairs = ww / 2;
+    const int iters = (npairs + nteams - 1) / nteams;
+    for (int rho = 0; rho < ww - 1; ++rho) {
+        for (int it = 0; it < iters; ++it) {
+            const int kp = t + it * nteams;
+            int ci = -1, cj = -1;
+            if (kp < npairs) {
+                ci = circle_player(kp, rho, ww);
+                cj = circle_player(ww - 1 - kp, rho, ww);
+                if (ci >= w || cj >= w) ci = cj = -1;
+            }
+            double al = 0, be = 0, gr = 0, gi = 0;
+            if (ci >= 0) {
+                const double2 *ai = sA + (size_t)ci * m;
+                const double2 *aj = sA + (size_t)cj * m;
+                for (int r = g; r < m; r += team) {
+                    const double2 x = ai[r], y = aj[r];
+                    al = fma(x.x, x.x, fma(x.y, x.y, al));
+                    be = fma(y.x, y.x, fma(y.y, y.y, be));
+                    gr = fma(x.x, y.x, fma(x.y, y.y, gr));   // Re(conj(x) y)
+                    gi = fma(x.x, y.y, fma(-x.y, y.x, gi));  // Im(conj(x) y)
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                if (o < team) {
+                    al += __shfl_xor_sync(0xffffffffu, al, o);
+                    be += __shfl_xor_sync(0xffffffffu, be, o);
+                    gr += __shfl_xor_sync(0xffffffffu, gr, o);
+                    gi += __shfl_xor_sync(0xffffffffu, gi, o);
+                }
+            }
+            if (ci >= 0) {
+                const double ag = hypot(gr, gi);
+                if (ag > tol * sqrt(al) * sqrt(be) && ag > 0.0) {
+                    const double zeta = (be - al) / (2.0 * ag);
+                    double tt;
+                    if (fabs(zeta) > 1e150) {
+                        tt = 0.5 / zeta;
+                    } else {
+                        tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                    }
+                    const double c = 1.0 / sqrt(1.0 + tt * tt);
+                    const double s = c * tt;
+                    const double2 e = make_double2(gr / ag, -gi / ag);  // e^{-i phi}
+                    double2 *ai = sA + (size_t)ci * m;
+                    double2 *aj = sA + (size_t)cj * m;
+                    for (int r = g; r < m; r += team) {
+                        const double2 x = ai[r];
+                        const double2 y = cmul(e, aj[r]);
+                        ai[r] = make_double2(c * x.x - s * y.x, c * x.y - s * y.y);
+                        aj[r] = make_double2(s * x.x + c * y.x, s * x.y + c * y.y);
+                    }
+                    double2 *vi = sV + (size_t)ci * nv;
+                    double2 *vj = sV + (size_t)cj * nv;
+                    for (int r = g; r < nv; r += team) {
+                        const double2 x = vi[r];
+                        const double2 y = cmul(e, vj[r]);
+                        vi[r] = make_double2(c * x.x - s * y.x, c * x.y - s * y.y);
+                        vj[r] = make_double2(s * x.x + c * y.x, s * x.y + c * y.y);
+                    }
+                    if (g == 0) *s_rot = 1;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__device__ int pick_team(int m) {
+    int t = 1;
+    while (t < 32 && 2 * t * 2 <= m) t <<= 1;  // about two rows per lane
+    return t;
+}
+
+// Singular values (column norms), permutation by decreasing value, and write-back helpers.
+__device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *sigma, int *perm) {
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+        double s = 0;
+        const double2 *a = A + (size_t)j * lda;
+        for (int r = 0; r < m; ++r) s = fma(a[r].x, a[r].x, fma(a[r].y, a[r].y, s));
+        sigma[j] = sqrt(s);
+    }
+    __syncthreads();
+    if (perm) {
+        for (int j = threadIdx.x; j < n; j += blockDim.x) {
+            const double sj = sigma[j];
+            int rank = 0;
+            for (int i = 0; i < n; ++i) {
+                const double si = sigma[i];
+                rank += (si > sj) || (si == sj && i < j);
+            }
+            perm[rank] = j;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kSvdThreads)
+    svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SvdJob &job = jobs[idx_map[blockIdx.x]];
+    const int m = job.m, n = job.n;
+    double2 *sA = reinterpret_cast<double2 *>(smem_raw);
+    double2 *sV = sA + (size_t)m * n;
+    __shared__ int s_rot;
+    for (int idx = threadIdx.x; idx < m * n; idx += blockDim.x) sA[idx] = job.A[idx];
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x)
+        sV[idx] = make_double2((idx % n) == (idx / n) ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    const int team = pick_team(m);
+    const double tol = (double)(m > 1 ? m : 1) * DBL_EPSILON;
+    int sweep = 0, converged = 0;
+    for (; sweep < max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) s_rot = 0;
+        __syncthreads();
+        inner_sweep(sA, m, sV, n, n, team, tol, &s_rot);
+        __syncthreads();
+        const int rot = s_rot;
+        __syncthreads();
+        if (!rot) {
+            converged = 1;
+            break;
+        }
+    }
+    for (int idx = threadIdx.x; idx < m * n; idx += blockDim.x) job.A[idx] = sA[idx];
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) job.V[idx] = sV[idx];
+    finish_sigma(sA, m, m, n, job.sigma, job.perm);
+    if (threadIdx.x == 0) {
+        job.status = converged ? PSKEL_OK : PSKEL_ERR_NOCONV;
+        job.sweeps = sweep + (converged ? 1 : 0);
+    }
+}
+
+// Blocked variant: 2b columns at a time in shared memory.
+__global__ void __launch_bounds__(kSvdThreads)
+    svd_blocked_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps, int smem_bytes) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SvdJob &job = jobs[idx_map[blockIdx.x]];
+    const int m = job.m, n = job.n;
+    int b = (int)(smem_bytes / (2 * (size_t)(m + n) * sizeof(double2)));
+    if (b < 1) b = 1;
+    if (b > n) b = n;
+    int nb = (n + b - 1) / b;
+    double2 *sA = reinterpret_cast<double2 *>(smem_raw);  // m x 2b
+    double2 *sV = sA + (size_t)m * 2 * b;                  // n x 2b
+    __shared__ int s_rot;
+    __shared__ int s_any;
+    // V = I
+    for (size_t idx = threadIdx.x; idx < (size_t)n * n; idx += blockDim.x)
+        job.V[idx] = make_double2((idx % n) == (idx / n) ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    const int team = pick_team(m);
+    const double tol = (double)(m > 1 ? m : 1) * DBL_EPSILON;
+    int sweep = 0, converged = 0;
+    if (nb == 1) nb = 2;  // a single block still needs its own inner sweep: pair it with empty
+    for (; sweep < max_sweeps; ++sweep) {
+        if (threadIdx.x == 0) s_any = 0;
+        for (int P = 0; P < nb; ++P) {
+            for (int Q = P + 1; Q < nb; ++Q) {
+                const int p0 = P * b, pw = max(0, min(b, n - p0));
+                const int q0 = Q * b, qw = max(0, min(b, n - q0));
+                const int w = pw + qw;
+                if (w == 0) continue;
+                // load columns [p0, p0+pw) and [q0, q0+qw)
+                for (size_t idx = threadIdx.x; idx < (size_t)m * w; idx += blockDim.x) {
+                    const int c = (int)(idx / m), r = (int)(idx % m);
+                    const int gc = c < pw ? p0 + c : q0 + (c - pw);
+                    sA[idx] = job.A[(size_t)gc * m + r];
+                }
+                for (size_t idx = threadIdx.x; idx < (size_t)n * w; idx += blockDim.x) {
+                    const int c = (int)(idx / n), r = (int)(idx % n);
+                    const int gc = c < pw ? p0 + c : q0 + (c - pw);
+                    sV[idx] = job.V[(size_t)gc * n + r];
+                }
+                if (threadIdx.x == 0) s_rot = 0;
+                __syncthreads();
+                inner_sweep(sA, m, sV, n, w, team, tol, &s_rot);
+                __syncthreads();
+                if (s_rot) {
+                    for (size_t idx = threadIdx.x; idx < (size_t)m * w; idx += blockDim.x) {
+                        const int c = (int)(idx / m), r = (int)(idx % m);
+                        const int gc = c < pw ? p0 + c : q0 + (c - pw);
+                        job.A[(size_t)gc * m + r] = sA[idx];
+                    }
+                    for (size_t idx = threadIdx.x; idx < (size_t)n * w; idx += blockDim.x) {
+                        const int c = (int)(idx / n), r = (int)(idx % n);
+                        const int gc = c < pw ? p0 + c : q0 + (c - pw);
+                        job.V[(size_t)gc * n + r] = sV[idx];
+                    }
+                    if (threadIdx.x == 0) s_any = 1;
+                }
+                __syncthreads();
+            }
+        }
+        __syncthreads();
+        const int any = s_any;
+        __syncthreads();
+        if (!any) {
+            converged = 1;
+            break;
+        }
+    }
+    __syncthreads();
+    finish_sigma(job.A, m, m, n, job.sigma, job.perm);
+    if (threadIdx.x == 0) {
+        job.status = converged ? PSKEL_OK : PSKEL_ERR_NOCONV;
+        job.sweeps = sweep + (converged ? 1 : 0);
+    }
+}
+
+static size_t resident_bytes(int m, int n) { return sizeof(double2) * ((size_t)m * n + (size_t)n * n); }
+
+int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_res,
+             size_t *max_res_smem) {
+    const int nj = (int)h_jobs.size();
+    idx.clear();
+    idx.reserve(nj);
+    *n_res = 0;
+    *max_res_smem = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (int i = 0; i < nj; ++i) {
+            const SvdJob &j = h_jobs[i];
+            if (j.m < j.n || j.n <= 0 || j.m <= 0) {
+                set_error(PSKEL_ERR_ARG, "svd: job %d has m=%d < n=%d or is empty", i, j.m, j.n);
+                return PSKEL_ERR_ARG;
+            }
+            const bool fits = resident_bytes(j.m, j.n) <= kSmemBudget;
+            if (fits == (pass == 0)) {
+                idx.push_back(i);
+                if (fits) {
+                    ++*n_res;
+                    *max_res_smem = std::max(*max_res_smem, resident_bytes(j.m, j.n));
+                }
+            }
+        }
+    return PSKEL_OK;
+}
+
+int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
+               int max_sweeps, cudaStream_t stream) {
+    static bool attr = false;
+    if (!attr) {
+        PSKEL_CUDA(cudaFuncSetAttribute(svd_resident_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kSmemBudget));
+        PSKEL_CUDA(cudaFuncSetAttribute(svd_blocked_kernel,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kSmemBudget));
+        attr = true;
+    }
+    if (n_res > 0) {
+        svd_resident_kernel<<<n_res, kSvdThreads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
+        PSKEL_CUDA(cudaGetLastError());
+    }
+    if (n_blk > 0) {
+        svd_blocked_kernel<<<n_blk, kSvdThreads, kSmemBudget, stream>>>(d_jobs, d_idx + n_res,
+                                                                        max_sweeps, (int)kSmemBudget);
+        PSKEL_CUDA(cudaGetLastError());
+    }
+    return PSKEL_OK;
+}
+
+int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
+                cudaStream_t stream, DevBuf &scratch) {
+    const int nj = (int)h_jobs.size();
+    if (nj == 0) return PSKEL_OK;
+    std::vector<int> idx;
+    int n_res = 0;
+    size_t max_res = 0;
+    PSKEL_TRY(svd_plan(h_jobs, idx, &n_res, &max_res));
+    PSKEL_TRY(scratch.reserve(sizeof(int) * idx.size()));
+    int *d_idx = scratch.as<int>();
+    PSKEL_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
+                               stream));
+    return svd_launch(d_jobs, d_idx, n_res, nj - n_res, max_res, max_sweeps, stream);
+}
+
+// ------------------------------------------------------------------ pseudo-inverse
+// P (n x m) = sum over kept j of (1/sigma_j^2) V[:, j] conj(AV[:, j])^T; one CTA per 32x32
+// output tile of one job (grid.y = job), K loop over the n columns in chunks of 16.
+__global__ void __launch_bounds__(256) pinv_kernel(const PinvJob *jobs) {
+    const PinvJob job = jobs[blockIdx.y];
+    const int n = job.n, m = job.m;
+    const int tiles_a = (n + 31) / 32;
+    const int tiles_b = (m + 31) / 32;
+    if ((int)blockIdx.x >= tiles_a * tiles_b) return;
+    const int a0 = (blockIdx.x % tiles_a) * 32;
+    const int b0 = (blockIdx.x / tiles_a) * 32;
+    __shared__ double smax;
+    __shared__ double w[16];
+    __shared__ double2 sVt[16][33];
+    __shared__ double2 sAt[16][33];
+    if (threadIdx.x == 0) {
+        double mx = 0;
+        for (int j = 0; j < n; ++j) mx = fmax(mx, job.sigma[j]);
+        smax = mx;
+    }
+    __syncthreads();
+    const double thr = job.relative ? job.tau * smax : job.tau;
+    const int tx = threadIdx.x % 32;  // output row a0 + tx
+    const int ty = threadIdx.x / 32;  // 8 groups of 4 output columns
+    double2 acc[4];
+    for (int c = 0; c < 4; ++c) acc[c] = make_double2(0, 0);
+    for (int k0 = 0; k0 < n; k0 += 16) {
+        if (threadIdx.x < 16) {
+            const int j = k0 + threadIdx.x;
+            double wj = 0;
+            if (j < n) {
+                const double s = job.sigma[j];
+                if (s >= thr && s > 0) wj = 1.0 / (s * s);
+            }
+            w[threadIdx.x] = wj;
+        }
+        for (int idx = threadIdx.x; idx < 16 * 32; idx += 256) {
+            const int kk = idx / 32, r = idx % 32;
+            const int j = k0 + kk;
+            sVt[kk][r] = (j < n && a0 + r < n) ? job.V[(size_t)j * n + a0 + r] : make_double2(0, 0);
+            sAt[kk][r] = (j < n && b0 + r < m) ? job.AV[(size_t)j * m + b0 + r] : make_double2(0, 0);
+        }
+        __syncthreads();
+        for (int kk = 0; kk < 16; ++kk) {
+            const double wk = w[kk];
+            if (wk == 0.0) continue;
+            const double2 v = sVt[kk][tx];
+            const double2 vw = make_double2(v.x * wk, v.y * wk);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const double2 a = sAt[kk][ty * 4 + c];  // conj(a)
+                acc[c].x = fma(vw.x, a.x, fma(vw.y, a.y, acc[c].x));
+                acc[c].y = fma(vw.y, a.x, fma(-vw.x, a.y, acc[c].y));
+            }
+        }
+        __syncthreads();
+    }
+    const int ra = a0 + tx;
+    if (ra < n) {
+        for (int c = 0; c < 4; ++c) {
+            const int cb = b0 + ty * 4 + c;
+            if (cb < m) job.P[ra + (size_t)cb * n] = acc[c];
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && job.rank) {
+        int k = 0;
+        for (int j = 0; j < n; ++j) k += (job.sigma[j] >= thr && job.sigma[j] > 0);
+        *job.rank = k;
+    }
+}
+
+int batched_pinv(const PinvJob *d_jobs, int njobs, int max_tiles, cudaStream_t stream) {
+    if (njobs <= 0) return PSKEL_OK;
+    dim3 grid(max_tiles, njobs);
+    pinv_kernel<<<grid, 256, 0, stream>>>(d_jobs);
+    PSKEL_CUDA(cudaGetLastError());
+    return PSKEL_OK;
+}
+
+}  // namespace pskel

@@ -1,0 +1,176 @@
+// Shared internals of libpskel_b200: status handling, device buffers, mesh records.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "pskel.h"
+
+namespace pskel {
+
+// ------------------------------------------------------------------ errors
+void set_error(int code, const char *fmt, ...);
+int last_code();
+
+#define PSKEL_CUDA(call)                                                                   \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            ::pskel::set_error(e_ == cudaErrorMemoryAllocation ? PSKEL_ERR_OOM            \
+                                                               : PSKEL_ERR_CUDA,          \
+                               "%s:%d %s: %s", __FILE__, __LINE__, #call,                  \
+                               cudaGetErrorString(e_));                                    \
+            return e_ == cudaErrorMemoryAllocation ? PSKEL_ERR_OOM : PSKEL_ERR_CUDA;       \
+        }                                                                                  \
+    } while (0)
+
+#define PSKEL_TRY(expr)                      \
+    do {                                     \
+        int s_ = (expr);                     \
+        if (s_ != PSKEL_OK) return s_;       \
+    } while (0)
+
+// ------------------------------------------------------------------ device buffer
+// Grow-only device allocation reused across calls (no cudaMalloc on the steady path).
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t want) {
+        if (want <= bytes) return PSKEL_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        size_t sz = want < 256 ? 256 : want;
+        sz = (sz + 255) & ~size_t(255);
+        PSKEL_CUDA(cudaMalloc(&ptr, sz));
+        bytes = sz;
+        return PSKEL_OK;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// ------------------------------------------------------------------ mesh records
+// Per-RWG quadrature record: for the 2Q points of the basis (Q on T+, then Q on T-), seven
+// fields stored field-major: x[2Q] y[2Q] z[2Q] ux[2Q] uy[2Q] uz[2Q] d[2Q], where
+//   u = w_p * (l/2) * rho(r_p),  rho = s (r_p - v_opp),  d = w_p * s * l,  s = +1 (T+), -1 (T-)
+// so that Z_mn = eta/(4 pi) * sum_{p,q} A_pq (sin kR + j cos kR) / R with
+//   A_pq = d_p e_q / k - k u_p . v_q.
+// The record stride is padded to an odd number of words so that 16 different records read by
+// 16 lanes fall in distinct shared-memory banks.
+__host__ __device__ constexpr int rec_points(int q) { return 2 * q; }
+__host__ __device__ constexpr int rec_stride(int q) { return (7 * 2 * q) | 1; }
+
+struct MeshRecords {
+    int q = 0;
+    DevBuf f64;  // ne * rec_stride(q) doubles
+    DevBuf f32;  // ne * rec_stride(q) floats
+};
+
+struct DevMesh {
+    int ne = 0, nt = 0, nv = 0;
+    DevBuf vertex, topol, edges, ln, cent;  // reference arrays as doubles
+    MeshRecords rec1, rec7;                 // Q = 1 and Q = 7 records (built on demand)
+    MeshRecords &records(int q) { return q == 1 ? rec1 : rec7; }
+};
+
+// Build (or rebuild) the Q-point records of a mesh whose raw arrays are on the device.
+int build_records(DevMesh &mesh, int q, cudaStream_t stream, int *d_flag);
+
+// Upload the raw reference arrays (host, column-major doubles) into mesh.
+int upload_mesh_arrays(DevMesh &mesh, const double *vertex, int nv, const double *topol, int nt,
+                       const double *edges, int ne, const double *ln, const double *cent,
+                       cudaStream_t stream);
+
+// ------------------------------------------------------------------ fill
+// One fill job: Z(rows, cols) -> out (column-major, leading dimension ld). rows/cols are
+// 0-based RWG ids in device memory.
+struct FillJob {
+    const int *rows;
+    const int *cols;
+    void *out;
+    int nr, nc, ld, pad;
+};
+
+struct FillParams {
+    double k, eta;
+    double r_near;     // > 0: flag triangle pairs whose centroids are closer than this
+    int q_test, q_src;
+    int precision;     // PSKEL_C128 / PSKEL_C64
+    int split;         // lanes per entry (1, 2 or 4); 0 = automatic
+};
+
+// Launch the batched fill over jobs (device array) with tile prefix offsets computed on the
+// host (tile_prefix has njobs+1 entries, device). flags[0] receives PSKEL near-field / range
+// bits. Returns PSKEL_OK or an error.
+int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
+                const int *d_tile_prefix, int njobs, int total_tiles, int *d_flags,
+                cudaStream_t stream);
+int fill_tile_shape(int precision, int q, int split, int *tm, int *tn);
+
+// Convert 1-based double ids to 0-based int32 with a range check (flags bit 1 on error).
+int launch_ids_from_double(const double *d_in, int *d_out, int n, int limit, int *d_flags,
+                           cudaStream_t stream);
+int launch_ids_from_int64(const int64_t *d_in, int *d_out, int n, int limit, int *d_flags,
+                          cudaStream_t stream);
+
+// ------------------------------------------------------------------ Jacobi SVD / pinv
+// Batched one-sided Jacobi SVD of complex128 matrices A_b (m_b x n_b, column-major, lda = m_b)
+// with m_b >= n_b. Work is in place: on return A_b holds A_b V_b (orthogonal columns) and V_b
+// (n_b x n_b) the accumulated rotations.
+struct SvdJob {
+    double2 *A;      // m x n, overwritten by A V
+    double2 *V;      // n x n
+    double *sigma;   // n, singular values in column order (unsorted)
+    int *perm;       // n, column indices sorted by decreasing sigma (may be null)
+    int m, n;
+    int status;      // written by the kernel: 0 converged, PSKEL_ERR_NOCONV otherwise
+    int sweeps;
+};
+
+// Run the SVD of every job to convergence (max_sweeps cap). jobs is a DEVICE array; the host
+// copy is used for sizes. Returns PSKEL_OK even if some job failed to converge (their status
+// field says so).
+int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
+                cudaStream_t stream, DevBuf &scratch);
+
+// The same split into a host plan (job order: resident jobs first, then blocked ones) and a
+// launch from device tables, so the launches can be captured in a CUDA graph.
+int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_res,
+             size_t *max_res_smem);
+int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
+               int max_sweeps, cudaStream_t stream);
+
+// pinv of each job after batched_svd: P_b (n_b x m_b) = V diag(1/sigma^2) (A V)^H over the
+// kept columns; rank_b receives the count kept. thr_b = tau (absolute) or tau * sigma_max.
+struct PinvJob {
+    const double2 *AV;
+    const double2 *V;
+    const double *sigma;
+    double2 *P;      // n x m output, ld = n
+    int *rank;
+    int m, n;
+    double tau;
+    int relative;
+};
+int batched_pinv(const PinvJob *d_jobs, int njobs, int max_n, cudaStream_t stream);
+
+// ------------------------------------------------------------------ small dense helpers
+// y = C (U (R x)) and the successive-estimate error of the reference (complex128).
+int cur_matvec_error(const double2 *C, const double2 *U, const double2 *R, const double2 *x,
+                     const double2 *y_old, double2 *y_new, int m, int r, int n, double *err,
+                     cudaStream_t stream, DevBuf &scratch);
+
+// ------------------------------------------------------------------ device properties
+int sm_count();
+
+}  // namespace pskel

@@ -1,0 +1,149 @@
+"""Python front end of the pskel_* handle API (resident mesh, batched far-block compression).
+
+    eng = Engine()
+    eng.upload_mesh(mesh, k=2*pi, eta=376.73, q=7)
+    eng.set_blocks(partition)
+    stats = eng.compress(tol=1e-4, precision="c64", r0=predicted)   # per-block outcome
+    C, U, R, I, J = eng.get_block(b)
+    err = eng.true_errors()                                          # vs dense FP64 fill
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+
+C128, C64 = 0, 1
+START_REFERENCE, START_GIVEN = 0, 1
+
+
+def _prec(p) -> int:
+    if p in (C128, "c128", "complex128", "f64"):
+        return C128
+    if p in (C64, "c64", "complex64", "f32"):
+        return C64
+    raise ValueError(f"precision {p!r}")
+
+
+class Engine:
+    def __init__(self, device: int = 0):
+        self._lib = _lib.lib()
+        h = ctypes.c_void_p()
+        _lib.check(self._lib.pskel_create(ctypes.byref(h), device))
+        self._h = h
+        self.mesh = None
+        self.partition = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.pskel_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------ mesh / blocks
+    def upload_mesh(self, mesh, k: float, eta: float, q: int = 7):
+        a = mesh.as_f64()
+        p = lambda x: x.ctypes.data_as(_lib.D)
+        em = _lib.EM(k=float(k), eta=float(eta), q_test=int(q), q_src=int(q))
+        _lib.check(self._lib.pskel_upload_mesh(self._h, p(a["vertex"]), mesh.Nv, p(a["topol"]),
+                                               mesh.Nt, p(a["edges"]), mesh.N, p(a["ln"]),
+                                               p(a["cent"]), ctypes.byref(em)))
+        self.mesh = mesh
+        self.k, self.eta, self.q = k, eta, q
+
+    def set_blocks(self, part=None, *, group_ptr=None, group_ids=None, gt=None, gs=None):
+        if part is not None:
+            group_ptr, group_ids, gt, gs = part.group_ptr, part.group_ids, part.gt, part.gs
+        gp = np.ascontiguousarray(group_ptr, dtype=np.int32)
+        gi = np.ascontiguousarray(group_ids, dtype=np.int32)
+        t = np.ascontiguousarray(gt, dtype=np.int32)
+        s = np.ascontiguousarray(gs, dtype=np.int32)
+        P = lambda x: x.ctypes.data_as(_lib.I32)
+        _lib.check(self._lib.pskel_set_blocks(self._h, P(gp), P(gi), len(gp) - 1, P(t), P(s), len(t)))
+        self.partition = part
+        self._gp, self._gi, self._gt, self._gs = gp, gi, t, s
+
+    @property
+    def n_blocks(self) -> int:
+        return len(self._gt)
+
+    def block_ids(self, b: int):
+        """0-based RWG ids of the rows and columns of block b."""
+        gt, gs = self._gt[b], self._gs[b]
+        return (self._gi[self._gp[gt]:self._gp[gt + 1]], self._gi[self._gp[gs]:self._gp[gs + 1]])
+
+    # ------------------------------------------------------------------ compression
+    def compress(self, tol: float, *, precision="c128", tau: float = 1e-8, tau_relative=True,
+                 r0=None, oversample: int = 10, extra_rows: int = 10, max_rounds: int = 12,
+                 seed: int = 0, use_graph: bool = False, recompress: bool = False,
+                 recompress_tol: float = 0.0) -> np.ndarray:
+        """Compress every block; returns a structured array of per-block stats
+        (m, n, r, rank, rank_recompressed, rounds, status, est)."""
+        o = _lib.Opts(tol=tol, tau=tau, tau_relative=int(bool(tau_relative)),
+                      precision=_prec(precision),
+                      start=START_GIVEN if r0 is not None else START_REFERENCE,
+                      oversample=int(oversample), extra_rows=int(extra_rows),
+                      max_rounds=int(max_rounds), seed=int(seed), recompress=int(recompress),
+                      recompress_tol=float(recompress_tol), use_graph=int(bool(use_graph)))
+        nb = self.n_blocks
+        stats = (_lib.BlockStat * nb)()
+        if r0 is not None:
+            r0a = np.ascontiguousarray(r0, dtype=np.int32)
+            if len(r0a) != nb:
+                raise ValueError("r0 must have one entry per block")
+            rp = r0a.ctypes.data_as(_lib.I32)
+        else:
+            r0a = None
+            rp = None
+        _lib.check(self._lib.pskel_compress_blocks(self._h, ctypes.byref(o), rp, stats))
+        self._precision = o.precision
+        dt = np.dtype([("m", "i4"), ("n", "i4"), ("r", "i4"), ("rank", "i4"),
+                       ("rank_recompressed", "i4"), ("rounds", "i4"), ("status", "i4"),
+                       ("est", "f8")])
+        return np.frombuffer(bytes(stats), dtype=dt).copy()
+
+    def timing(self) -> dict:
+        t = np.zeros(6)
+        _lib.check(self._lib.pskel_last_timing(self._h, t.ctypes.data_as(_lib.D)))
+        return dict(zip(("sample", "fill", "pinv", "estimate", "recompress", "total"), t.tolist()))
+
+    def get_block(self, b: int, stats=None):
+        rows, cols = self.block_ids(b)
+        m, n = len(rows), len(cols)
+        if stats is None:
+            raise ValueError("pass the stats array returned by compress()")
+        r = int(stats["r"][b])
+        C = np.zeros((m, r), dtype=np.complex128, order="F")
+        U = np.zeros((r, r), dtype=np.complex128, order="F")
+        R = np.zeros((r, n), dtype=np.complex128, order="F")
+        I = np.zeros(r, dtype=np.int32)
+        J = np.zeros(r, dtype=np.int32)
+        vp = lambda x: ctypes.c_void_p(x.ctypes.data)
+        _lib.check(self._lib.pskel_get_block(self._h, b, vp(C), vp(U), vp(R),
+                                             I.ctypes.data_as(_lib.I32), J.ctypes.data_as(_lib.I32)))
+        return C, U, R, I, J
+
+    def true_errors(self) -> np.ndarray:
+        err = np.zeros(self.n_blocks)
+        _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
+        return err
+
+    def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,
+                    precision="c128"):
+        """Fill into device buffers given as raw device pointers (e.g. torch data_ptr())."""
+        _lib.check(self._lib.pskel_fill_device(self._h, ctypes.c_void_p(rows_dev), nr,
+                                               ctypes.c_void_p(cols_dev), nc,
+                                               ctypes.c_void_p(out_dev), ld, _prec(precision)))

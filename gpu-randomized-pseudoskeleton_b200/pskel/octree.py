@@ -1,0 +1,104 @@
+"""Single-level octree grouping of RWG basis functions and the far-field block list.
+
+The reference has no partitioner of its own: its only multi-block code rebuilds a matrix from
+block lists produced by MATLAB (compres_single_block_spheres.jl:1109-1347; the .mat data are
+not shipped). This module supplies the partition the far-field workloads are defined on:
+
+* every RWG is assigned to the leaf box containing its basis centre (mean of its two triangle
+  centroids, ``user_get_OG_basis_center.m:36-39``); boxes are cubes of side ``leaf`` aligned
+  at ``origin`` (default: the mesh's bounding-box centre);
+* groups = non-empty leaf boxes, listed in Morton order of their integer box coordinates;
+  groups smaller than ``min_group`` are merged into the nearest larger group (by box-centre
+  distance) so that every block has at least that many rows and columns;
+* far pairs = ordered group pairs (i, j), i != j, whose box centres are at least
+  ``admissibility`` x the box diameter (sqrt(3) * leaf) apart.
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Partition:
+    group_ptr: np.ndarray   # (G+1,) int32 CSR offsets
+    group_ids: np.ndarray   # (N,) int32 0-based RWG ids grouped
+    centres: np.ndarray     # (G, 3) group centre (centre of the group's bounding box of boxes)
+    extents: np.ndarray     # (G,) diameter of the bounding sphere of the group's basis centres
+    gt: np.ndarray          # (B,) test group of each far block
+    gs: np.ndarray          # (B,) source group of each far block
+    leaf: float
+
+    @property
+    def n_groups(self) -> int:
+        return len(self.group_ptr) - 1
+
+    @property
+    def n_blocks(self) -> int:
+        return len(self.gt)
+
+    def sizes(self) -> np.ndarray:
+        return np.diff(self.group_ptr)
+
+    def members(self, g: int) -> np.ndarray:
+        return self.group_ids[self.group_ptr[g]:self.group_ptr[g + 1]]
+
+
+def _morton3(ix, iy, iz):
+    def spread(v):
+        v = v.astype(np.uint64) & np.uint64(0x1FFFFF)
+        v = (v | (v << np.uint64(32))) & np.uint64(0x1F00000000FFFF)
+        v = (v | (v << np.uint64(16))) & np.uint64(0x1F0000FF0000FF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x100F00F00F00F00F)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x10C30C30C30C30C3)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x1249249249249249)
+        return v
+    return spread(ix) | (spread(iy) << np.uint64(1)) | (spread(iz) << np.uint64(2))
+
+
+def partition(mesh, leaf: float, origin=None, admissibility: float = 2.0,
+              min_group: int = 1, symmetric: bool = False) -> Partition:
+    c = mesh.basis_centres().T  # (N, 3)
+    if origin is None:
+        origin = 0.5 * (c.min(axis=0) + c.max(axis=0))
+    origin = np.asarray(origin, dtype=np.float64)
+    idx = np.floor((c - origin) / leaf).astype(np.int64)
+    shift = idx.min(axis=0)
+    ui = idx - shift
+    keys = _morton3(ui[:, 0], ui[:, 1], ui[:, 2])
+    order = np.lexsort((np.arange(len(keys)), keys))
+    ks = keys[order]
+    starts = np.concatenate([[0], np.nonzero(np.diff(ks))[0] + 1, [len(ks)]])
+    groups = [order[starts[i]:starts[i + 1]] for i in range(len(starts) - 1)]
+    box_centre = [origin + (idx[g[0]] + 0.5) * leaf for g in groups]
+    # merge small groups into the nearest group that is already large enough
+    if min_group > 1:
+        sizes = np.array([len(g) for g in groups])
+        big = [i for i in range(len(groups)) if sizes[i] >= min_group]
+        if not big:
+            big = [int(np.argmax(sizes))]
+        bc = np.array(box_centre)
+        merged = {i: list(groups[i]) for i in big}
+        for i in range(len(groups)):
+            if i in merged:
+                continue
+            j = big[int(np.argmin(np.linalg.norm(bc[big] - bc[i], axis=1)))]
+            merged[j].extend(groups[i])
+        keep = sorted(merged)
+        groups = [np.sort(np.array(merged[i], dtype=np.int64)) for i in keep]
+        box_centre = [box_centre[i] for i in keep]
+    ptr = np.zeros(len(groups) + 1, dtype=np.int32)
+    ptr[1:] = np.cumsum([len(g) for g in groups])
+    ids = np.concatenate(groups).astype(np.int32)
+    centres = np.array(box_centre)
+    ext = np.array([2 * np.linalg.norm(c[g] - c[g].mean(axis=0), axis=1).max() for g in groups])
+    diam = np.sqrt(3.0) * leaf
+    d = np.linalg.norm(centres[:, None, :] - centres[None, :, :], axis=2)
+    far = d >= admissibility * diam
+    np.fill_diagonal(far, False)
+    if symmetric:
+        far = np.triu(far, 1)
+    gt, gs = np.nonzero(far)
+    return Partition(group_ptr=ptr, group_ids=ids, centres=centres, extents=ext,
+                     gt=gt.astype(np.int32), gs=gs.astype(np.int32), leaf=leaf)

@@ -1,0 +1,244 @@
+/*
+ * pskel.h - C ABI of the B200 pseudoskeleton (CUR) library (libpskel_b200.so).
+ *
+ * Two groups of entry points:
+ *
+ *  1. Reference-named symbols, drop-ins for the ones the reference's Julia drivers ccall from
+ *     "./functionsExternal_cuda.so" and "./functions_cur_external_cuda.so". Argument lists and
+ *     return types are the reference's, in the same order; each declaration cites the
+ *     definition it replaces (paths relative to codes/GPU_implementation/seed/). As in the
+ *     reference, every pointer is a HOST pointer, every matrix is column-major, and the
+ *     r1/r2/row_samples/col_samples arrays hold 1-based RWG ids stored as doubles even though
+ *     the C prototype says int* (the Julia callers pass Vector{Cdouble}; the reference copies
+ *     n*sizeof(double) bytes, user_impedance_for_julia_cuda.cu:1100-1101,1735-1736).
+ *     Launch-geometry arguments (blocks_*, threads_*, limx, limy) are accepted and ignored:
+ *     the library picks its own launch shapes. Errors: functions returning double return NaN,
+ *     functions returning int return 0 (the reference returns 1 on success and has no error
+ *     path); pskel_last_error() gives the reason.
+ *
+ *  2. pskel_* handle API: the mesh, group lists and compressed blocks stay resident on the
+ *     device; calls return PSKEL_OK (0) or a negative status.
+ *
+ * Mesh arrays (column-major Float64, 1-based ids, as passed by the Julia wrappers, e.g.
+ * compres_single_block_spheres_for_sweep2.jl:380-388): vertex 3 x Nv, topol 3 x Nt,
+ * trian 3 x Nt, edges 4 x Ne (T+, T-, opposite vertex in T+, opposite vertex in T-),
+ * un 3 x Nt, ds 1 x Nt, ln Ne, cent 3 x Nt. Only vertex, topol, edges, ln and cent are read.
+ */
+#ifndef PSKEL_H
+#define PSKEL_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* complex128 laid out like Julia ComplexF64 / cuDoubleComplex */
+typedef struct { double re, im; } pskel_c128;
+/* complex64 laid out like Julia ComplexF32 / cuFloatComplex */
+typedef struct { float re, im; } pskel_c64;
+
+/* ---------------------------------------------------------------- status codes */
+#define PSKEL_OK 0
+#define PSKEL_ERR_ARG (-1)        /* bad size, pointer or option */
+#define PSKEL_ERR_CUDA (-2)       /* a CUDA runtime call failed */
+#define PSKEL_ERR_NOCONV (-3)     /* Jacobi SVD hit its sweep limit */
+#define PSKEL_ERR_NEAR (-4)       /* a triangle pair lies inside an integration radius */
+#define PSKEL_ERR_OOM (-5)        /* device allocation failed */
+#define PSKEL_ERR_RANGE (-6)      /* an RWG id is out of range */
+#define PSKEL_ERR_UNSUPPORTED (-7) /* field != 1 (only EFIE is implemented) */
+#define PSKEL_ERR_STATE (-8)      /* call order (e.g. no mesh uploaded) */
+
+/* Last error of the calling thread: status code and a short message. */
+int pskel_last_error(const char **message);
+
+/* ======================================================= 1. reference-named entry points */
+
+/* Dense fill of Z(r1, r2) into Ztotal (n_r1 x n_r2 complex128). Returns the fill kernel time
+   in ms. Replaces impedance_matrix_cuda_elbyel4, user_impedance_for_julia_cuda.cu:1022-1064
+   (Julia caller compres_single_block_spheres_for_sweep2.jl:433-478). */
+double impedance_matrix_cuda_elbyel4(pskel_c128 *Ztotal, int field, double k, double eta,
+    double Rinteg_s, double Ranal_s, double Rinteg_f, int cor_solid, int flag, int *r1, int *r2,
+    double *vertex, double *topol, double *trian, double *edges, double *un, double *ds,
+    double *ln, double *cent, int N, int n_r1, int n_r2, int rows_vertex, int cols_vertex,
+    int rows_topol, int cols_topol, int rows_trian, int cols_trian, int rows_edges,
+    int cols_edges, int rows_un, int cols_un, int rows_ds, int cols_ds, int n_ln,
+    int rows_cent, int cols_cent, int blocks_x, int blocks_y, int threads_x, int threads_y,
+    int limx, int limy);
+
+/* Same fill, returns 1. Replaces impedance_matrix_cuda_elbyel3,
+   user_impedance_for_julia_cuda.cu:770-812 (caller compres_single_block_spheres.jl:1708). */
+int impedance_matrix_cuda_elbyel3(pskel_c128 *Ztotal, int field, double k, double eta,
+    double Rinteg_s, double Ranal_s, double Rinteg_f, int cor_solid, int flag, int *r1, int *r2,
+    double *vertex, double *topol, double *trian, double *edges, double *un, double *ds,
+    double *ln, double *cent, int N, int n_r1, int n_r2, int rows_vertex, int cols_vertex,
+    int rows_topol, int cols_topol, int rows_trian, int cols_trian, int rows_edges,
+    int cols_edges, int rows_un, int cols_un, int rows_ds, int cols_ds, int n_ln,
+    int rows_cent, int cols_cent, int blocks_x, int blocks_y, int threads_x, int threads_y,
+    int limx, int limy);
+
+/* Same fill into split real/imaginary arrays, returns 1. Replaces
+   impedance_matrix_cuda_elbyel2, user_impedance_for_julia_cuda.cu:602-645
+   (caller compres_single_block_spheres.jl:1578). */
+int impedance_matrix_cuda_elbyel2(double *Zr, double *Zi, int field, double k, double eta,
+    double Rinteg_s, double Ranal_s, double Rinteg_f, int cor_solid, int flag, int *r1, int *r2,
+    double *vertex, double *topol, double *trian, double *edges, double *un, double *ds,
+    double *ln, double *cent, int N, int n_r1, int n_r2, int rows_vertex, int cols_vertex,
+    int rows_topol, int cols_topol, int rows_trian, int cols_trian, int rows_edges,
+    int cols_edges, int rows_un, int cols_un, int rows_ds, int cols_ds, int n_ln,
+    int rows_cent, int cols_cent, int blocks_x, int blocks_y, int threads_x, int threads_y,
+    int limx, int limy);
+
+/* Split-array fill of Z(r1, r2) into Zr/Zi; the C/U/R outputs are left untouched and
+   tol_compress is ignored, exactly as in the reference. Returns 1. Replaces cuda_cur_pure,
+   user_impedance_for_julia_cuda.cu:1273-1432 (caller compres_single_block_spheres.jl:2035). */
+int cuda_cur_pure(double *Zr, double *Zi, int field, double k, double eta, double Rinteg_s,
+    double Ranal_s, double Rinteg_f, int cor_solid, int flag, int *r1, int *r2, double *vertex,
+    double *topol, double *trian, double *edges, double *un, double *ds, double *ln,
+    double *cent, double *Cmat_r, double *Cmat_i, double *Umat_r, double *Umat_i,
+    double *Rmat_r, double *Rmat_i, int N, int n_r1, int n_r2, int rows_vertex,
+    int cols_vertex, int rows_topol, int cols_topol, int rows_trian, int cols_trian,
+    int rows_edges, int cols_edges, int rows_un, int cols_un, int rows_ds, int cols_ds,
+    int n_ln, int rows_cent, int cols_cent, int blocks_x, int blocks_y, int threads_x,
+    int threads_y, int limx, int limy, double tol_compress);
+
+/* One CUR round with caller-supplied samples: C = Z(r1, col_samples) (n_r1 x cur_order),
+   U = pinv(Z(row_samples, col_samples)) with singular values below the ABSOLUTE threshold
+   pinv_tol dropped, R = Z(row_samples, r2) (cur_order x n_r2), Avtest_new = C (U (R vtest)).
+   Returns ||Avtest_old - Avtest_new|| / ||Avtest_new||; vec_time_cuda[0] = device time of
+   the round in ms (the reference reports alloc + compute ms and excludes the mesh upload and
+   result download, user_impedance_for_julia_cuda.cu:1706-1711,1965-1975; here the device
+   buffers are pooled, so the figure is compute only). Ztotal is unused. Replaces
+   cuda_complete_compression, user_impedance_for_julia_cuda.cu:1564-1629
+   (caller compres_single_block_spheres_for_sweep2.jl:591-660). */
+double cuda_complete_compression(pskel_c128 *Ccompressed, pskel_c128 *Ucompressed,
+    pskel_c128 *Rcompressed, int cur_order, double *vec_time_cuda, double pinv_tol,
+    pskel_c128 *Avtest_old, pskel_c128 *Avtest_new, pskel_c128 *vtest, int *col_samples,
+    int *row_samples, int C_blocks_x, int C_blocks_y, int C_threads_x, int C_threads_y,
+    int U_blocks_x, int U_blocks_y, int U_threads_x, int U_threads_y, int R_blocks_x,
+    int R_blocks_y, int R_threads_x, int R_threads_y, pskel_c128 *Ztotal, int field, double k,
+    double eta, double Rinteg_s, double Ranal_s, double Rinteg_f, int cor_solid, int flag,
+    int *r1, int *r2, double *vertex, double *topol, double *trian, double *edges, double *un,
+    double *ds, double *ln, double *cent, int N, int n_r1, int n_r2, int rows_vertex,
+    int cols_vertex, int rows_topol, int cols_topol, int rows_trian, int cols_trian,
+    int rows_edges, int cols_edges, int rows_un, int cols_un, int rows_ds, int cols_ds,
+    int n_ln, int rows_cent, int cols_cent, int blocks_x, int blocks_y, int threads_x,
+    int threads_y, int limx, int limy);
+
+/* Avtest_new = C (U (R vtest)) with C M1 x N1, U N1 x N1, R N1 x M2; returns
+   ||Avtest_old - Avtest_new|| / ||Avtest_new||. Replaces compute_error_compression,
+   user_impedance_for_julia_cuda.cu:1449-1556 and cur_external_cuda.cu:612-725
+   (caller compres_single_block_spheres_for_sweep2.jl:992-995). */
+double compute_error_compression(pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
+    pskel_c128 *Avtest_old, pskel_c128 *Avtest_new, pskel_c128 *vtest, int M1, int N1, int M2);
+
+/* CUR of a dense host matrix A (M x N) at given 1-based samples: C = A(:, col_samples),
+   R = A(row_samples, :), U = pinv(A(row_samples, col_samples)) with absolute threshold
+   tolerance. Returns 1. The sample arrays are Int64, as the Julia caller passes them
+   (compres_single_block_spheres_for_sweep2.jl:777-789 declares Ptr{Int64}; the reference's C
+   prototype says int*). Replaces aux_pinv_compression, cur_external_cuda.cu:572-610. */
+int aux_pinv_compression(pskel_c128 *C, pskel_c128 *U, pskel_c128 *R, pskel_c128 *A,
+    int64_t *row_samples, int64_t *col_samples, int ns, int M, int N, double tolerance);
+
+/* pinvA (N x M) = V diag(s >= treshold ? 1/s : 0) U^H of A (M x N); also returns the thin
+   left singular vectors U (M x min(M,N)), S (min(M,N)) and, as the reference does,
+   diag(1/s) V^H in Vt (N x N, rows beyond min(M,N) zero). Returns 1. Replaces cuda_pinv,
+   cur_external_cuda.cu:217-367. */
+int cuda_pinv(pskel_c128 *pinvA, pskel_c128 *U, double *S, pskel_c128 *Vt, pskel_c128 *A,
+    int M, int N, double treshold);
+
+/* Thin SVD A = U diag(S) Vt of A (M x N): U M x min(M,N), S min(M,N) descending, Vt N x N
+   (rows beyond min(M,N) zero). Returns 1. Replaces cuda_svd (cur_external_cuda.cu:400-517)
+   and cuda_svd2 (cur_external_cuda.cu:86-201), which compute the same outputs. */
+int cuda_svd(pskel_c128 *U, double *S, pskel_c128 *Vt, pskel_c128 *A, int M, int N);
+int cuda_svd2(pskel_c128 *U, double *S, pskel_c128 *Vt, pskel_c128 *A, int M, int N);
+
+/* In place V[i] = V[i] < treshold ? 0 : 1/V[i]. Returns 1. Replaces cuda_filter,
+   cur_external_cuda.cu:372-398. */
+int cuda_filter(double *V, double treshold, int N);
+
+/* =========================================================== 2. pskel_* handle API */
+
+typedef struct pskel_ctx pskel_ctx;
+
+/* Precision of the sampled fills and of the stored C/R factors. */
+#define PSKEL_C128 0
+#define PSKEL_C64 1
+
+/* Where each block's first sample count comes from. */
+#define PSKEL_START_REFERENCE 0 /* min(m,n)/10, as the reference's drivers */
+#define PSKEL_START_GIVEN 1     /* the per-block r0 array (e.g. the rank predictor) */
+
+typedef struct {
+    double k, eta;       /* wavenumber and impedance */
+    int q_test, q_src;   /* quadrature points per triangle: 1 (centroid) or 7 */
+} pskel_em_t;
+
+typedef struct {
+    double tol;          /* target relative Frobenius error of each block */
+    double tau;          /* pinv threshold */
+    int tau_relative;    /* 1: keep s >= tau*s_max, 0: keep s >= tau (reference rule) */
+    int precision;       /* PSKEL_C128 or PSKEL_C64 */
+    int start;           /* PSKEL_START_* */
+    int oversample;      /* p added to a given r0 */
+    int extra_rows;      /* rows of the randomized error estimate */
+    int max_rounds;      /* adaptive rounds before giving up (the block keeps its last CUR) */
+    uint64_t seed;       /* Philox seed of the index sets */
+    int recompress;      /* 1: run the recompression after the last round */
+    double recompress_tol; /* relative singular-value threshold of the recompression */
+    int use_graph;       /* 1: replay the first round from a captured CUDA graph */
+} pskel_opts_t;
+
+/* Per-block outcome, filled by pskel_compress_blocks. */
+typedef struct {
+    int m, n;            /* block rows (test RWG) and columns (source RWG) */
+    int r;               /* final sample count */
+    int rank;            /* singular values kept by the pinv */
+    int rank_recompressed; /* rank after recompression (0 if not run) */
+    int rounds;          /* sampling rounds used (1 = first guess accepted) */
+    int status;          /* PSKEL_OK or a negative status */
+    double est;          /* extra-row error estimate of the final round */
+} pskel_block_stat_t;
+
+int pskel_create(pskel_ctx **ctx, int device);
+int pskel_destroy(pskel_ctx *ctx);
+
+/* Upload a mesh (reference layout, host arrays) and build the device quadrature records. */
+int pskel_upload_mesh(pskel_ctx *ctx, const double *vertex, int nv, const double *topol,
+                      int nt, const double *edges, int ne, const double *ln,
+                      const double *cent, const pskel_em_t *em);
+
+/* Fill Z(rows, cols) into a DEVICE buffer (column-major, leading dimension ld) with 0-based
+   int32 RWG ids in DEVICE memory; precision PSKEL_C128 (pskel_c128*) or PSKEL_C64
+   (pskel_c64*). Asynchronous on the context's stream. */
+int pskel_fill_device(pskel_ctx *ctx, const int *rows_dev, int nr, const int *cols_dev,
+                      int nc, void *Z_dev, int ld, int precision);
+
+/* Groups (CSR over 0-based RWG ids) and the block list: block b = (test group gt[b],
+   source group gs[b]). Host arrays; copied to the device. */
+int pskel_set_blocks(pskel_ctx *ctx, const int *group_ptr, const int *group_ids,
+                     int n_groups, const int *gt, const int *gs, int n_blocks);
+
+/* Compress every block. r0 (host, n_blocks) is read when opts->start == PSKEL_START_GIVEN.
+   stats (host, n_blocks) receives the per-block outcome. The factors stay on the device. */
+int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r0,
+                          pskel_block_stat_t *stats);
+
+/* Device time in ms of the last pskel_compress_blocks call, split by phase
+   (sample, fill, pinv, estimate, recompress, total). */
+int pskel_last_timing(pskel_ctx *ctx, double *ms6);
+
+/* Copy block b's factors to host buffers (complex128): C m x r, U r x r, R r x n, 0-based
+   local samples I (r) and J (r). Any pointer may be NULL. */
+int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
+                    int *I, int *J);
+
+/* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
+   block); err (host, n_blocks). */
+int pskel_true_errors(pskel_ctx *ctx, double *err);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSKEL_H */

@@ -1,0 +1,77 @@
+"""Handle API: device sampler bit-parity with the oracle, batched fills against the oracle,
+and per-block errors of the batched compression against dense FP64 fills."""
+import numpy as np
+import pytest
+
+from oracle import cur_oracle as co
+from oracle import element as el
+from pskel import mesh as pmesh
+from pskel import octree
+from pskel.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_sphere():
+    m = pmesh.icosphere(2.0, 3)  # 1280 triangles, 1920 RWG
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=20)
+    return m, part
+
+
+def test_sampler_and_fill_parity(small_sphere):
+    m, part = small_sphere
+    k, eta = 2 * np.pi, 376.73
+    with Engine() as eng:
+        eng.upload_mesh(m, k, eta, q=7)
+        eng.set_blocks(part)
+        nb = eng.n_blocks
+        r0 = np.full(nb, 6, dtype=np.int32)
+        st = eng.compress(1.0, precision="c128", r0=r0, oversample=4, seed=1234, max_rounds=1)
+        assert np.all(st["r"] == np.minimum(10, np.minimum(st["m"], st["n"])))
+        for b in list(range(0, nb, max(1, nb // 7)))[:7]:
+            rows, cols = eng.block_ids(b)
+            C, U, R, I, J = eng.get_block(b, st)
+            r = st["r"][b]
+            assert np.array_equal(I, el.sample(r, len(rows), b, 0, 0, 1234))
+            assert np.array_equal(J, el.sample(r, len(cols), b, 0, 1, 1234))
+            Co = el.fill(m, rows + 1, cols[J] + 1, k, eta, 7, 7)
+            Ro = el.fill(m, rows[I] + 1, cols + 1, k, eta, 7, 7)
+            assert np.abs(C - Co).max() / np.abs(Co).max() < 1e-12
+            assert np.abs(R - Ro).max() / np.abs(Ro).max() < 1e-12
+            Uo = co.my_pinv(Co[I, :], 1e-8, relative=True)
+            assert np.linalg.norm(C @ U @ R - Co @ Uo @ Ro) / np.linalg.norm(Co @ Uo @ Ro) < 1e-6
+
+
+@pytest.mark.parametrize("prec", ["c128", "c64"])
+def test_batched_compression_errors(small_sphere, prec):
+    m, part = small_sphere
+    tol = 1e-4
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        st = eng.compress(tol, precision=prec, tau=1e-7, seed=0)
+        assert np.all(st["status"] == 0)
+        err = eng.true_errors()
+    assert np.all(np.isfinite(err))
+    assert np.median(err) < tol
+    assert np.max(err) < 10 * tol, np.max(err)
+    # every block either met the estimate or ran out of room
+    ok = (st["est"] <= tol) | (st["r"] == np.minimum(st["m"], st["n"]))
+    assert np.all(ok)
+
+
+def test_true_error_matches_oracle(small_sphere):
+    m, part = small_sphere
+    k, eta = 2 * np.pi, 376.73
+    with Engine() as eng:
+        eng.upload_mesh(m, k, eta, q=7)
+        eng.set_blocks(part)
+        st = eng.compress(1e-3, precision="c128", tau=1e-6, seed=3)
+        err = eng.true_errors()
+        for b in (0, eng.n_blocks // 2, eng.n_blocks - 1):
+            rows, cols = eng.block_ids(b)
+            C, U, R, I, J = eng.get_block(b, st)
+            Z = el.fill(m, rows + 1, cols + 1, k, eta, 7, 7)
+            e = co.rel_fro_error(Z, C, U, R)
+            assert abs(e - err[b]) <= 1e-6 * max(e, 1e-12) + 1e-12
