@@ -1,0 +1,414 @@
+"""Benchmark: far-block CUR compression time at relative error 1e-4, learned + mixed precision
++ batched (product) against the plain FP64 GPU pseudoskeleton, on the 30,720-RWG sphere.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sphere30k|sphere7k|sphere122k] [--save out.npz]
+
+A step compresses every far-field block of the workload once: rank predictor inference on the
+GPU (own MLP kernel), then one pskel_compress_blocks call (complex FP32 fill with FP64
+geometry, FP64 Jacobi pinv, randomized extra-row/extra-column estimate, plain adaptive growth
+as fallback; the first round replayed from a CUDA graph). ``value`` is ms per step (lower is
+better). Under torchrun the block list is split across ranks (strong scaling, no collective on
+the data path); the step time is the maximum over ranks.
+
+``--impl reference`` times the CPU restatement of the reference's algorithm for this path
+(oracle/: C element integral + numpy LAPACK pinv, plain adaptive growth) on a bounded sample of
+blocks over all host cores and extrapolates to the whole workload.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import multiprocessing as mp
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gpu-randomized-pseudoskeleton_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "far-block CUR compress time @ rel err 1e-4: learned+mixed+batched vs plain GPU"
+K_WAVE, ETA = 2 * np.pi, 376.73
+TOL = 1e-4
+FLOPS_PER_PAIR = 32  # fixed convention for one point-pair evaluation (see roofline.py)
+
+WORKLOADS = {
+    "sphere30k": dict(R=2.0, sub=5, leaf=0.5, min_group=40,
+                      desc="PEC icosphere R=2 lambda, 5 subdivisions (20,480 triangles, 30,720 RWG), "
+                           "octree leaf 0.5 lambda, far pairs at >= 2 box diameters"),
+    "sphere7k": dict(R=2.0, sub=4, leaf=0.5, min_group=30,
+                     desc="PEC icosphere R=2 lambda, 4 subdivisions (7,680 RWG), leaf 0.5 lambda"),
+    "sphere122k": dict(R=4.0, sub=6, leaf=0.5, min_group=40,
+                       desc="PEC icosphere R=4 lambda, 6 subdivisions (81,920 triangles, 122,880 RWG), "
+                            "octree leaf 0.5 lambda"),
+}
+
+PRODUCT = dict(precision="c64", tau=1e-7, extra_rows=16, extra_cols=16, est_safety=2.0,
+               oversample=0, max_rounds=12, seed=0)
+PLAIN = dict(precision="c128", tau=1e-7, extra_rows=16, extra_cols=16, est_safety=2.0,
+             max_rounds=12, seed=0)
+
+
+def build_workload(name):
+    from pskel import mesh as pmesh
+    from pskel import octree
+    w = WORKLOADS[name]
+    m = pmesh.icosphere(w["R"], w["sub"])
+    part = octree.partition(m, w["leaf"], origin=(0, 0, 0), min_group=w["min_group"])
+    return m, part
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def _cpu_worker(args):
+    name, blocks = args
+    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+    from oracle import cur_oracle as co
+    from oracle import element as el
+    m, part = build_workload(name)
+    fill = lambda a, c: el.fill(m, a, c, K_WAVE, ETA, 7, 7)
+    out = []
+    for b in blocks:
+        rows = part.members(part.gt[b]) + 1
+        cols = part.members(part.gs[b]) + 1
+        t0 = time.perf_counter()
+        r = co.plain_adaptive(fill, rows, cols, TOL, int(b), 0, extra_rows=16, extra_cols=16,
+                              safety=2.0, tau=1e-7)
+        out.append((int(b), time.perf_counter() - t0, int(r["r"])))
+    return out
+
+
+def cpu_baseline(name, n_sample=96, seed=0):
+    """Oracle plain adaptive compression (C element integral, numpy/LAPACK pinv) of a random
+    sample of blocks over all host cores; extrapolated to the whole block list."""
+    _, part = build_workload(name)
+    rng = np.random.default_rng(seed)
+    sample = rng.choice(part.n_blocks, min(n_sample, part.n_blocks), replace=False)
+    cores = os.cpu_count() or 1
+    chunks = [(name, sample[i::cores].tolist()) for i in range(cores) if len(sample[i::cores])]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(len(chunks)) as pool:
+        res = [x for part_res in pool.map(_cpu_worker, chunks) for x in part_res]
+    wall = time.perf_counter() - t0
+    per_block = np.array([t for _, t, _ in res])
+    core_s = per_block.sum()
+    est_ms = per_block.mean() * part.n_blocks / cores * 1e3
+    return dict(value=float(est_ms), unit="ms", cores=cores, kind="port",
+                sample=f"{len(sample)} random far blocks of {part.n_blocks} (seed {seed}); "
+                       f"{core_s:.1f} core-s, {wall:.1f} s wall; whole-job time extrapolated "
+                       f"as mean block time x blocks / cores",
+                cpu=_cpu_model())
+
+
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
+                                 f".clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}",
+                                          f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        try:
+            os.remove(self.path)
+        except OSError:
+            pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return dict(sm_mhz=float(np.median(sm)) if sm else None,
+                    sm_max_mhz=float(max(mx)) if mx else None, reasons=reasons,
+                    samples=len(rows), power_w_max=max(float(r[3]) for r in rows
+                                                        if r[3].replace(".", "").isdigit()))
+
+
+# ----------------------------------------------------------------------------- GPU arm
+def run_ours(args, rank, world, dev):
+    import torch
+
+    from pskel import _lib
+    from pskel.engine import Engine
+    from pskel.predictor import Predictor, features
+
+    torch.cuda.set_device(dev)
+    L = _lib.lib()
+    m, part = build_workload(args.workload)
+    # shard blocks over ranks (interleaved: balanced sizes)
+    mine = np.arange(part.n_blocks)[rank::world]
+    sub_gt, sub_gs = part.gt[mine], part.gs[mine]
+    pred = Predictor.load()
+    eng = Engine(dev)
+    eng.upload_mesh(m, K_WAVE, ETA, q=7)
+    eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt, gs=sub_gs)
+    nb = len(mine)
+
+    class Sub:  # the rank's block list, for the feature builder
+        pass
+    sp = Sub()
+    sp.gt, sp.gs = sub_gt, sub_gs
+    sp.sizes = part.sizes
+    sp.extents, sp.centres = part.extents, part.centres
+    feats = features(sp, K_WAVE, TOL)
+    x_dev = torch.from_numpy(((feats - pred.mean) / pred.std).astype(np.float32)).cuda()
+    p_dev = torch.from_numpy(pred.params).cuda()
+    y_dev = torch.empty(nb, dtype=torch.float32, device="cuda")
+    Dmin = np.minimum(part.sizes()[sub_gt], part.sizes()[sub_gs])
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+
+    def predict_r0():
+        _lib.check(L.pskel_mlp_forward(vp(p_dev), vp(x_dev), nb, vp(y_dev), None))
+        y = y_dev.cpu().numpy().astype(np.float64)
+        return np.clip(np.ceil(pred.margin * np.exp2(y)), 1, Dmin).astype(np.int32)
+
+    def step():
+        r0 = predict_r0()
+        return eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        times = []
+        launches0 = L.pskel_kernel_launches()
+        for _ in range(steps):
+            flush.zero_()
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            out = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        launches = L.pskel_kernel_launches() - launches0
+        t = torch.tensor([float(np.mean(times))], device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item()), out, launches // max(steps, 1), times
+
+    with ClockSampler(dev) as clk:
+        ms, st, launches, times = timed(step, args.steps, args.warmup)
+    clocks = clk.summary()
+    tinfo = eng.timing()
+    # plain FP64 GPU pseudoskeleton (the drop-in baseline), same blocks and estimator
+    plain = lambda: eng.compress(TOL, **PLAIN)
+    plain_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
+    t_plain = eng.timing()
+    # per-phase timing of the product without the graph (roofline of the fill)
+    r0 = predict_r0()
+    st_np = eng.compress(TOL, r0=r0, use_graph=False, **PRODUCT)
+    tph = eng.timing()
+    fp32_peak = ctypes.c_double()
+    fp64_peak = ctypes.c_double()
+    _lib.check(L.pskel_fma_peak(ctypes.byref(fp32_peak), ctypes.byref(fp64_peak)))
+    achieved = tph["point_pairs"] * FLOPS_PER_PAIR / (tph["fill"] * 1e-3) / 1e12
+    # accuracy of the timed product and of the plain baseline against dense FP64 fills
+    st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
+    err = eng.true_errors()
+    err_plain = None
+    if args.plain_errors:
+        st_plain = eng.compress(TOL, **PLAIN)
+        err_plain = eng.true_errors()
+    # e2e: the public call path from host buffers: mesh + groups + features up, stats down
+    e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush)
+    if args.save and rank == 0:
+        np.savez(args.save, m=st["m"], n=st["n"], r=st["r"], rounds=st["rounds"], est=st["est"],
+                 err=err, r_plain=st_plain["r"], rounds_plain=st_plain["rounds"],
+                 err_plain=err_plain if err_plain is not None else np.zeros(0))
+    out = dict(
+        metric=METRIC, value=round(ms, 3), unit="ms", n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=False,
+        scaling="strong" if world > 1 else "weak", vs_baseline=None,
+        dtype="c64 fill (FP64 geometry) + FP64 Jacobi pinv",
+        data="synthetic: " + WORKLOADS[args.workload]["desc"] + "; no dataset",
+        config=dict(workload=args.workload, rwg=m.N, groups=part.n_groups,
+                    blocks=int(part.n_blocks), blocks_this_rank=int(nb), tol=TOL,
+                    quadrature="7-point per triangle", precision=PRODUCT["precision"],
+                    pinv_tau_relative=PRODUCT["tau"], estimator="16 extra rows + 16 extra columns, safety 2",
+                    l2="512 MB write before every timed step (inputs also exceed L2)"),
+        plain_ms=round(plain_ms, 3), speedup_vs_plain=round(plain_ms / ms, 3),
+        step_times_ms=[round(t, 3) for t in times],
+        phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},
+        product=dict(r_mean=float(st["r"].mean()), rounds_mean=float(st["rounds"].mean()),
+                     first_round_accepted=float(np.mean(st["rounds"] == 1)),
+                     err_max=float(err.max()), err_median=float(np.median(err)),
+                     blocks_over_tol=int((err > TOL).sum()),
+                     fill_point_pairs=float(tph["point_pairs"])),
+        plain=dict(r_mean=float(st_plain["r"].mean()), rounds_mean=float(st_plain["rounds"].mean()),
+                   fill_point_pairs=float(t_plain["point_pairs"]),
+                   err_max=None if err_plain is None else float(err_plain.max()),
+                   blocks_over_tol=None if err_plain is None else int((err_plain > TOL).sum())),
+        roofline=dict(bound="alu", kernel="fill_kernel<float,7> (c64, FP64 geometry)",
+                      achieved=round(achieved, 3), peak=round(fp32_peak.value, 3), unit="TFLOP/s",
+                      frac=round(achieved / fp32_peak.value, 4), traffic=None,
+                      peak_source="measured FP32 FMA microbenchmark on this GPU (pskel_fma_peak); "
+                                  f"FP64 FMA {fp64_peak.value:.2f} TFLOP/s",
+                      flops="32 flops per point-pair evaluation x point pairs / fill device time",
+                      fill_ms=round(tph["fill"], 3), fill_launches=int(tph["fill_launches"])),
+        e2e=dict(value=round(e2e_ms, 3), unit="ms", h2d_bytes_per_step=int(h2d),
+                 d2h_bytes_per_step=int(d2h)),
+        clocks=clocks, gpu_launches=int(launches),
+    )
+    eng.close()
+    return out
+
+
+def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush):
+    """Host data in, compressed blocks resident on the GPU, per-block stats out."""
+    import torch
+
+    from pskel import _lib
+    from pskel.engine import Engine
+    from pskel.predictor import features
+
+    class Sub:
+        pass
+    sp = Sub()
+    sp.gt, sp.gs, sp.sizes, sp.extents, sp.centres = sub_gt, sub_gs, part.sizes, part.extents, part.centres
+    a = m.as_f64()
+    eng = Engine(dev)
+    L = _lib.lib()
+    feats_host = features(sp, K_WAVE, TOL)
+    x_pin = torch.from_numpy(((feats_host - pred.mean) / pred.std).astype(np.float32)).pin_memory()
+    p_dev = torch.from_numpy(pred.params).cuda()
+    Dmin = np.minimum(part.sizes()[sub_gt], part.sizes()[sub_gs])
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    h2d = sum(a[k].nbytes for k in ("vertex", "topol", "edges", "ln", "cent"))
+    h2d += part.group_ptr.nbytes + part.group_ids.nbytes + sub_gt.nbytes + sub_gs.nbytes
+    h2d += x_pin.numel() * 4 + p_dev.numel() * 4
+    d2h = len(sub_gt) * 40 + len(sub_gt) * 4
+
+    def one():
+        eng.upload_mesh(m, K_WAVE, ETA, q=7)
+        eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt, gs=sub_gs)
+        x = x_pin.cuda(non_blocking=True)
+        y = torch.empty(len(sub_gt), dtype=torch.float32, device="cuda")
+        _lib.check(L.pskel_mlp_forward(vp(p_dev), vp(x), len(sub_gt), vp(y), None))
+        r0 = np.clip(np.ceil(pred.margin * np.exp2(y.cpu().numpy().astype(np.float64))), 1, Dmin)
+        return eng.compress(TOL, r0=r0.astype(np.int32), use_graph=False, **PRODUCT)
+
+    for _ in range(max(1, args.warmup)):
+        one()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(max(1, min(args.steps, 3))):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        one()
+        e1.record()
+        torch.cuda.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    t = torch.tensor([float(np.mean(ts))], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    eng.close()
+    return float(t.item()), h2d, d2h
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", choices=tuple(WORKLOADS), default="sphere30k")
+    ap.add_argument("--save", default=None, help="write per-block stats (npz)")
+    ap.add_argument("--plain-errors", action="store_true", help="also check the plain run's errors")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        times, last = [], None
+        for i in range(max(1, args.warmup) + max(1, args.steps)):
+            cb = cpu_baseline(args.workload, n_sample=48, seed=i)
+            if i >= max(1, args.warmup):
+                times.append(cb["value"])
+            last = cb
+        v = float(np.median(times))
+        line = dict(impl="reference", metric=METRIC, value=round(v, 1), unit="ms", n_gpus=world,
+                    steps=args.steps, warmup=args.warmup, ms_per_step=round(v, 1),
+                    higher_is_better=False, scaling="weak", vs_baseline=None, dtype="c128",
+                    data="synthetic: " + WORKLOADS[args.workload]["desc"],
+                    config=dict(workload=args.workload, tol=TOL, quadrature="7-point per triangle"),
+                    cpu_baseline=dict(last, value=round(v, 1)),
+                    e2e=dict(value=round(v, 1), unit="ms", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    out = run_ours(args, rank, world, local)
+    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args.workload)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -31,14 +31,15 @@ static constexpr int kMaxExtra = 32;
 struct BlockWork {
     const int *rows_g;  // global RWG ids of the test group (m)
     const int *cols_g;  // global RWG ids of the source group (n)
-    int m, n, r, pe;
+    int m, n, r, pe, pc;
     int block_id, round;
-    int *I, *J, *Ix;    // local indices (sorted)
+    int *I, *J, *Ix, *Jx;  // local indices (sorted)
     int *Ig;            // global ids of rows I then Ix (r + pe)
-    int *Jg;            // global ids of columns J (r)
-    void *C;            // m x r
-    void *Rx;           // (r + pe) x n, ld = r + pe
+    int *Jg;            // global ids of columns J then Jx (r + pc)
+    void *C;            // m x (r + pc): C = Z(:, J), then the extra columns Z(:, Jx)
+    void *Rx;           // (r + pe) x n, ld = r + pe: R = Z(I, :), then the extra rows Z(Ix, :)
     double2 *AV, *V, *U;
+    double2 *T;         // estimator scratch: C(Ix, :) U (pe x r), then U R(:, Jx) (r x pc)
     double *sigma;
     int *perm, *rank;
     double *est;
@@ -103,52 +104,61 @@ __device__ void draw_bitmap(uint32_t *words, uint32_t *bits, int *scan, int r, i
     __syncthreads();
 }
 
+// p extra draws out of the D - r values not set in bits_set (D bits valid); the k-th unset
+// value is taken for draw k, results sorted. All threads of the CTA must call it.
+__device__ void draw_extra(uint32_t *words, const uint32_t *bits_set, uint32_t *bitsX, int *scan,
+                           int *pick, int p, int D, int r, uint32_t block, uint32_t round,
+                           uint32_t stream, uint64_t seed, int *out) {
+    if (p <= 0) return;
+    draw_bitmap(words, bitsX, scan, p, D - r, block, round, stream, seed, pick);
+    const int nw = (D + 31) / 32;
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int q = 0; q < nw; ++q) {
+            const uint32_t valid = (q == nw - 1 && (D & 31)) ? ((1u << (D & 31)) - 1u) : 0xffffffffu;
+            scan[q] = acc;
+            acc += __popc(~bits_set[q] & valid);
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < p; e += blockDim.x) {
+        const int kk = pick[e];
+        int q = 0;
+        while (q + 1 < nw && scan[q + 1] <= kk) ++q;
+        const uint32_t valid = (q == nw - 1 && (D & 31)) ? ((1u << (D & 31)) - 1u) : 0xffffffffu;
+        uint32_t z = ~bits_set[q] & valid;
+        int left = kk - scan[q];
+        while (left-- > 0) z &= z - 1;
+        out[e] = q * 32 + __ffs(z) - 1;
+    }
+    __syncthreads();
+}
+
 __global__ void __launch_bounds__(128) sample_kernel(const BlockWork *__restrict__ works,
                                                      uint64_t seed) {
     extern __shared__ __align__(16) uint32_t sh[];
     uint32_t *words = sh;                       // kMaxGroup
-    uint32_t *bitsI = words + kMaxGroup;        // kMaxGroup/32
-    uint32_t *bitsX = bitsI + kMaxGroup / 32;   // kMaxGroup/32
-    int *scan = reinterpret_cast<int *>(bitsX + kMaxGroup / 32);  // kMaxGroup/32
+    uint32_t *bitsI = words + kMaxGroup;        // kMaxGroup/32 each
+    uint32_t *bitsJ = bitsI + kMaxGroup / 32;
+    uint32_t *bitsX = bitsJ + kMaxGroup / 32;
+    int *scan = reinterpret_cast<int *>(bitsX + kMaxGroup / 32);
     int *pick = scan + kMaxGroup / 32;          // kMaxExtra
     const BlockWork w = works[blockIdx.x];
-    // columns first (uses bitsX as scratch), then rows (kept in bitsI)
-    draw_bitmap(words, bitsX, scan, w.r, w.n, w.block_id, w.round, 1u, seed, w.J);
+    // streams: 0 rows I, 1 columns J, 2 extra rows, 3 extra columns
+    draw_bitmap(words, bitsJ, scan, w.r, w.n, w.block_id, w.round, 1u, seed, w.J);
     draw_bitmap(words, bitsI, scan, w.r, w.m, w.block_id, w.round, 0u, seed, w.I);
-    if (w.pe > 0) {
-        // pe draws out of the m - r unsampled rows; the k-th unsampled row is taken for draw k
-        draw_bitmap(words, bitsX, scan, w.pe, w.m - w.r, w.block_id, w.round, 2u, seed, pick);
-        const int nw = (w.m + 31) / 32;
-        if (threadIdx.x == 0) {
-            int acc = 0;
-            for (int q = 0; q < nw; ++q) {
-                const uint32_t valid = (q == nw - 1 && (w.m & 31)) ? ((1u << (w.m & 31)) - 1u) : 0xffffffffu;
-                scan[q] = acc;
-                acc += __popc(~bitsI[q] & valid);
-            }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < w.pe; e += blockDim.x) {
-            const int kk = pick[e];
-            int q = 0;
-            while (q + 1 < nw && scan[q + 1] <= kk) ++q;
-            const uint32_t valid = (q == nw - 1 && (w.m & 31)) ? ((1u << (w.m & 31)) - 1u) : 0xffffffffu;
-            uint32_t z = ~bitsI[q] & valid;
-            int left = kk - scan[q];
-            while (left-- > 0) z &= z - 1;
-            w.Ix[e] = q * 32 + __ffs(z) - 1;
-        }
-        __syncthreads();
-    }
+    draw_extra(words, bitsI, bitsX, scan, pick, w.pe, w.m, w.r, w.block_id, w.round, 2u, seed, w.Ix);
+    draw_extra(words, bitsJ, bitsX, scan, pick, w.pc, w.n, w.r, w.block_id, w.round, 3u, seed, w.Jx);
     for (int i = threadIdx.x; i < w.r; i += blockDim.x) {
         w.Ig[i] = w.rows_g[w.I[i]];
         w.Jg[i] = w.cols_g[w.J[i]];
     }
     for (int e = threadIdx.x; e < w.pe; e += blockDim.x) w.Ig[w.r + e] = w.rows_g[w.Ix[e]];
+    for (int e = threadIdx.x; e < w.pc; e += blockDim.x) w.Jg[w.r + e] = w.cols_g[w.Jx[e]];
 }
 
 static size_t sample_smem() {
-    return sizeof(uint32_t) * (kMaxGroup + 3 * (kMaxGroup / 32)) + sizeof(int) * kMaxExtra;
+    return sizeof(uint32_t) * (kMaxGroup + 4 * (kMaxGroup / 32)) + sizeof(int) * kMaxExtra;
 }
 
 // ------------------------------------------------------------------ core gather
@@ -166,62 +176,92 @@ __global__ void __launch_bounds__(256) gather_core_kernel(const BlockWork *__res
     }
 }
 
-// ------------------------------------------------------------------ extra-row estimate
+// ------------------------------------------------------------------ randomized estimate
+// est = max( ||Z(Ix,:) - C(Ix,:) U R||_F / ||Z(Ix,:)||_F ,  ||Z(:,Jx) - C U R(:,Jx)||_F / ||Z(:,Jx)||_F )
+// on pe extra rows and pc extra columns that were not sampled (0 if neither exists).
 template <typename S>
 __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restrict__ works) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double2 *T = reinterpret_cast<double2 *>(smem_raw);  // pe x r
-    __shared__ double s_num[256], s_den[256];
+    __shared__ double s_red[4][256];
     const BlockWork w = works[blockIdx.x];
-    const int r = w.r, pe = w.pe, n = w.n, m = w.m, ldr = w.r + w.pe;
+    const int r = w.r, pe = w.pe, pc = w.pc, n = w.n, m = w.m, ldr = w.r + w.pe;
     const S *C = reinterpret_cast<const S *>(w.C);
     const S *Rx = reinterpret_cast<const S *>(w.Rx);
-    if (pe == 0) {
-        if (threadIdx.x == 0) *w.est = 0.0;
-        return;
-    }
-    // T = C(Ix, :) U
-    for (int idx = threadIdx.x; idx < pe * r; idx += blockDim.x) {
-        const int e = idx % pe, k = idx / pe;
-        const int row = w.Ix[e];
+    double2 *Tr = w.T;             // pe x r
+    double2 *Sc = w.T + pe * r;    // r x pc
+    // Tr = C(Ix, :) U ; Sc = U R(:, Jx)
+    for (int idx = threadIdx.x; idx < pe * r + r * pc; idx += blockDim.x) {
         double sx = 0, sy = 0;
-        for (int l = 0; l < r; ++l) {
-            const double2 c = promote(C[row + (size_t)l * m]);
-            const double2 u = w.U[l + (size_t)k * r];
-            sx = fma(c.x, u.x, fma(-c.y, u.y, sx));
-            sy = fma(c.x, u.y, fma(c.y, u.x, sy));
+        if (idx < pe * r) {
+            const int e = idx % pe, k = idx / pe;
+            const int row = w.Ix[e];
+            for (int l = 0; l < r; ++l) {
+                const double2 c = promote(C[row + (size_t)l * m]);
+                const double2 u = w.U[l + (size_t)k * r];
+                sx = fma(c.x, u.x, fma(-c.y, u.y, sx));
+                sy = fma(c.x, u.y, fma(c.y, u.x, sy));
+            }
+            Tr[idx] = make_double2(sx, sy);
+        } else {
+            const int q = idx - pe * r;
+            const int k = q % r, cc = q / r;
+            const int col = w.Jx[cc];
+            for (int l = 0; l < r; ++l) {
+                const double2 u = w.U[k + (size_t)l * r];
+                const double2 rv = promote(Rx[l + (size_t)col * ldr]);
+                sx = fma(u.x, rv.x, fma(-u.y, rv.y, sx));
+                sy = fma(u.x, rv.y, fma(u.y, rv.x, sy));
+            }
+            Sc[q] = make_double2(sx, sy);
         }
-        T[e + k * pe] = make_double2(sx, sy);
     }
     __syncthreads();
-    double num = 0, den = 0;
-    for (int j = threadIdx.x; j < n; j += blockDim.x) {
+    double nr_ = 0, dr_ = 0, nc_ = 0, dc_ = 0;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) {  // extra rows, column j
         const S *col = Rx + (size_t)j * ldr;
         for (int e = 0; e < pe; ++e) {
             double zx = 0, zy = 0;
             for (int k = 0; k < r; ++k) {
-                const double2 t = T[e + k * pe];
+                const double2 t = Tr[e + k * pe];
                 const double2 rv = promote(col[k]);
                 zx = fma(t.x, rv.x, fma(-t.y, rv.y, zx));
                 zy = fma(t.x, rv.y, fma(t.y, rv.x, zy));
             }
             const double2 x = promote(col[r + e]);
             const double dx = x.x - zx, dy = x.y - zy;
-            num = fma(dx, dx, fma(dy, dy, num));
-            den = fma(x.x, x.x, fma(x.y, x.y, den));
+            nr_ = fma(dx, dx, fma(dy, dy, nr_));
+            dr_ = fma(x.x, x.x, fma(x.y, x.y, dr_));
         }
     }
-    s_num[threadIdx.x] = num;
-    s_den[threadIdx.x] = den;
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {  // extra columns, row i
+        for (int cc = 0; cc < pc; ++cc) {
+            double zx = 0, zy = 0;
+            for (int k = 0; k < r; ++k) {
+                const double2 c = promote(C[i + (size_t)k * m]);
+                const double2 t = Sc[k + cc * r];
+                zx = fma(c.x, t.x, fma(-c.y, t.y, zx));
+                zy = fma(c.x, t.y, fma(c.y, t.x, zy));
+            }
+            const double2 x = promote(C[i + (size_t)(r + cc) * m]);
+            const double dx = x.x - zx, dy = x.y - zy;
+            nc_ = fma(dx, dx, fma(dy, dy, nc_));
+            dc_ = fma(x.x, x.x, fma(x.y, x.y, dc_));
+        }
+    }
+    s_red[0][threadIdx.x] = nr_;
+    s_red[1][threadIdx.x] = dr_;
+    s_red[2][threadIdx.x] = nc_;
+    s_red[3][threadIdx.x] = dc_;
     __syncthreads();
     for (int o = 128; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) {
-            s_num[threadIdx.x] += s_num[threadIdx.x + o];
-            s_den[threadIdx.x] += s_den[threadIdx.x + o];
-        }
+        if ((int)threadIdx.x < o)
+            for (int q = 0; q < 4; ++q) s_red[q][threadIdx.x] += s_red[q][threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) *w.est = s_den[0] > 0 ? sqrt(s_num[0] / s_den[0]) : 0.0;
+    if (threadIdx.x == 0) {
+        const double er = s_red[1][0] > 0 ? sqrt(s_red[0][0] / s_red[1][0]) : 0.0;
+        const double ec = s_red[3][0] > 0 ? sqrt(s_red[2][0] / s_red[3][0]) : 0.0;
+        *w.est = fmax(er, ec);
+    }
 }
 
 // per-block outcome gather: est, rank, svd status into one compact array for a single D2H
@@ -267,7 +307,7 @@ __global__ void promote_kernel(const S *in, double2 *out, long long n) {
 using namespace pskel;
 
 struct BlockResult {
-    int m = 0, n = 0, r = 0, pe = 0, round = -1, rank = 0, status = 0;
+    int m = 0, n = 0, r = 0, pe = 0, pc = 0, round = -1, rank = 0, status = 0;
     double est = 0;
     int arena = -1;
     size_t offC = 0, offRx = 0, offU = 0, offI = 0, offJ = 0;
@@ -297,9 +337,10 @@ struct pskel_ctx {
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;
-    double timing[6] = {0, 0, 0, 0, 0, 0};
+    double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;
+    long long graph_kernels = 0;  // kernel nodes of the captured graph
     std::vector<int> graph_key;
     std::vector<int> last_key;  // round-0 key of the previous call (capture on a repeat)
     DevBuf tmp, tmp2, tmp3;
@@ -320,7 +361,7 @@ size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct RoundPlan {
     std::vector<int> blocks;     // block ids of this round
-    std::vector<int> r, pe;
+    std::vector<int> r, pe, pc;
     int round = 0;
     // device table views (inside arena.tables)
     BlockWork *d_works = nullptr;
@@ -333,7 +374,6 @@ struct RoundPlan {
     size_t max_res_smem = 0;
     PinvJob *d_pinv = nullptr;
     int pinv_tiles = 0;
-    size_t est_smem = 0;
     int nb = 0;
 };
 
@@ -351,20 +391,21 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         const int b = p.blocks[i];
         const size_t m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
         const size_t n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
-        const size_t r = p.r[i], pe = p.pe[i];
+        const size_t r = p.r[i], pe = p.pe[i], pc = p.pc[i];
         size_t s = 0;
-        s += al16(m * r * es);              // C
+        s += al16(m * (r + pc) * es);       // C (+ extra columns)
         s += al16((r + pe) * n * es);       // Rx
         s += al16(r * r * sizeof(double2)); // U
         s += al16(sizeof(int) * r) * 2;     // I, J
         s += al16(sizeof(int) * (pe + 1));  // Ix
+        s += al16(sizeof(int) * (pc + 1));  // Jx
         s += al16(sizeof(int) * (r + pe));  // Ig
-        s += al16(sizeof(int) * r);         // Jg
+        s += al16(sizeof(int) * (r + pc));  // Jg
         s += al16(sizeof(double) * r);      // sigma
         s += al16(sizeof(int) * r);         // perm
         s += 16 + 16;                       // rank, est
         off[i + 1] = off[i] + ((s + 255) & ~size_t(255));
-        scratch_total += 2 * al16(r * r * sizeof(double2));
+        scratch_total += 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
     }
     PSKEL_TRY(ar.keep.reserve(off[nb] + 256));
     PSKEL_TRY(ar.work.reserve(scratch_total + 256));
@@ -377,7 +418,6 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     char *kb = ar.keep.as<char>();
     char *sb = ar.work.as<char>();
     size_t soff = 0;
-    size_t max_est_smem = 0;
     int max_pinv_tiles = 0;
     for (int i = 0; i < nb; ++i) {
         const int b = p.blocks[i];
@@ -389,19 +429,21 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         w.n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
         w.r = p.r[i];
         w.pe = p.pe[i];
+        w.pc = p.pc[i];
         w.block_id = b;
         w.round = p.round;
         char *q = kb + off[i];
         auto take = [&](size_t bytes) { char *x = q; q += al16(bytes); return x; };
-        const size_t m = w.m, n = w.n, r = w.r, pe = w.pe;
-        w.C = take(m * r * es);
+        const size_t m = w.m, n = w.n, r = w.r, pe = w.pe, pc = w.pc;
+        w.C = take(m * (r + pc) * es);
         w.Rx = take((r + pe) * n * es);
         w.U = reinterpret_cast<double2 *>(take(r * r * sizeof(double2)));
         w.I = reinterpret_cast<int *>(take(sizeof(int) * r));
         w.J = reinterpret_cast<int *>(take(sizeof(int) * r));
         w.Ix = reinterpret_cast<int *>(take(sizeof(int) * (pe + 1)));
+        w.Jx = reinterpret_cast<int *>(take(sizeof(int) * (pc + 1)));
         w.Ig = reinterpret_cast<int *>(take(sizeof(int) * (r + pe)));
-        w.Jg = reinterpret_cast<int *>(take(sizeof(int) * r));
+        w.Jg = reinterpret_cast<int *>(take(sizeof(int) * (r + pc)));
         w.sigma = reinterpret_cast<double *>(take(sizeof(double) * r));
         w.perm = reinterpret_cast<int *>(take(sizeof(int) * r));
         w.rank = reinterpret_cast<int *>(take(16));
@@ -410,16 +452,18 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         soff += al16(r * r * sizeof(double2));
         w.V = reinterpret_cast<double2 *>(sb + soff);
         soff += al16(r * r * sizeof(double2));
-        fills.push_back(FillJob{w.rows_g, w.Jg, w.C, w.m, w.r, w.m, 0});
+        w.T = reinterpret_cast<double2 *>(sb + soff);
+        soff += al16((pe + pc) * r * sizeof(double2));
+        fills.push_back(FillJob{w.rows_g, w.Jg, w.C, w.m, w.r + w.pc, w.m, 0});
         fills.push_back(FillJob{w.Ig, w.cols_g, w.Rx, w.r + w.pe, w.n, w.r + w.pe, 0});
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, o.tau, o.tau_relative};
-        max_est_smem = std::max(max_est_smem, sizeof(double2) * pe * r);
         max_pinv_tiles = std::max(max_pinv_tiles, ((w.r + 31) / 32) * ((w.r + 31) / 32));
         res.m = w.m;
         res.n = w.n;
         res.r = w.r;
         res.pe = w.pe;
+        res.pc = w.pc;
         res.round = p.round;
         res.arena = p.round;
         res.offC = (char *)w.C - kb;
@@ -466,11 +510,6 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.d_svd_idx = reinterpret_cast<int *>(d + o_idx);
     p.d_pinv = reinterpret_cast<PinvJob *>(d + o_pinv);
     p.pinv_tiles = max_pinv_tiles;
-    p.est_smem = max_est_smem;
-    if (max_est_smem > 200 * 1024) {
-        set_error(PSKEL_ERR_ARG, "extra_rows x r too large for the estimator (%zu bytes)", max_est_smem);
-        return PSKEL_ERR_ARG;
-    }
     return PSKEL_OK;
 }
 
@@ -479,7 +518,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     cudaStream_t s = c->stream;
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[0], s));
     sample_kernel<<<p.nb, 128, sample_smem(), s>>>(p.d_works, o.seed);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[1], s));
     FillParams fp;
     fp.k = c->em.k;
@@ -496,18 +535,18 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
         gather_core_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_works);
     else
         gather_core_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.n_res, p.n_blk, p.max_res_smem, 60, s));
     PSKEL_TRY(batched_pinv(p.d_pinv, p.nb, p.pinv_tiles, s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));
     if (o.precision == PSKEL_C64)
-        estimate_kernel<float2><<<p.nb, 256, p.est_smem, s>>>(p.d_works);
+        estimate_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_works);
     else
-        estimate_kernel<double2><<<p.nb, 256, p.est_smem, s>>>(p.d_works);
-    PSKEL_CUDA(cudaGetLastError());
+        estimate_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
+    PSKEL_LAUNCHED(1);
     collect_kernel<<<(p.nb + 255) / 256, 256, 0, s>>>(p.d_works, p.d_svd, p.nb,
                                                      c->arenas[p.round].outs.as<RoundOut>());
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[4], s));
     return PSKEL_OK;
 }
@@ -517,10 +556,6 @@ int set_kernel_attrs() {
     if (done) return PSKEL_OK;
     PSKEL_CUDA(cudaFuncSetAttribute(sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)sample_smem()));
-    PSKEL_CUDA(cudaFuncSetAttribute(estimate_kernel<float2>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    PSKEL_CUDA(cudaFuncSetAttribute(estimate_kernel<double2>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     done = true;
     return PSKEL_OK;
 }
@@ -564,8 +599,8 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
         if (e) cudaEventDestroy(e);
     c->mesh.vertex.release(); c->mesh.topol.release(); c->mesh.edges.release();
     c->mesh.ln.release(); c->mesh.cent.release();
-    c->mesh.rec1.f64.release(); c->mesh.rec1.f32.release();
-    c->mesh.rec7.f64.release(); c->mesh.rec7.f32.release();
+    c->mesh.rec1.f64.release();
+    c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
     c->tmp.release(); c->tmp2.release(); c->tmp3.release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
@@ -693,23 +728,26 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     }
     const pskel_opts_t o = *opts;
     if (!(o.tol > 0) || o.tau < 0 || (o.precision != PSKEL_C128 && o.precision != PSKEL_C64) ||
-        o.extra_rows < 0 || o.extra_rows > kMaxExtra || o.max_rounds < 1 ||
+        o.extra_rows < 0 || o.extra_rows > kMaxExtra || o.extra_cols < 0 ||
+        o.extra_cols > kMaxExtra || o.max_rounds < 1 ||
         (o.start == PSKEL_START_GIVEN && !r0)) {
         set_error(PSKEL_ERR_ARG, "compress: bad options");
         return PSKEL_ERR_ARG;
     }
     PSKEL_TRY(set_kernel_attrs());
+    const double safety = o.est_safety >= 1.0 ? o.est_safety : 1.0;
     c->precision = o.precision;
     for (double &t : c->timing) t = 0;
     const int nb = c->n_blocks;
     // first sample counts
-    std::vector<int> r_cur(nb), Dmin(nb), mrows(nb);
+    std::vector<int> r_cur(nb), Dmin(nb), mrows(nb), ncols(nb);
     for (int b = 0; b < nb; ++b) {
         const int m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
         const int n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
         const int D = std::min(m, n);
         Dmin[b] = D;
         mrows[b] = m;
+        ncols[b] = n;
         int r;
         if (o.start == PSKEL_START_GIVEN) r = r0[b] + o.oversample;
         else r = D < 10 ? 1 : D / 10;
@@ -730,10 +768,24 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         p.blocks = active;
         p.r.resize(active.size());
         p.pe.resize(active.size());
+        p.pc.resize(active.size());
         for (size_t i = 0; i < active.size(); ++i) {
             const int b = active[i];
             p.r[i] = r_cur[b];
             p.pe[i] = std::min(o.extra_rows, mrows[b] - r_cur[b]);
+            p.pc[i] = std::min(o.extra_cols, ncols[b] - r_cur[b]);
+        }
+        {
+            double ent = 0;
+            for (size_t i = 0; i < active.size(); ++i) {
+                const int b = active[i];
+                ent += (double)mrows[b] * (p.r[i] + p.pc[i]) + (double)(p.r[i] + p.pe[i]) * ncols[b];
+            }
+            const double q2 = 4.0 * c->em.q_test * c->em.q_src;
+            c->timing[6] += ent;
+            c->timing[7] += ent * q2;
+            c->timing[8] += 1;
+            c->timing[9] += 1;
         }
         // graph of the first round: key = the sample counts and options that shape it
         bool try_graph = o.use_graph && round == 0;
@@ -743,6 +795,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back(o.precision);
             key.push_back((int)(o.seed & 0x7fffffff));
             key.push_back(o.extra_rows);
+            key.push_back(o.extra_cols);
             key.push_back((int)std::lround(std::log10(std::max(o.tau, 1e-300)) * 1000));
             key.push_back(o.tau_relative);
             // capture only when the same first round ran eagerly before (warm, attributes set)
@@ -755,6 +808,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             for (size_t i = 0; i < active.size(); ++i) c->results[active[i]] = c->graph_results[active[i]];
             PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
             PSKEL_CUDA(cudaGraphLaunch(c->graph, c->stream));
+            count_launch(c->graph_kernels);
             PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
         } else {
             if (round == 0 && c->graph) {
@@ -772,7 +826,10 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
                 PSKEL_CUDA(cudaStreamSynchronize(c->stream));
                 cudaGraph_t g;
                 PSKEL_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                const long long before = launches_so_far();
                 int st = launch_round(c, p, o, false);
+                c->graph_kernels = launches_so_far() - before;
+                count_launch(-c->graph_kernels);  // captured, not run
                 cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
                 if (st != PSKEL_OK) return st;
                 if (ce != cudaSuccess) {
@@ -785,6 +842,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
                 c->graph_results = c->results;
                 PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
                 PSKEL_CUDA(cudaGraphLaunch(c->graph, c->stream));
+                count_launch(c->graph_kernels);
                 PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
             } else {
                 PSKEL_TRY(launch_round(c, p, o, true));
@@ -815,7 +873,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             res.rank = hout[i].rank;
             res.status = hout[i].status;
             rounds_used[b] = round + 1;
-            const bool ok = hout[i].status == PSKEL_OK && hout[i].est <= o.tol;
+            const bool ok = hout[i].status == PSKEL_OK && hout[i].est <= o.tol / safety;
             if (ok || r_cur[b] >= Dmin[b] || round + 1 >= o.max_rounds) continue;
             r_cur[b] = std::min(2 * r_cur[b], Dmin[b]);
             next.push_back(b);
@@ -856,13 +914,13 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     return PSKEL_OK;
 }
 
-extern "C" int pskel_last_timing(pskel_ctx *c, double *ms6) {
+extern "C" int pskel_last_timing(pskel_ctx *c, double *out, int n) {
     PSKEL_TRY(ctx_ok(c));
-    if (!ms6) {
+    if (!out || n < 0) {
         set_error(PSKEL_ERR_ARG, "null output");
         return PSKEL_ERR_ARG;
     }
-    for (int i = 0; i < 6; ++i) ms6[i] = c->timing[i];
+    for (int i = 0; i < n && i < 10; ++i) out[i] = c->timing[i];
     return PSKEL_OK;
 }
 
@@ -968,6 +1026,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
                     reinterpret_cast<const float2 *>(base + res.offC), Cc, nC);
                 promote_kernel<float2><<<(unsigned)((nR + 255) / 256), 256, 0, c->stream>>>(
                     reinterpret_cast<const float2 *>(base + res.offRx), Rc, nR);
+                count_launch(2);
                 Cd = Cc;
                 Rd = Rc;
             } else {
@@ -1010,11 +1069,11 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         fp.split = 1;
         PSKEL_TRY(launch_fill(c->mesh, fp, d_f, d_p, nbb, prefix.back(), c->flags.as<int>(), c->stream));
         block_norm_kernel<<<nbb, 256, 0, c->stream>>>(d_m, d_s, d_nz);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
         PSKEL_TRY(launch_zgemm(g1, c->stream, c->tmp3));
         PSKEL_TRY(launch_zgemm(g2, c->stream, c->tmp3));
         block_norm_kernel<<<nbb, 256, 0, c->stream>>>(d_m, d_s, d_ne);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
         std::vector<double> nz(nbb), ne(nbb);
         PSKEL_CUDA(cudaMemcpyAsync(nz.data(), d_nz, sizeof(double) * nbb, cudaMemcpyDeviceToHost, c->stream));
         PSKEL_CUDA(cudaMemcpyAsync(ne.data(), d_ne, sizeof(double) * nbb, cudaMemcpyDeviceToHost, c->stream));
@@ -1022,5 +1081,60 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         for (int i = 0; i < nbb; ++i) err[b0 + i] = nz[i] > 0 ? ne[i] / nz[i] : 0.0;
         b0 = b1;
     }
+    return PSKEL_OK;
+}
+
+extern "C" long long pskel_kernel_launches(void) { return launches_so_far(); }
+
+// ------------------------------------------------------------------ FMA peak microbenchmark
+namespace pskel {
+template <typename T>
+__global__ void __launch_bounds__(256) fma_chain_kernel(T *out, int iters, T a, T b) {
+    T x0 = (T)threadIdx.x, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5,
+      x6 = x0 + 6, x7 = x0 + 7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+}  // namespace pskel
+
+template <typename T>
+static int fma_peak_t(double *tflops) {
+    const int blocks = sm_count() * 8, threads = 256;
+    T *out = nullptr;
+    PSKEL_CUDA(cudaMalloc(&out, sizeof(T) * blocks * threads));
+    cudaEvent_t e0, e1;
+    PSKEL_CUDA(cudaEventCreate(&e0));
+    PSKEL_CUDA(cudaEventCreate(&e1));
+    const int iters = sizeof(T) == 8 ? 2048 : 4096;
+    fma_chain_kernel<T><<<blocks, threads>>>(out, 64, (T)0.999, (T)0.001);  // warm-up
+    PSKEL_LAUNCHED(1);
+    PSKEL_CUDA(cudaEventRecord(e0));
+    fma_chain_kernel<T><<<blocks, threads>>>(out, iters, (T)0.999, (T)0.001);
+    PSKEL_LAUNCHED(1);
+    PSKEL_CUDA(cudaEventRecord(e1));
+    PSKEL_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    const double flops = 2.0 * 64.0 * (double)iters * blocks * threads;
+    *tflops = flops / (ms * 1e-3) / 1e12;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_fma_peak(double *fp32_tflops, double *fp64_tflops) {
+    if (!fp32_tflops || !fp64_tflops) {
+        set_error(PSKEL_ERR_ARG, "null output");
+        return PSKEL_ERR_ARG;
+    }
+    PSKEL_TRY(fma_peak_t<float>(fp32_tflops));
+    PSKEL_TRY(fma_peak_t<double>(fp64_tflops));
     return PSKEL_OK;
 }

@@ -301,12 +301,12 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t ma
     }
     if (n_res > 0) {
         svd_resident_kernel<<<n_res, kSvdThreads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
     }
     if (n_blk > 0) {
         svd_blocked_kernel<<<n_blk, kSvdThreads, kSmemBudget, stream>>>(d_jobs, d_idx + n_res,
                                                                         max_sweeps, (int)kSmemBudget);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
     }
     return PSKEL_OK;
 }
@@ -401,7 +401,7 @@ int batched_pinv(const PinvJob *d_jobs, int njobs, int max_tiles, cudaStream_t s
     if (njobs <= 0) return PSKEL_OK;
     dim3 grid(max_tiles, njobs);
     pinv_kernel<<<grid, 256, 0, stream>>>(d_jobs);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 

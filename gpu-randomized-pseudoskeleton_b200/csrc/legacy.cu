@@ -318,7 +318,7 @@ int matvec_err(LegacyCtx &c, const double2 *C, const double2 *U, const double2 *
     std::vector<ZgemmJob> j3{zjob(C, m, ZOP_N, t2, r, ZOP_N, y, m, m, 1, r)};
     PSKEL_TRY(launch_zgemm(j3, c.stream, c.scratch));
     err_kernel<<<1, 256, 0, c.stream>>>(y_old, y, m, d_err);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 
@@ -420,7 +420,7 @@ int device_pinv(LegacyCtx &c, const double2 *d_A, int M, int N, PinvOut &o, int 
     } else {
         const long long tot = (long long)M * N;
         conj_transpose_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(d_A, M, N, AV);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
     }
     std::vector<SvdJob> hj(1);
     hj[0] = SvdJob{AV, V, sigma, perm, m, n, 0, 0};
@@ -439,7 +439,7 @@ int device_pinv(LegacyCtx &c, const double2 *d_A, int M, int N, PinvOut &o, int 
     if (tr) {
         const long long tot = (long long)M * N;
         conj_transpose_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(Pt, M, N, o.P);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
     }
     if (need_sorted && (o.Uleft || o.S || o.Vt)) {
         double smax_thr = o.tau;
@@ -455,7 +455,7 @@ int device_pinv(LegacyCtx &c, const double2 *d_A, int M, int N, PinvOut &o, int 
         const long long tot = std::max<long long>((long long)M * n, (long long)N * N);
         svd_outputs_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c.stream>>>(
             AV, V, sigma, perm, m, n, tr ? 1 : 0, o.Uleft, o.S, o.Vt, M, N, o.vt_scaled, smax_thr);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
     }
     int st[2] = {0, 0};
     PSKEL_CUDA(cudaMemcpyAsync(st, &d_job->status, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
@@ -684,7 +684,7 @@ extern "C" int cuda_filter(double *V, double treshold, int N) {
         PSKEL_TRY(c.out.reserve(sizeof(double) * N));
         PSKEL_CUDA(cudaMemcpyAsync(c.out.ptr, V, sizeof(double) * N, cudaMemcpyHostToDevice, c.stream));
         filter_kernel<<<(N + 255) / 256, 256, 0, c.stream>>>(c.out.as<double>(), N, treshold);
-        PSKEL_CUDA(cudaGetLastError());
+        PSKEL_LAUNCHED(1);
         PSKEL_CUDA(cudaMemcpyAsync(V, c.out.ptr, sizeof(double) * N, cudaMemcpyDeviceToHost, c.stream));
         PSKEL_CUDA(cudaStreamSynchronize(c.stream));
         return PSKEL_OK;

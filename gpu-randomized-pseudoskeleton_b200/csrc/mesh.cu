@@ -1,4 +1,5 @@
 // Mesh upload, per-RWG quadrature records and id conversion.
+#include <atomic>
 #include <cstdarg>
 #include <cmath>
 
@@ -18,6 +19,10 @@ void set_error(int code, const char *fmt, ...) {
     va_end(ap);
 }
 int last_code() { return g_code; }
+
+static std::atomic<long long> g_launches{0};
+void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 int sm_count() {
     static int n = 0;
@@ -67,8 +72,7 @@ __global__ void build_records_kernel(const double *__restrict__ vertex,
                                      const double *__restrict__ edges,
                                      const double *__restrict__ ln,
                                      const double *__restrict__ cent, int ne, int nt, int nv,
-                                     int q, RuleArg rule, double *__restrict__ rec64,
-                                     float *__restrict__ rec32, int *flags) {
+                                     int q, RuleArg rule, double *__restrict__ rec64, int *flags) {
     const int np = 2 * q;
     const int stride = (7 * np) | 1;
     const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -113,15 +117,8 @@ __global__ void build_records_kernel(const double *__restrict__ vertex,
     f[5] = w * 0.5 * l * rho[2];
     f[6] = w * s * l;
     double *r64 = rec64 + (size_t)e * stride;
-    float *r32 = rec32 + (size_t)e * stride;
-    for (int k = 0; k < 7; ++k) {
-        r64[k * np + pp] = f[k];
-        r32[k * np + pp] = (float)f[k];
-    }
-    if (pp == 0) {
-        r64[stride - 1] = 0.0;
-        r32[stride - 1] = 0.0f;
-    }
+    for (int k = 0; k < 7; ++k) r64[k * np + pp] = f[k];
+    if (pp == 0) r64[stride - 1] = 0.0;
 }
 
 int upload_mesh_arrays(DevMesh &mesh, const double *vertex, int nv, const double *topol, int nt,
@@ -162,7 +159,6 @@ int build_records(DevMesh &mesh, int q, cudaStream_t stream, int *d_flag) {
     MeshRecords &rec = mesh.records(q);
     const size_t n = (size_t)mesh.ne * rec_stride(q);
     PSKEL_TRY(rec.f64.reserve(n * sizeof(double)));
-    PSKEL_TRY(rec.f32.reserve(n * sizeof(float)));
     static const Rule7 r7 = make_rule7();
     RuleArg ra;
     for (int i = 0; i < 7; ++i) {
@@ -177,8 +173,8 @@ int build_records(DevMesh &mesh, int q, cudaStream_t stream, int *d_flag) {
     build_records_kernel<<<blocks, threads, 0, stream>>>(
         mesh.vertex.as<double>(), mesh.topol.as<double>(), mesh.edges.as<double>(),
         mesh.ln.as<double>(), mesh.cent.as<double>(), mesh.ne, mesh.nt, mesh.nv, q, ra,
-        rec.f64.as<double>(), rec.f32.as<float>(), d_flag);
-    PSKEL_CUDA(cudaGetLastError());
+        rec.f64.as<double>(), d_flag);
+    PSKEL_LAUNCHED(1);
     rec.q = q;
     return PSKEL_OK;
 }
@@ -214,7 +210,7 @@ int launch_ids_from_double(const double *d_in, int *d_out, int n, int limit, int
                            cudaStream_t stream) {
     if (n <= 0) return PSKEL_OK;
     ids_from_double_kernel<<<(n + 255) / 256, 256, 0, stream>>>(d_in, d_out, n, limit, d_flags);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 
@@ -223,7 +219,7 @@ int launch_ids_from_int64(const int64_t *d_in, int *d_out, int n, int limit, int
     if (n <= 0) return PSKEL_OK;
     ids_from_int64_kernel<<<(n + 255) / 256, 256, 0, stream>>>(
         reinterpret_cast<const long long *>(d_in), d_out, n, limit, d_flags);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 

@@ -65,15 +65,13 @@ struct DevBuf {
 //   u = w_p * (l/2) * rho(r_p),  rho = s (r_p - v_opp),  d = w_p * s * l,  s = +1 (T+), -1 (T-)
 // so that Z_mn = eta/(4 pi) * sum_{p,q} A_pq (sin kR + j cos kR) / R with
 //   A_pq = d_p e_q / k - k u_p . v_q.
-// The record stride is padded to an odd number of words so that 16 different records read by
-// 16 lanes fall in distinct shared-memory banks.
+// The record stride is padded to an odd number of doubles.
 __host__ __device__ constexpr int rec_points(int q) { return 2 * q; }
 __host__ __device__ constexpr int rec_stride(int q) { return (7 * 2 * q) | 1; }
 
 struct MeshRecords {
     int q = 0;
     DevBuf f64;  // ne * rec_stride(q) doubles
-    DevBuf f32;  // ne * rec_stride(q) floats
 };
 
 struct DevMesh {
@@ -172,5 +170,15 @@ int cur_matvec_error(const double2 *C, const double2 *U, const double2 *R, const
 
 // ------------------------------------------------------------------ device properties
 int sm_count();
+
+// Count of kernels launched by the library (reported by pskel_kernel_launches).
+void count_launch(long long n = 1);
+long long launches_so_far();
+// After each kernel launch: count it and surface a launch error.
+#define PSKEL_LAUNCHED(n)                 \
+    do {                                  \
+        ::pskel::count_launch(n);         \
+        PSKEL_CUDA(cudaGetLastError());   \
+    } while (0)
 
 }  // namespace pskel

@@ -98,7 +98,7 @@ int launch_zgemm(const std::vector<ZgemmJob> &jobs, cudaStream_t stream, DevBuf 
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), pb, cudaMemcpyHostToDevice, stream));
     zgemm_kernel<<<total, 256, 0, stream>>>(d_jobs, d_prefix, nj);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 
@@ -106,7 +106,7 @@ int launch_zgemm_device(const ZgemmJob *d_jobs, const int *d_prefix, int njobs, 
                         cudaStream_t stream) {
     if (total_tiles <= 0) return PSKEL_OK;
     zgemm_kernel<<<total_tiles, 256, 0, stream>>>(d_jobs, d_prefix, njobs);
-    PSKEL_CUDA(cudaGetLastError());
+    PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
 

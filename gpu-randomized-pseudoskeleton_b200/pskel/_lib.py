@@ -39,9 +39,9 @@ class EM(ctypes.Structure):
 
 class Opts(ctypes.Structure):
     _fields_ = [("tol", cd), ("tau", cd), ("tau_relative", ci), ("precision", ci),
-                ("start", ci), ("oversample", ci), ("extra_rows", ci), ("max_rounds", ci),
-                ("seed", ctypes.c_uint64), ("recompress", ci), ("recompress_tol", cd),
-                ("use_graph", ci)]
+                ("start", ci), ("oversample", ci), ("extra_rows", ci), ("extra_cols", ci),
+                ("max_rounds", ci), ("recompress", ci), ("seed", ctypes.c_uint64),
+                ("recompress_tol", cd), ("est_safety", cd), ("use_graph", ci)]
 
 
 class BlockStat(ctypes.Structure):
@@ -75,9 +75,16 @@ SIGNATURES = {
     "pskel_fill_device": (ci, [VP, VP, ci, VP, ci, VP, ci, ci]),
     "pskel_set_blocks": (ci, [VP, I32, I32, ci, I32, I32, ci]),
     "pskel_compress_blocks": (ci, [VP, ctypes.POINTER(Opts), I32, ctypes.POINTER(BlockStat)]),
-    "pskel_last_timing": (ci, [VP, D]),
+    "pskel_last_timing": (ci, [VP, D, ci]),
     "pskel_get_block": (ci, [VP, ci, VP, VP, VP, I32, I32]),
     "pskel_true_errors": (ci, [VP, D]),
+    "pskel_mlp_num_params": (ci, []),
+    "pskel_mlp_forward": (ci, [VP, VP, ci, VP, VP]),
+    "pskel_mlp_grad": (ci, [VP, VP, VP, ci, VP, VP, VP]),
+    "pskel_mlp_adam": (ci, [VP, VP, VP, VP, ci, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                            ctypes.c_float, VP]),
+    "pskel_kernel_launches": (ctypes.c_longlong, []),
+    "pskel_fma_peak": (ci, [D, D]),
 }
 
 _LIB = None

@@ -27,6 +27,17 @@ def _prec(p) -> int:
     raise ValueError(f"precision {p!r}")
 
 
+STAT_DTYPE = np.dtype([("m", "i4"), ("n", "i4"), ("r", "i4"), ("rank", "i4"),
+                       ("rank_recompressed", "i4"), ("rounds", "i4"), ("status", "i4"),
+                       ("est", "f8")], align=True)
+
+
+def stats_array(stats) -> np.ndarray:
+    """ctypes pskel_block_stat_t array -> numpy structured array (C layout, aligned)."""
+    assert ctypes.sizeof(_lib.BlockStat) == STAT_DTYPE.itemsize
+    return np.frombuffer(bytes(stats), dtype=STAT_DTYPE).copy()
+
+
 class Engine:
     def __init__(self, device: int = 0):
         self._lib = _lib.lib()
@@ -87,8 +98,9 @@ class Engine:
 
     # ------------------------------------------------------------------ compression
     def compress(self, tol: float, *, precision="c128", tau: float = 1e-8, tau_relative=True,
-                 r0=None, oversample: int = 10, extra_rows: int = 10, max_rounds: int = 12,
-                 seed: int = 0, use_graph: bool = False, recompress: bool = False,
+                 r0=None, oversample: int = 10, extra_rows: int = 16, extra_cols: int = 16,
+                 est_safety: float = 2.0, max_rounds: int = 12, seed: int = 0,
+                 use_graph: bool = False, recompress: bool = False,
                  recompress_tol: float = 0.0) -> np.ndarray:
         """Compress every block; returns a structured array of per-block stats
         (m, n, r, rank, rank_recompressed, rounds, status, est)."""
@@ -96,8 +108,10 @@ class Engine:
                       precision=_prec(precision),
                       start=START_GIVEN if r0 is not None else START_REFERENCE,
                       oversample=int(oversample), extra_rows=int(extra_rows),
-                      max_rounds=int(max_rounds), seed=int(seed), recompress=int(recompress),
-                      recompress_tol=float(recompress_tol), use_graph=int(bool(use_graph)))
+                      extra_cols=int(extra_cols), max_rounds=int(max_rounds),
+                      recompress=int(recompress), seed=int(seed),
+                      recompress_tol=float(recompress_tol), est_safety=float(est_safety),
+                      use_graph=int(bool(use_graph)))
         nb = self.n_blocks
         stats = (_lib.BlockStat * nb)()
         if r0 is not None:
@@ -110,15 +124,14 @@ class Engine:
             rp = None
         _lib.check(self._lib.pskel_compress_blocks(self._h, ctypes.byref(o), rp, stats))
         self._precision = o.precision
-        dt = np.dtype([("m", "i4"), ("n", "i4"), ("r", "i4"), ("rank", "i4"),
-                       ("rank_recompressed", "i4"), ("rounds", "i4"), ("status", "i4"),
-                       ("est", "f8")])
-        return np.frombuffer(bytes(stats), dtype=dt).copy()
+        return stats_array(stats)
 
     def timing(self) -> dict:
-        t = np.zeros(6)
-        _lib.check(self._lib.pskel_last_timing(self._h, t.ctypes.data_as(_lib.D)))
-        return dict(zip(("sample", "fill", "pinv", "estimate", "recompress", "total"), t.tolist()))
+        """Device ms per phase of the last compress() and its work counters."""
+        t = np.zeros(10)
+        _lib.check(self._lib.pskel_last_timing(self._h, t.ctypes.data_as(_lib.D), 10))
+        return dict(zip(("sample", "fill", "pinv", "estimate", "recompress", "total",
+                         "fill_entries", "point_pairs", "fill_launches", "rounds"), t.tolist()))
 
     def get_block(self, b: int, stats=None):
         rows, cols = self.block_ids(b)

@@ -252,25 +252,29 @@ def icosphere(R: float, subdivisions: int, centre=(0.0, 0.0, 0.0)) -> RWGMesh:
     return get_edge(v.T.copy(), (f + 1).T.copy(), name=f"icosphere{subdivisions}")
 
 
-def ellipsoid(a: float, b: float, c: float, edge: float) -> RWGMesh:
+def ellipsoid(a: float, b: float, c: float, edge: float, max_rwg: int = 1 << 30) -> RWGMesh:
     """Ellipsoid with semi-axes (a, b, c): an icosphere scaled per axis, subdivided until the
-    mean edge length is at most ``edge``."""
+    mean edge length is at most ``edge`` or one more subdivision would exceed ``max_rwg``
+    RWG functions (30 * 4^level)."""
     v0, f0 = _icosahedron()
     lev = 0
     while True:
         v, f = _subdivide_unit(v0, f0, lev)
         w = v * np.array([a, b, c])
         el = np.linalg.norm(w[f[:, 0]] - w[f[:, 1]], axis=1).mean()
-        if el <= edge or lev >= 8:
+        if el <= edge or lev >= 8 or 30 * 4 ** (lev + 1) > max_rwg:
             break
         lev += 1
     return get_edge(w.T.copy(), (f + 1).T.copy(), name="ellipsoid")
 
 
-def cube(side: float, edge: float) -> RWGMesh:
-    """Closed cube of the given side, each face an n x n grid (n = ceil(side/edge)) split
-    along one diagonal; shared face-boundary vertices are merged."""
+def cube(side: float, edge: float, max_rwg: int = 1 << 30) -> RWGMesh:
+    """Closed cube of the given side, each face an n x n grid (n = ceil(side/edge), reduced
+    until the 18 n^2 RWG fit in ``max_rwg``) split along one diagonal; shared face-boundary
+    vertices are merged."""
     n = max(1, int(math.ceil(side / edge)))
+    while n > 1 and 18 * n * n > max_rwg:
+        n -= 1
     h = side / 2
     s = np.linspace(-h, h, n + 1)
     verts = {}

@@ -8,8 +8,8 @@ not shipped). This module supplies the partition the far-field workloads are def
   centroids, ``user_get_OG_basis_center.m:36-39``); boxes are cubes of side ``leaf`` aligned
   at ``origin`` (default: the mesh's bounding-box centre);
 * groups = non-empty leaf boxes, listed in Morton order of their integer box coordinates;
-  groups smaller than ``min_group`` are merged into the nearest larger group (by box-centre
-  distance) so that every block has at least that many rows and columns;
+  groups smaller than ``min_group`` are folded, smallest first, into the nearest group (by
+  size-weighted centre) so that every block has at least that many rows and columns;
 * far pairs = ordered group pairs (i, j), i != j, whose box centres are at least
   ``admissibility`` x the box diameter (sqrt(3) * leaf) apart.
 """
@@ -24,7 +24,7 @@ import numpy as np
 class Partition:
     group_ptr: np.ndarray   # (G+1,) int32 CSR offsets
     group_ids: np.ndarray   # (N,) int32 0-based RWG ids grouped
-    centres: np.ndarray     # (G, 3) group centre (centre of the group's bounding box of boxes)
+    centres: np.ndarray     # (G, 3) group centre (box centre, size-weighted after merges)
     extents: np.ndarray     # (G,) diameter of the bounding sphere of the group's basis centres
     gt: np.ndarray          # (B,) test group of each far block
     gs: np.ndarray          # (B,) source group of each far block
@@ -72,22 +72,27 @@ def partition(mesh, leaf: float, origin=None, admissibility: float = 2.0,
     starts = np.concatenate([[0], np.nonzero(np.diff(ks))[0] + 1, [len(ks)]])
     groups = [order[starts[i]:starts[i + 1]] for i in range(len(starts) - 1)]
     box_centre = [origin + (idx[g[0]] + 0.5) * leaf for g in groups]
-    # merge small groups into the nearest group that is already large enough
-    if min_group > 1:
-        sizes = np.array([len(g) for g in groups])
-        big = [i for i in range(len(groups)) if sizes[i] >= min_group]
-        if not big:
-            big = [int(np.argmax(sizes))]
-        bc = np.array(box_centre)
-        merged = {i: list(groups[i]) for i in big}
-        for i in range(len(groups)):
-            if i in merged:
-                continue
-            j = big[int(np.argmin(np.linalg.norm(bc[big] - bc[i], axis=1)))]
-            merged[j].extend(groups[i])
-        keep = sorted(merged)
-        groups = [np.sort(np.array(merged[i], dtype=np.int64)) for i in keep]
-        box_centre = [box_centre[i] for i in keep]
+    # merge small groups: repeatedly fold the smallest group into the nearest other group
+    # (size-weighted centre), until every group has at least min_group members
+    if min_group > 1 and len(groups) > 1:
+        members = [list(g) for g in groups]
+        cen = [np.asarray(bc, dtype=np.float64) for bc in box_centre]
+        alive = list(range(len(groups)))
+        while len(alive) > 1:
+            sizes = [len(members[i]) for i in alive]
+            k = int(np.argmin(sizes))
+            if sizes[k] >= min_group:
+                break
+            i = alive[k]
+            others = [j for j in alive if j != i]
+            d = [np.linalg.norm(cen[j] - cen[i]) for j in others]
+            j = others[int(np.argmin(d))]
+            ni, nj = len(members[i]), len(members[j])
+            cen[j] = (cen[j] * nj + cen[i] * ni) / (ni + nj)
+            members[j].extend(members[i])
+            alive.remove(i)
+        groups = [np.sort(np.array(members[i], dtype=np.int64)) for i in alive]
+        box_centre = [cen[i] for i in alive]
     ptr = np.zeros(len(groups) + 1, dtype=np.int32)
     ptr[1:] = np.cumsum([len(g) for g in groups])
     ids = np.concatenate(groups).astype(np.int32)

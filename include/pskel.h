@@ -182,12 +182,14 @@ typedef struct {
     int precision;       /* PSKEL_C128 or PSKEL_C64 */
     int start;           /* PSKEL_START_* */
     int oversample;      /* p added to a given r0 */
-    int extra_rows;      /* rows of the randomized error estimate */
+    int extra_rows;      /* unsampled rows of the randomized error estimate (<= 32) */
+    int extra_cols;      /* unsampled columns of the randomized error estimate (<= 32) */
     int max_rounds;      /* adaptive rounds before giving up (the block keeps its last CUR) */
-    uint64_t seed;       /* Philox seed of the index sets */
     int recompress;      /* 1: run the recompression after the last round */
+    uint64_t seed;       /* Philox seed of the index sets */
     double recompress_tol; /* relative singular-value threshold of the recompression */
-    int use_graph;       /* 1: replay the first round from a captured CUDA graph */
+    double est_safety;   /* a block is accepted when est <= tol / est_safety (>= 1) */
+    int use_graph;       /* 1: replay the first round from a CUDA graph captured on a repeat call */
 } pskel_opts_t;
 
 /* Per-block outcome, filled by pskel_compress_blocks. */
@@ -198,7 +200,8 @@ typedef struct {
     int rank_recompressed; /* rank after recompression (0 if not run) */
     int rounds;          /* sampling rounds used (1 = first guess accepted) */
     int status;          /* PSKEL_OK or a negative status */
-    double est;          /* extra-row error estimate of the final round */
+    double est;          /* randomized error estimate of the final round: the larger of the
+                            relative errors on the extra rows and on the extra columns */
 } pskel_block_stat_t;
 
 int pskel_create(pskel_ctx **ctx, int device);
@@ -225,9 +228,11 @@ int pskel_set_blocks(pskel_ctx *ctx, const int *group_ptr, const int *group_ids,
 int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r0,
                           pskel_block_stat_t *stats);
 
-/* Device time in ms of the last pskel_compress_blocks call, split by phase
-   (sample, fill, pinv, estimate, recompress, total). */
-int pskel_last_timing(pskel_ctx *ctx, double *ms6);
+/* Timing and work counters of the last pskel_compress_blocks call: out[0..5] = device ms of
+   the phases sample, fill, pinv, estimate, recompress and the whole call (a round replayed
+   from a CUDA graph is booked under fill as a whole); out[6] = entries filled, out[7] =
+   point pairs evaluated, out[8] = fill launches, out[9] = rounds. n = length of out (<= 10). */
+int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 
 /* Copy block b's factors to host buffers (complex128): C m x r, U r x r, R r x n, 0-based
    local samples I (r) and J (r). Any pointer may be NULL. */
@@ -237,6 +242,29 @@ int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
+
+/* ================================================= 3. rank / sample-count predictor (MLP) */
+/* 8 -> 64 -> 64 -> 1 MLP with GELU in FP32 (parameter layout W1[64x8] b1[64] W2[64x64] b2[64]
+   W3[1x64] b3[1], row-major, contiguous). All pointers are DEVICE pointers; stream may be
+   NULL (legacy default stream). No counterpart in the reference, which grows the sample
+   count adaptively only (compres_single_block_spheres_for_sweep2.jl:878-973). */
+int pskel_mlp_num_params(void);
+/* y[s] = MLP(x[s, 0:8]) for s < n (x row-major n x 8, standardised features). */
+int pskel_mlp_forward(const float *params, const float *x, int n, float *y, void *stream);
+/* grad = d/dparams of mean((MLP(x) - t)^2) over the batch; loss[0] = summed squared error. */
+int pskel_mlp_grad(const float *params, const float *x, const float *t, int n, float *grad,
+                   float *loss, void *stream);
+/* One Adam step (t >= 1) on params with moment buffers m, v. */
+int pskel_mlp_adam(float *params, const float *grad, float *m, float *v, int t, float lr,
+                   float beta1, float beta2, float eps, void *stream);
+
+/* Device kernels launched by this library since load (graph replays count their kernel
+   nodes); used to report how many of the library's kernels ran in a timed region. */
+long long pskel_kernel_launches(void);
+
+/* Measured FMA throughput of this GPU's FP32 and FP64 pipes (TFLOP/s, 2 flops per FMA), from
+   a dependent-chain microbenchmark of about a hundred milliseconds. */
+int pskel_fma_peak(double *fp32_tflops, double *fp64_tflops);
 
 #ifdef __cplusplus
 }

@@ -127,8 +127,8 @@ def cuda_cur_compress3(fill, rows, cols, tol, rng, pinv_tol=1e-10):
 
 
 def extra_row_estimate(C, U, R, Zx, Ix):
-    """Randomized error estimate on extra rows Ix (local row ids, not in I):
-    ||Z(Ix,:) - C(Ix,:) U R||_F / ||Z(Ix,:)||_F; 0 when no extra rows exist."""
+    """Relative error on extra rows Ix (local ids, not in I):
+    ||Z(Ix,:) - C(Ix,:) U R||_F / ||Z(Ix,:)||_F; 0 when there are none."""
     if len(Ix) == 0:
         return 0.0
     approx = (C[Ix, :] @ U) @ R
@@ -136,11 +136,24 @@ def extra_row_estimate(C, U, R, Zx, Ix):
     return float(np.linalg.norm(Zx - approx) / den) if den > 0 else 0.0
 
 
-def plain_adaptive(fill, rows, cols, tol, block_id, seed, p_extra=10, tau=1e-3,
-                   relative=True, r0=None, max_rounds=16):
-    """Plain adaptive pseudoskeleton with seeded sampling and the extra-row estimate:
-    start at r0 (default D/10), double until the estimate is <= tol or r = D. Index sets
-    come from the same Philox/Floyd definition as the device sampler."""
+def extra_col_estimate(C, U, R, Zc, Jx):
+    """Relative error on extra columns Jx (local ids, not in J):
+    ||Z(:,Jx) - C U R(:,Jx)||_F / ||Z(:,Jx)||_F; 0 when there are none."""
+    if len(Jx) == 0:
+        return 0.0
+    approx = C @ (U @ R[:, Jx])
+    den = np.linalg.norm(Zc)
+    return float(np.linalg.norm(Zc - approx) / den) if den > 0 else 0.0
+
+
+def plain_adaptive(fill, rows, cols, tol, block_id, seed, extra_rows=16, extra_cols=16,
+                   safety=2.0, tau=1e-8, relative=True, r0=None, max_rounds=12):
+    """Plain adaptive pseudoskeleton with seeded sampling and the randomized estimate: start at
+    r0 (default D/10), double until max(extra-row, extra-column relative error) <= tol/safety
+    or r = D. Index sets come from the same Philox/Floyd definition as the device sampler
+    (streams 0 rows, 1 columns, 2 extra rows, 3 extra columns)."""
+    rows = np.asarray(rows)
+    cols = np.asarray(cols)
     M, N = len(rows), len(cols)
     D = min(M, N)
     r = start_size(D) if r0 is None else min(max(int(r0), 1), D)
@@ -148,12 +161,14 @@ def plain_adaptive(fill, rows, cols, tol, block_id, seed, p_extra=10, tau=1e-3,
     while True:
         I = el.sample(r, M, block_id, rnd, 0, seed)
         J = el.sample(r, N, block_id, rnd, 1, seed)
-        Ix = el.sample_extra(p_extra, I, M, block_id, rnd, seed)
+        Ix = el.sample_extra(extra_rows, I, M, block_id, rnd, seed, stream=2)
+        Jx = el.sample_extra(extra_cols, J, N, block_id, rnd, seed, stream=3)
         C, U, R = cur_from_indices(fill, rows, cols, I, J, tau, relative)
-        Zx = fill(np.asarray(rows)[Ix], cols) if len(Ix) else np.zeros((0, N), complex)
-        est = extra_row_estimate(C, U, R, Zx, Ix)
-        if est <= tol or r >= D or rnd + 1 >= max_rounds:
-            return dict(C=C, U=U, R=R, I=I, J=J, Ix=Ix, est=est, r=r, rounds=rnd + 1)
+        Zx = fill(rows[Ix], cols) if len(Ix) else np.zeros((0, N), complex)
+        Zc = fill(rows, cols[Jx]) if len(Jx) else np.zeros((M, 0), complex)
+        est = max(extra_row_estimate(C, U, R, Zx, Ix), extra_col_estimate(C, U, R, Zc, Jx))
+        if est <= tol / safety or r >= D or rnd + 1 >= max_rounds:
+            return dict(C=C, U=U, R=R, I=I, J=J, Ix=Ix, Jx=Jx, est=est, r=r, rounds=rnd + 1)
         r = next_size(r, D)
         rnd += 1
 

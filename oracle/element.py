@@ -47,7 +47,8 @@ def lib():
                                        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
         _LIB.oracle_sample_extra.restype = ctypes.c_int
         _LIB.oracle_sample_extra.argtypes = [_I, ctypes.c_int, _I, ctypes.c_int, ctypes.c_int,
-                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]
+                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_uint64]
     return _LIB
 
 
@@ -99,9 +100,10 @@ def sample(r: int, D: int, block: int, rnd: int, stream: int, seed: int) -> np.n
     return out[:r].copy()
 
 
-def sample_extra(p: int, I: np.ndarray, m: int, block: int, rnd: int, seed: int) -> np.ndarray:
+def sample_extra(p: int, I: np.ndarray, m: int, block: int, rnd: int, seed: int,
+                 stream: int = 2) -> np.ndarray:
     I = np.ascontiguousarray(I, dtype=np.int32)
     out = np.zeros(max(p, 1), dtype=np.int32)
     n = lib().oracle_sample_extra(out.ctypes.data_as(_I), p, I.ctypes.data_as(_I), len(I), m,
-                                  block, rnd, seed)
+                                  block, rnd, stream, seed)
     return out[:max(n, 0)].copy()

@@ -15,7 +15,8 @@
  *   output   = taken values in increasing order (0-based)
  *
  * Streams: 0 = sampled rows I, 1 = sampled columns J, 2 = extra estimator rows drawn from
- * the rows not in I (the k-th smallest unsampled row is returned for a draw of k).
+ * the rows not in I, 3 = extra estimator columns drawn from the columns not in J (the k-th
+ * smallest unsampled index is returned for a draw of k).
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -80,16 +81,17 @@ int oracle_sample(int *out, int r, int D, uint32_t block, uint32_t round, uint32
     return 0;
 }
 
-/* p extra rows drawn from the complement of the sorted set I (size r) in [0, m). */
+/* p extra indices drawn from the complement of the sorted set I (size r) in [0, m); stream 2
+   for extra rows, 3 for extra columns. */
 int oracle_sample_extra(int *out, int p, const int *I, int r, int m, uint32_t block,
-                        uint32_t round, uint64_t seed)
+                        uint32_t round, uint32_t stream, uint64_t seed)
 {
     const int free_rows = m - r;
     if (p > free_rows) p = free_rows;
     if (p <= 0) return 0;
     int *pick = (int *)malloc(sizeof(int) * (size_t)p);
     if (!pick) return -1;
-    oracle_sample(pick, p, free_rows, block, round, 2u, seed);
+    oracle_sample(pick, p, free_rows, block, round, stream, seed);
     /* map the k-th free row to its index */
     int k = 0, ii = 0, n = 0;
     for (int v = 0; v < m && n < p; ++v) {

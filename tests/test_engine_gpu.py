@@ -50,7 +50,7 @@ def test_batched_compression_errors(small_sphere, prec):
     with Engine() as eng:
         eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
         eng.set_blocks(part)
-        st = eng.compress(tol, precision=prec, tau=1e-7, seed=0)
+        st = eng.compress(tol, precision=prec, tau=1e-7, seed=0, est_safety=2.0)
         assert np.all(st["status"] == 0)
         err = eng.true_errors()
     assert np.all(np.isfinite(err))
@@ -75,3 +75,25 @@ def test_true_error_matches_oracle(small_sphere):
             Z = el.fill(m, rows + 1, cols + 1, k, eta, 7, 7)
             e = co.rel_fro_error(Z, C, U, R)
             assert abs(e - err[b]) <= 1e-6 * max(e, 1e-12) + 1e-12
+
+
+def test_adaptive_rounds_match_oracle(small_sphere):
+    """The device adaptive loop takes the same sample counts and rounds as the oracle's
+    restatement (same Philox index sets, same randomized estimate and acceptance rule)."""
+    m, part = small_sphere
+    k, eta = 2 * np.pi, 376.73
+    tol, tau, seed = 1e-4, 1e-7, 11
+    with Engine() as eng:
+        eng.upload_mesh(m, k, eta, q=7)
+        eng.set_blocks(part)
+        st = eng.compress(tol, precision="c128", tau=tau, seed=seed, extra_rows=16,
+                          extra_cols=16, est_safety=2.0)
+        for b in (1, eng.n_blocks // 3, eng.n_blocks - 2):
+            rows, cols = eng.block_ids(b)
+            fill = lambda a, c: el.fill(m, a, c, k, eta, 7, 7)
+            o = co.plain_adaptive(fill, rows + 1, cols + 1, tol, b, seed, extra_rows=16,
+                                  extra_cols=16, safety=2.0, tau=tau)
+            assert st["r"][b] == o["r"] and st["rounds"][b] == o["rounds"], (b, st[b], o["r"], o["rounds"])
+            assert abs(st["est"][b] - o["est"]) <= 1e-6 * o["est"] + 1e-14
+            C, U, R, I, J = eng.get_block(b, st)
+            assert np.array_equal(I, o["I"]) and np.array_equal(J, o["J"])
