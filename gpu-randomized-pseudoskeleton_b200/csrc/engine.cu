@@ -337,6 +337,7 @@ struct pskel_ctx {
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;
+    int split[2] = {1, 1};  // fill lanes per entry: c128, c64
     double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;
@@ -474,7 +475,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     }
     // fill tile prefix
     int tm, tn;
-    fill_tile_shape(o.precision, c->em.q_test, 1, &tm, &tn);
+    fill_tile_shape(o.precision, c->em.q_test, c->split[o.precision == PSKEL_C64 ? 1 : 0], &tm, &tn);
     std::vector<int> prefix(fills.size() + 1, 0);
     for (size_t i = 0; i < fills.size(); ++i)
         prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
@@ -527,7 +528,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.q_test = c->em.q_test;
     fp.q_src = c->em.q_src;
     fp.precision = o.precision;
-    fp.split = 1;
+    fp.split = c->split[o.precision == PSKEL_C64 ? 1 : 0];
     PSKEL_TRY(launch_fill(c->mesh, fp, p.d_fill, p.d_fill_prefix, p.fill_jobs, p.fill_tiles,
                           c->flags.as<int>(), s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
@@ -798,6 +799,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back(o.extra_cols);
             key.push_back((int)std::lround(std::log10(std::max(o.tau, 1e-300)) * 1000));
             key.push_back(o.tau_relative);
+            key.push_back(c->split[0] * 8 + c->split[1]);
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -911,6 +913,18 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         if (res.status != PSKEL_OK) worst = res.status;
     }
     (void)worst;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_set_fill_split(pskel_ctx *c, int split_c128, int split_c64) {
+    PSKEL_TRY(ctx_ok(c));
+    auto ok = [](int v) { return v == 0 || v == 1 || v == 2 || v == 4; };
+    if (!ok(split_c128) || !ok(split_c64)) {
+        set_error(PSKEL_ERR_ARG, "fill split must be 1, 2 or 4 (0 = unchanged)");
+        return PSKEL_ERR_ARG;
+    }
+    if (split_c128) c->split[0] = split_c128;
+    if (split_c64) c->split[1] = split_c64;
     return PSKEL_OK;
 }
 

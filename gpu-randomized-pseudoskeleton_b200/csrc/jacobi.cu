@@ -328,15 +328,16 @@ int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweep
 
 // ------------------------------------------------------------------ pseudo-inverse
 // P (n x m) = sum over kept j of (1/sigma_j^2) V[:, j] conj(AV[:, j])^T; one CTA per 32x32
-// output tile of one job (grid.y = job), K loop over the n columns in chunks of 16.
+// output tile of one job (grid.x = job, grid.y = tile), K loop over the n columns in chunks of
+// 16.
 __global__ void __launch_bounds__(256) pinv_kernel(const PinvJob *jobs) {
-    const PinvJob job = jobs[blockIdx.y];
+    const PinvJob job = jobs[blockIdx.x];
     const int n = job.n, m = job.m;
     const int tiles_a = (n + 31) / 32;
     const int tiles_b = (m + 31) / 32;
-    if ((int)blockIdx.x >= tiles_a * tiles_b) return;
-    const int a0 = (blockIdx.x % tiles_a) * 32;
-    const int b0 = (blockIdx.x / tiles_a) * 32;
+    if ((int)blockIdx.y >= tiles_a * tiles_b) return;
+    const int a0 = (blockIdx.y % tiles_a) * 32;
+    const int b0 = (blockIdx.y / tiles_a) * 32;
     __shared__ double smax;
     __shared__ double w[16];
     __shared__ double2 sVt[16][33];
@@ -390,7 +391,7 @@ __global__ void __launch_bounds__(256) pinv_kernel(const PinvJob *jobs) {
             if (cb < m) job.P[ra + (size_t)cb * n] = acc[c];
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && job.rank) {
+    if (blockIdx.y == 0 && threadIdx.x == 0 && job.rank) {
         int k = 0;
         for (int j = 0; j < n; ++j) k += (job.sigma[j] >= thr && job.sigma[j] > 0);
         *job.rank = k;
@@ -399,7 +400,11 @@ __global__ void __launch_bounds__(256) pinv_kernel(const PinvJob *jobs) {
 
 int batched_pinv(const PinvJob *d_jobs, int njobs, int max_tiles, cudaStream_t stream) {
     if (njobs <= 0) return PSKEL_OK;
-    dim3 grid(max_tiles, njobs);
+    if (max_tiles > 65535) {
+        set_error(PSKEL_ERR_ARG, "pinv: %d output tiles per matrix exceed the grid limit", max_tiles);
+        return PSKEL_ERR_ARG;
+    }
+    dim3 grid(njobs, max_tiles);
     pinv_kernel<<<grid, 256, 0, stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;

@@ -78,6 +78,7 @@ SIGNATURES = {
     "pskel_last_timing": (ci, [VP, D, ci]),
     "pskel_get_block": (ci, [VP, ci, VP, VP, VP, I32, I32]),
     "pskel_true_errors": (ci, [VP, D]),
+    "pskel_set_fill_split": (ci, [VP, ci, ci]),
     "pskel_mlp_num_params": (ci, []),
     "pskel_mlp_forward": (ci, [VP, VP, ci, VP, VP]),
     "pskel_mlp_grad": (ci, [VP, VP, VP, ci, VP, VP, VP]),

@@ -154,6 +154,10 @@ class Engine:
         _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
         return err
 
+    def set_fill_split(self, split_c128: int = 0, split_c64: int = 0):
+        """Fill-kernel variant (lanes per entry: 1, 2 or 4; 0 = unchanged)."""
+        _lib.check(self._lib.pskel_set_fill_split(self._h, int(split_c128), int(split_c64)))
+
     def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,
                     precision="c128"):
         """Fill into device buffers given as raw device pointers (e.g. torch data_ptr())."""

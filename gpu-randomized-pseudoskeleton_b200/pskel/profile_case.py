@@ -1,0 +1,47 @@
+"""One small, repeatable compression workload for kernel profiling and variant timing.
+
+    python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py PRECISION [CALLS] [SPLIT]
+
+builds the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions, 0.5-lambda leaves), then
+makes CALLS (default 3) single-round compressions of every far block at a fixed sample count of
+24 with the given precision (c128 or c64) and fill split, printing the fill time and point-pair
+rate of each call. Under a profiler the fill launch of call i is the i-th fill_kernel launch.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+if __package__ in (None, ""):
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+
+from pskel import mesh as pmesh  # noqa: E402
+from pskel import octree  # noqa: E402
+from pskel.engine import Engine  # noqa: E402
+
+
+def main():
+    prec = sys.argv[1] if len(sys.argv) > 1 else "c64"
+    calls = int(sys.argv[2]) if len(sys.argv) > 2 else 3
+    split = int(sys.argv[3]) if len(sys.argv) > 3 else 1
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        if prec == "c128":
+            eng.set_fill_split(split_c128=split)
+        else:
+            eng.set_fill_split(split_c64=split)
+        for i in range(calls):
+            eng.compress(1.0, precision=prec, r0=np.full(part.n_blocks, 24), oversample=0,
+                         max_rounds=1, seed=i)
+            t = eng.timing()
+            print(f"{prec} split {split} call {i}: fill {t['fill']:.3f} ms, "
+                  f"{t['point_pairs'] / t['fill'] / 1e6:.1f} G point pairs/s", flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -239,6 +239,10 @@ int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
                     int *I, int *J);
 
+/* Fill-kernel variant used by this context: lanes per matrix entry (1, 2 or 4) for the
+   complex128 and complex64 fills (0 keeps the current choice). Set by the autotuner. */
+int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
+
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
