@@ -287,8 +287,7 @@ int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_re
     return PSKEL_OK;
 }
 
-int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
-               int max_sweeps, cudaStream_t stream) {
+int svd_resident_attr() {
     static bool attr = false;
     if (!attr) {
         PSKEL_CUDA(cudaFuncSetAttribute(svd_resident_kernel,
@@ -299,6 +298,12 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t ma
                                         (int)kSmemBudget));
         attr = true;
     }
+    return PSKEL_OK;
+}
+
+int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
+               int max_sweeps, cudaStream_t stream) {
+    PSKEL_TRY(svd_resident_attr());
     if (n_res > 0) {
         svd_resident_kernel<<<n_res, kSvdThreads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
         PSKEL_LAUNCHED(1);

@@ -96,7 +96,9 @@ struct FillJob {
     const int *rows;
     const int *cols;
     void *out;
-    int nr, nc, ld, pad;
+    int nr, nc, ld;
+    int trans;  // 1: store Z(rows, cols) transposed, out[j + i * ld] (Galerkin symmetry lets a
+                // caller fill Z(a, b) as the transpose of Z(b, a) with the long side on rows)
 };
 
 struct FillParams {
@@ -104,7 +106,7 @@ struct FillParams {
     double r_near;     // > 0: flag triangle pairs whose centroids are closer than this
     int q_test, q_src;
     int precision;     // PSKEL_C128 / PSKEL_C64
-    int split;         // lanes per entry (1, 2 or 4); 0 = automatic
+    int split;         // 0: two rows per thread (default kernel); 1, 2, 4: lanes per entry
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the
@@ -147,6 +149,8 @@ int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_re
              size_t *max_res_smem);
 int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
                int max_sweeps, cudaStream_t stream);
+// Shared-memory attributes of the SVD kernels (set once per process).
+int svd_resident_attr();
 
 // pinv of each job after batched_svd: P_b (n_b x m_b) = V diag(1/sigma^2) (A V)^H over the
 // kept columns; rank_b receives the count kept. thr_b = tau (absolute) or tau * sigma_max.

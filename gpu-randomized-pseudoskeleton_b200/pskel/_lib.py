@@ -86,6 +86,7 @@ SIGNATURES = {
                             ctypes.c_float, VP]),
     "pskel_kernel_launches": (ctypes.c_longlong, []),
     "pskel_fma_peak": (ci, [D, D]),
+    "pskel_pinv_noalloc": (ci, [VP, ci, ci, cd, ci, VP, VP, VP, VP]),
 }
 
 _LIB = None

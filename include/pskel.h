@@ -262,6 +262,20 @@ int pskel_mlp_grad(const float *params, const float *x, const float *t, int n, f
 int pskel_mlp_adam(float *params, const float *grad, float *m, float *v, int t, float lr,
                    float beta1, float beta2, float eps, void *stream);
 
+/* Truncated pseudo-inverse P (N x M) of one complex128 matrix A (M x N), M, N <= 64, that
+   allocates no device memory: for callers that cannot call cudaMalloc (a host framework that
+   owns device memory through its own pool, or a latency-critical loop where an allocation
+   could block or synchronise the device). No counterpart in the reference, whose pinv
+   helpers allocate on every call. A and P (and the optional sigma, min(M, N) values sorted
+   descending, and rank) are DEVICE buffers; singular values below tau (relative = 0) or
+   tau * s_max (relative = 1) are dropped. The scratch is one fixed 256 KiB device array per
+   GPU, shared by all calls: calls that overlap on the GPU race. The first call on a device
+   looks up that array's address; make it before any stream capture. Returns after its stream
+   has finished, with PSKEL_ERR_ARG for sizes above 64 and PSKEL_ERR_NOCONV if the Jacobi
+   sweeps did not converge. */
+int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau, int relative,
+                       pskel_c128 *P, double *sigma, int *rank, void *stream);
+
 /* Device kernels launched by this library since load (graph replays count their kernel
    nodes); used to report how many of the library's kernels ran in a timed region. */
 long long pskel_kernel_launches(void);
