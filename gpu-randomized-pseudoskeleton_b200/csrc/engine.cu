@@ -337,7 +337,7 @@ struct pskel_ctx {
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;
-    int split[2] = {1, 1};  // fill lanes per entry: c128, c64
+    int split[2] = {0, 0};  // fill variant (0: two rows per thread; 1, 2, 4: lanes per entry)
     double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;
@@ -456,7 +456,9 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         w.T = reinterpret_cast<double2 *>(sb + soff);
         soff += al16((pe + pc) * r * sizeof(double2));
         fills.push_back(FillJob{w.rows_g, w.Jg, w.C, w.m, w.r + w.pc, w.m, 0});
-        fills.push_back(FillJob{w.Ig, w.cols_g, w.Rx, w.r + w.pe, w.n, w.r + w.pe, 0});
+        // Rx = Z([I; Ix], group_s) filled as the transpose of Z(group_s, [I; Ix]) (the Galerkin
+        // block is symmetric for equal test and source rules), so the long side is on rows
+        fills.push_back(FillJob{w.cols_g, w.Ig, w.Rx, w.n, w.r + w.pe, w.r + w.pe, 1});
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, o.tau, o.tau_relative};
         max_pinv_tiles = std::max(max_pinv_tiles, ((w.r + 31) / 32) * ((w.r + 31) / 32));
@@ -651,7 +653,7 @@ extern "C" int pskel_fill_device(pskel_ctx *c, const int *rows_dev, int nr, cons
     }
     if ((size_t)nr * nc == 0) return PSKEL_OK;
     int tm, tn;
-    fill_tile_shape(precision, c->em.q_test, 1, &tm, &tn);
+    fill_tile_shape(precision, c->em.q_test, c->split[precision == PSKEL_C64 ? 1 : 0], &tm, &tn);
     FillJob job{rows_dev, cols_dev, Z_dev, nr, nc, ld, 0};
     int prefix[2] = {0, ((nr + tm - 1) / tm) * ((nc + tn - 1) / tn)};
     PSKEL_TRY(c->tmp3.reserve(512));
@@ -665,7 +667,7 @@ extern "C" int pskel_fill_device(pskel_ctx *c, const int *rows_dev, int nr, cons
     fp.q_test = c->em.q_test;
     fp.q_src = c->em.q_src;
     fp.precision = precision;
-    fp.split = 1;
+    fp.split = c->split[precision == PSKEL_C64 ? 1 : 0];
     return launch_fill(c->mesh, fp, c->tmp3.as<FillJob>(),
                        reinterpret_cast<int *>(c->tmp3.as<char>() + 256), 1, prefix[1],
                        c->flags.as<int>(), c->stream);
@@ -918,13 +920,13 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
 
 extern "C" int pskel_set_fill_split(pskel_ctx *c, int split_c128, int split_c64) {
     PSKEL_TRY(ctx_ok(c));
-    auto ok = [](int v) { return v == 0 || v == 1 || v == 2 || v == 4; };
+    auto ok = [](int v) { return v == -1 || v == 0 || v == 1 || v == 2 || v == 4; };
     if (!ok(split_c128) || !ok(split_c64)) {
-        set_error(PSKEL_ERR_ARG, "fill split must be 1, 2 or 4 (0 = unchanged)");
+        set_error(PSKEL_ERR_ARG, "fill variant must be -1 (unchanged), 0, 1, 2 or 4");
         return PSKEL_ERR_ARG;
     }
-    if (split_c128) c->split[0] = split_c128;
-    if (split_c64) c->split[1] = split_c64;
+    if (split_c128 >= 0) c->split[0] = split_c128;
+    if (split_c64 >= 0) c->split[1] = split_c64;
     return PSKEL_OK;
 }
 
@@ -1013,7 +1015,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         std::vector<long long> sizes(nbb);
         size_t zo = 0, wo = 0;
         int tm, tn;
-        fill_tile_shape(PSKEL_C128, c->em.q_test, 1, &tm, &tn);
+        fill_tile_shape(PSKEL_C128, c->em.q_test, c->split[0], &tm, &tn);
         std::vector<int> prefix(nbb + 1, 0);
         for (int i = 0; i < nbb; ++i) {
             const int b = b0 + i;
@@ -1080,7 +1082,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         fp.q_test = c->em.q_test;
         fp.q_src = c->em.q_src;
         fp.precision = PSKEL_C128;
-        fp.split = 1;
+        fp.split = c->split[0];
         PSKEL_TRY(launch_fill(c->mesh, fp, d_f, d_p, nbb, prefix.back(), c->flags.as<int>(), c->stream));
         block_norm_kernel<<<nbb, 256, 0, c->stream>>>(d_m, d_s, d_nz);
         PSKEL_LAUNCHED(1);

@@ -173,6 +173,262 @@ __global__ void __launch_bounds__(TM *TN *SPLIT, FillOcc<T>::value)
     }
 }
 
+// ===================================================================== default fill kernel
+// Sin and cos of the phase, evaluated without a library call: the phase t (in wavelengths, FP64)
+// is split as t = q/4 + g with q = rint(4 t) (the integer lands in the low mantissa word of
+// 4 t + 1.5 * 2^52, so no conversion instruction is needed) and |g| <= 1/8, then
+// sin/cos(2 pi g) come from their Taylor series about 0 (coefficients (-1)^k / n!), truncated
+// where the first omitted term is below half an ulp at |2 pi g| = pi/4 (FP32: theta^9 / theta^10,
+// FP64: theta^17 / theta^16), and a rotation by q quarter turns gives sin/cos(2 pi t).
+__host__ __device__ constexpr double inv_fact(int n) { return n <= 1 ? 1.0 : inv_fact(n - 1) / n; }
+
+__device__ __forceinline__ void rotate_quadrant(int q, float sn, float cs, float *s, float *c) {
+    float a = (q & 1) ? cs : sn;
+    float b = (q & 1) ? sn : cs;
+    *s = (q & 2) ? -a : a;
+    *c = ((q + 1) & 2) ? -b : b;
+}
+__device__ __forceinline__ void rotate_quadrant(int q, double sn, double cs, double *s, double *c) {
+    double a = (q & 1) ? cs : sn;
+    double b = (q & 1) ? sn : cs;
+    *s = (q & 2) ? -a : a;
+    *c = ((q + 1) & 2) ? -b : b;
+}
+
+__device__ __forceinline__ void sincos_2pi(float g, int q, float *s, float *c) {
+    const float th = g * 6.28318530717958647692f;
+    const float t2 = th * th;
+    float ps = fmaf(t2, (float)inv_fact(9), -(float)inv_fact(7));
+    ps = fmaf(t2, ps, (float)inv_fact(5));
+    ps = fmaf(t2, ps, -(float)inv_fact(3));
+    const float sn = fmaf(th * t2, ps, th);
+    float pc = fmaf(t2, -(float)inv_fact(10), (float)inv_fact(8));
+    pc = fmaf(t2, pc, -(float)inv_fact(6));
+    pc = fmaf(t2, pc, (float)inv_fact(4));
+    pc = fmaf(t2, pc, -0.5f);
+    const float cs = fmaf(t2, pc, 1.0f);
+    rotate_quadrant(q, sn, cs, s, c);
+}
+
+__device__ __forceinline__ void sincos_2pi(double g, int q, double *s, double *c) {
+    const double th = g * 6.28318530717958647692;
+    const double t2 = th * th;
+    double ps = fma(t2, inv_fact(17), -inv_fact(15));
+    ps = fma(t2, ps, inv_fact(13));
+    ps = fma(t2, ps, -inv_fact(11));
+    ps = fma(t2, ps, inv_fact(9));
+    ps = fma(t2, ps, -inv_fact(7));
+    ps = fma(t2, ps, inv_fact(5));
+    ps = fma(t2, ps, -inv_fact(3));
+    const double sn = fma(th * t2, ps, th);
+    double pc = fma(t2, inv_fact(16), -inv_fact(14));
+    pc = fma(t2, pc, inv_fact(12));
+    pc = fma(t2, pc, -inv_fact(10));
+    pc = fma(t2, pc, inv_fact(8));
+    pc = fma(t2, pc, -inv_fact(6));
+    pc = fma(t2, pc, inv_fact(4));
+    pc = fma(t2, pc, -0.5);
+    const double cs = fma(t2, pc, 1.0);
+    rotate_quadrant(q, sn, cs, s, c);
+}
+
+// t (wavelengths) -> (g, q) with t = q/4 + g, |g| <= 1/8
+__device__ __forceinline__ double split_quarter(double t, int *q) {
+    const double M = 6755399441055744.0;  // 1.5 * 2^52
+    const double tm = fma(t, 4.0, M);
+    *q = __double2loint(tm);
+    return fma(tm - M, -0.25, t);
+}
+
+template <typename T> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { using type = double4; };
+template <typename T> struct Fill2Occ { static constexpr int value = sizeof(T) == 8 ? 2 : 3; };
+
+// Two rows per thread: thread (il, jl) computes entries (i0 + il, j) and (i0 + il + TM/2, j),
+// so every source point read from shared memory serves two entries. Source points are staged
+// as {x, y} (double2), z (double), {ux, uy, uz, e} (T4); test points field-major per row with
+// odd strides. Persistent grid over the tile list of all jobs, like fill_kernel.
+template <typename T, int Q, int TM, int TN>
+__global__ void __launch_bounds__(TM / 2 * TN, Fill2Occ<T>::value)
+    fill2_kernel(const double *__restrict__ rec_t, const double *__restrict__ rec_s,
+                 const FillJob *__restrict__ jobs, const int *__restrict__ tile_prefix,
+                 int njobs, int total_tiles, T k, T kinv, double kturn, T scale,
+                 double r_near2, int *flags) {
+    constexpr int NP = 2 * Q;
+    constexpr int RS = (7 * NP) | 1;
+    constexpr int PS = (3 * NP) | 1;
+    constexpr int VS = (4 * NP) | 1;
+    constexpr int HALF = TM / 2;
+    constexpr int NT = HALF * TN;
+    using C2 = typename Cplx<T>::type;
+    using T4 = typename Vec4<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *s_xy = reinterpret_cast<double2 *>(smem_raw);         // TN x NP
+    double *s_z = reinterpret_cast<double *>(s_xy + TN * NP);        // TN x NP
+    T4 *s_v = reinterpret_cast<T4 *>(s_z + TN * NP);                 // TN x NP
+    double *p_t = reinterpret_cast<double *>(s_v + TN * NP);         // TM x PS
+    T *v_t = reinterpret_cast<T *>(p_t + TM * PS);                   // TM x VS
+
+    const int tid = threadIdx.x;
+    const int il = tid % HALF;
+    const int jl = tid / HALF;
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const int jb = find_job(tile_prefix, njobs, tile);
+        const FillJob job = jobs[jb];
+        const int local = tile - tile_prefix[jb];
+        const int tiles_r = (job.nr + TM - 1) / TM;
+        const int i0 = (local % tiles_r) * TM;
+        const int j0 = (local / tiles_r) * TN;
+
+        for (int idx = tid; idx < TM * 7 * NP; idx += NT) {
+            const int r = idx / (7 * NP), f = idx - r * (7 * NP);
+            const int row = i0 + r;
+            const double v = row < job.nr ? rec_t[(size_t)job.rows[row] * RS + f] : 0.0;
+            if (f < 3 * NP) p_t[r * PS + f] = v; else v_t[r * VS + f - 3 * NP] = (T)v;
+        }
+        for (int idx = tid; idx < TN * NP; idx += NT) {
+            const int c = idx / NP, q = idx - c * NP;
+            const int col = j0 + c;
+            const double *src = rec_s + (size_t)(col < job.nc ? job.cols[col] : 0) * RS;
+            const bool ok = col < job.nc;
+            s_xy[idx] = make_double2(ok ? src[q] : 0.0, ok ? src[NP + q] : 0.0);
+            s_z[idx] = ok ? src[2 * NP + q] : 0.0;
+            T4 v;
+            v.x = ok ? (T)src[3 * NP + q] : T(0);
+            v.y = ok ? (T)src[4 * NP + q] : T(0);
+            v.z = ok ? (T)src[5 * NP + q] : T(0);
+            v.w = ok ? (T)src[6 * NP + q] : T(0);
+            s_v[idx] = v;
+        }
+        __syncthreads();
+
+        const int ia = i0 + il, ib = i0 + il + HALF, j = j0 + jl;
+        const bool live_a = ia < job.nr && j < job.nc;
+        const bool live_b = ib < job.nr && j < job.nc;
+        if (live_a) {
+            T re_a = 0, im_a = 0, re_b = 0, im_b = 0;
+            const double *pa = p_t + il * PS;
+            const double *pb = p_t + (il + HALF) * PS;
+            const T *va = v_t + il * VS;
+            const T *vb = v_t + (il + HALF) * VS;
+            const double2 *sxy = s_xy + jl * NP;
+            const double *sz = s_z + jl * NP;
+            const T4 *sv = s_v + jl * NP;
+            if (r_near2 > 0.0) {
+                bool near = false;
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        const double2 xy = sxy[b * Q];
+                        const double z = sz[b * Q];
+                        double dx = pa[a * Q] - xy.x, dy = pa[NP + a * Q] - xy.y, dz = pa[2 * NP + a * Q] - z;
+                        near |= dx * dx + dy * dy + dz * dz < r_near2;
+                        if (live_b) {
+                            dx = pb[a * Q] - xy.x; dy = pb[NP + a * Q] - xy.y; dz = pb[2 * NP + a * Q] - z;
+                            near |= dx * dx + dy * dy + dz * dz < r_near2;
+                        }
+                    }
+                if (near) atomicOr(flags, 1);
+            }
+#pragma unroll 1
+            for (int p = 0; p < NP; ++p) {
+                const double xa = pa[p], ya = pa[NP + p], za = pa[2 * NP + p];
+                const double xb = pb[p], yb = pb[NP + p], zb = pb[2 * NP + p];
+                const T uxa = k * va[p], uya = k * va[NP + p], uza = k * va[2 * NP + p];
+                const T da = kinv * va[3 * NP + p];
+                const T uxb = k * vb[p], uyb = k * vb[NP + p], uzb = k * vb[2 * NP + p];
+                const T db = kinv * vb[3 * NP + p];
+#pragma unroll 2
+                for (int q = 0; q < NP; ++q) {
+                    const double2 xy = sxy[q];
+                    const double z = sz[q];
+                    const T4 v = sv[q];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const double dx = (h ? xb : xa) - xy.x;
+                        const double dy = (h ? yb : ya) - xy.y;
+                        const double dz = (h ? zb : za) - z;
+                        const double R2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                        T rinv, sn, cs;
+                        int quad;
+                        if constexpr (sizeof(T) == 8) {
+                            rinv = rsqrt(R2);
+                            const double g = split_quarter(R2 * rinv * kturn, &quad);
+                            sincos_2pi(g, quad, &sn, &cs);
+                        } else {
+                            const float y = rsqrtf((float)R2);
+                            const double yd = (double)y;
+                            const double R0 = R2 * yd;
+                            const double R = fma(fma(-R0, R0, R2), 0.5 * yd, R0);
+                            const double g = split_quarter(R * kturn, &quad);
+                            sincos_2pi((float)g, quad, &sn, &cs);
+                            rinv = y;
+                        }
+                        const T ux = h ? uxb : uxa, uy = h ? uyb : uya, uz = h ? uzb : uza;
+                        const T dd = h ? db : da;
+                        const T A = fma(dd, v.w, -fma(ux, v.x, fma(uy, v.y, uz * v.z)));
+                        const T t = A * rinv;
+                        if (h) {
+                            re_b = fma(t, sn, re_b);
+                            im_b = fma(t, cs, im_b);
+                        } else {
+                            re_a = fma(t, sn, re_a);
+                            im_a = fma(t, cs, im_a);
+                        }
+                    }
+                }
+            }
+            C2 za_, zb_;
+            za_.x = scale * re_a;
+            za_.y = scale * im_a;
+            zb_.x = scale * re_b;
+            zb_.y = scale * im_b;
+            C2 *out = reinterpret_cast<C2 *>(job.out);
+            if (!job.trans) {
+                out[ia + (size_t)j * job.ld] = za_;
+                if (live_b) out[ib + (size_t)j * job.ld] = zb_;
+            } else {
+                out[j + (size_t)ia * job.ld] = za_;
+                if (live_b) out[j + (size_t)ib * job.ld] = zb_;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int Q, int TM, int TN>
+static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jobs,
+                     const int *d_prefix, int njobs, int total_tiles, int *d_flags,
+                     cudaStream_t stream) {
+    constexpr int NP = 2 * Q;
+    constexpr int PS = (3 * NP) | 1;
+    constexpr int VS = (4 * NP) | 1;
+    constexpr int NT = TM / 2 * TN;
+    const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
+                        (sizeof(double) * PS + sizeof(T) * VS) * (size_t)TM + 16;
+    auto kern = fill2_kernel<T, Q, TM, TN>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    if (per_sm < 1) per_sm = 1;
+    long long grid = (long long)sm_count() * per_sm;
+    if (grid > total_tiles) grid = total_tiles;
+    if (grid < 1) return PSKEL_OK;
+    const double pi = 3.14159265358979323846;
+    kern<<<(int)grid, NT, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
+                                          (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)),
+                                          p.r_near > 0 ? p.r_near * p.r_near : 0.0, d_flags);
+    PSKEL_LAUNCHED(1);
+    return PSKEL_OK;
+}
+
 template <typename T, int Q, int TM, int TN, int SPLIT>
 static int launch_t(const double *rec_t, const double *rec_s, const FillParams &p,
                     const FillJob *d_jobs, const int *d_prefix, int njobs, int total_tiles,
@@ -209,7 +465,11 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
 
 int fill_tile_shape(int precision, int q, int split, int *tm, int *tn) {
     (void)q;
-    if (split <= 0) split = 1;
+    if (split <= 0) {  // default kernel: 64 rows (two per thread) x 8 columns
+        *tm = 64;
+        *tn = 8;
+        return PSKEL_OK;
+    }
     if (precision == PSKEL_C128) {
         *tm = 16;
         *tn = split == 1 ? 16 : (split == 2 ? 8 : 4);
@@ -234,8 +494,18 @@ int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
         set_error(PSKEL_ERR_STATE, "fill: records for Q=%d not built", p.q_test);
         return PSKEL_ERR_STATE;
     }
-    const int split = p.split <= 0 ? 1 : p.split;
+    const int split = p.split;
     const double *r64 = rec.f64.as<double>();
+    if (split <= 0) {
+        if (p.precision == PSKEL_C128) {
+            if (p.q_test == 7)
+                return launch2_t<double, 7, 64, 8>(r64, p, d_jobs, d_tile_prefix, njobs, total_tiles, d_flags, stream);
+            return launch2_t<double, 1, 64, 8>(r64, p, d_jobs, d_tile_prefix, njobs, total_tiles, d_flags, stream);
+        }
+        if (p.q_test == 7)
+            return launch2_t<float, 7, 64, 8>(r64, p, d_jobs, d_tile_prefix, njobs, total_tiles, d_flags, stream);
+        return launch2_t<float, 1, 64, 8>(r64, p, d_jobs, d_tile_prefix, njobs, total_tiles, d_flags, stream);
+    }
 #define PSKEL_FILL_CASE(T, REC, Q, TM, TN, S)                                                   \
     return launch_t<T, Q, TM, TN, S>(REC, REC, p, d_jobs, d_tile_prefix, njobs, total_tiles,   \
                                      d_flags, stream)
@@ -263,4 +533,37 @@ int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
 #undef PSKEL_FILL_CASE
 }
 
+// ---------------------------------------------------------------- diagnostics
+// The fill's sin/cos of 2 pi t next to CUDA's sincospi(2 t), for tests of the polynomial.
+__global__ void diag_sincos_kernel(const double *t, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int q;
+    const double g = split_quarter(t[i], &q);
+    double s, c;
+    sincos_2pi(g, q, &s, &c);
+    float sf, cf;
+    sincos_2pi((float)g, q, &sf, &cf);
+    double rs, rc;
+    sincospi(2.0 * t[i], &rs, &rc);
+    out[6 * i + 0] = s;
+    out[6 * i + 1] = c;
+    out[6 * i + 2] = sf;
+    out[6 * i + 3] = cf;
+    out[6 * i + 4] = rs;
+    out[6 * i + 5] = rc;
+}
+
 }  // namespace pskel
+
+extern "C" int pskel_diag_sincos(const double *t_dev, int n, double *out_dev) {
+    using namespace pskel;
+    if (!t_dev || !out_dev || n < 0) {
+        set_error(PSKEL_ERR_ARG, "diag_sincos: bad arguments");
+        return PSKEL_ERR_ARG;
+    }
+    if (n == 0) return PSKEL_OK;
+    diag_sincos_kernel<<<(n + 255) / 256, 256>>>(t_dev, n, out_dev);
+    PSKEL_LAUNCHED(1);
+    return PSKEL_OK;
+}

@@ -86,7 +86,7 @@ int upload_ids(LegacyCtx &c, const double *const *lists, const int *lens, int nl
 int fill_jobs(LegacyCtx &c, const std::vector<FillJob> &jobs, double k, double eta,
               double r_near) {
     int tm, tn;
-    fill_tile_shape(PSKEL_C128, 1, 1, &tm, &tn);
+    fill_tile_shape(PSKEL_C128, 1, 0, &tm, &tn);
     std::vector<int> prefix(jobs.size() + 1, 0);
     for (size_t i = 0; i < jobs.size(); ++i)
         prefix[i + 1] = prefix[i] + ((jobs[i].nr + tm - 1) / tm) * ((jobs[i].nc + tn - 1) / tn);
@@ -103,7 +103,7 @@ int fill_jobs(LegacyCtx &c, const std::vector<FillJob> &jobs, double k, double e
     p.r_near = r_near;
     p.q_test = p.q_src = 1;
     p.precision = PSKEL_C128;
-    p.split = 1;
+    p.split = 0;
     return launch_fill(c.mesh, p, d_jobs, d_prefix, (int)jobs.size(), prefix.back(),
                        c.flags.as<int>(), c.stream);
 }

@@ -87,6 +87,7 @@ SIGNATURES = {
     "pskel_kernel_launches": (ctypes.c_longlong, []),
     "pskel_fma_peak": (ci, [D, D]),
     "pskel_pinv_noalloc": (ci, [VP, ci, ci, cd, ci, VP, VP, VP, VP]),
+    "pskel_diag_sincos": (ci, [VP, ci, VP]),
 }
 
 _LIB = None

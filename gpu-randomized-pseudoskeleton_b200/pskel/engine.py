@@ -154,8 +154,9 @@ class Engine:
         _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
         return err
 
-    def set_fill_split(self, split_c128: int = 0, split_c64: int = 0):
-        """Fill-kernel variant (lanes per entry: 1, 2 or 4; 0 = unchanged)."""
+    def set_fill_split(self, split_c128: int = -1, split_c64: int = -1):
+        """Fill-kernel variant: 0 two rows per thread (default), 1/2/4 lanes per entry with a
+        shuffle reduction, -1 unchanged."""
         _lib.check(self._lib.pskel_set_fill_split(self._h, int(split_c128), int(split_c64)))
 
     def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,

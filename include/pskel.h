@@ -239,8 +239,9 @@ int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
                     int *I, int *J);
 
-/* Fill-kernel variant used by this context: lanes per matrix entry (1, 2 or 4) for the
-   complex128 and complex64 fills (0 keeps the current choice). Set by the autotuner. */
+/* Fill-kernel variant used by this context for the complex128 and complex64 fills: 0 = two
+   matrix rows per thread (default), 1, 2 or 4 = lanes per matrix entry with a warp-shuffle
+   reduction over the quadrature points, -1 = keep the current choice. Set by the autotuner. */
 int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
 
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
@@ -275,6 +276,11 @@ int pskel_mlp_adam(float *params, const float *grad, float *m, float *v, int t, 
    sweeps did not converge. */
 int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau, int relative,
                        pskel_c128 *P, double *sigma, int *rank, void *stream);
+
+/* Diagnostics: for n phases t (DEVICE array, in wavelengths) writes 6 values per phase to
+   out: the fill kernels' own sin(2 pi t), cos(2 pi t) in FP64, the same in FP32, and CUDA's
+   sincospi(2 t) for comparison. Runs on the legacy default stream. No reference counterpart. */
+int pskel_diag_sincos(const double *t, int n, double *out);
 
 /* Device kernels launched by this library since load (graph replays count their kernel
    nodes); used to report how many of the library's kernels ran in a timed region. */
