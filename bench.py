@@ -243,10 +243,20 @@ def run_ours(args, rank, world, dev):
         ms, st, launches, times = timed(step, args.steps, args.warmup)
     clocks = clk.summary()
     tinfo = eng.timing()
-    # plain FP64 GPU pseudoskeleton (the drop-in baseline), same blocks and estimator
+    # plain FP64 GPU pseudoskeleton (the drop-in baseline): start at min(m,n)/10 and double,
+    # driven one block at a time as the reference's drivers call its GPU CUR; same kernels,
+    # samples and estimator as the batched modes
+    plain_pb = lambda: eng.compress(TOL, per_block=True, **PLAIN)
+    plain_ms, _, _, _ = timed(plain_pb, 1, 1)
+    # ablations, all blocks batched per round: plain FP64, mixed precision only, learned only
     plain = lambda: eng.compress(TOL, **PLAIN)
-    plain_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
+    plain_b_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
     t_plain = eng.timing()
+    mixed_only = lambda: eng.compress(TOL, **dict(PLAIN, precision="c64"))
+    mixed_ms, _, _, _ = timed(mixed_only, 1, 1)
+    learned_only = lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
+                                        **dict(PRODUCT, precision="c128"))
+    learned_ms, _, _, _ = timed(learned_only, 1, 2)
     # per-phase timing of the product without the graph (roofline of the fill)
     r0 = predict_r0()
     st_np = eng.compress(TOL, r0=r0, use_graph=False, **PRODUCT)
@@ -280,6 +290,11 @@ def run_ours(args, rank, world, dev):
                     pinv_tau_relative=PRODUCT["tau"], estimator="16 extra rows + 16 extra columns, safety 2",
                     l2="512 MB write before every timed step (inputs also exceed L2)"),
         plain_ms=round(plain_ms, 3), speedup_vs_plain=round(plain_ms / ms, 3),
+        plain_desc="plain FP64 GPU pseudoskeleton: start min(m,n)/10, doubling, same estimator, "
+                   "driven one block at a time (the reference's per-block driving)",
+        ablation_ms=dict(plain_batched=round(plain_b_ms, 3), mixed_batched=round(mixed_ms, 3),
+                         learned_batched=round(learned_ms, 3), learned_mixed_batched=round(ms, 3)),
+        speedup_vs_plain_batched=round(plain_b_ms / ms, 3),
         step_times_ms=[round(t, 3) for t in times],
         phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},
         product=dict(r_mean=float(st["r"].mean()), rounds_mean=float(st["rounds"].mean()),

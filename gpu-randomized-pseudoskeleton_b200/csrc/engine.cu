@@ -756,15 +756,15 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         else r = D < 10 ? 1 : D / 10;
         r_cur[b] = std::max(1, std::min(r, D));
     }
-    std::vector<int> active(nb);
-    std::iota(active.begin(), active.end(), 0);
     std::vector<int> rounds_used(nb, 0);
     cudaEvent_t t0, t1;
     PSKEL_CUDA(cudaEventCreate(&t0));
     PSKEL_CUDA(cudaEventCreate(&t1));
     PSKEL_CUDA(cudaEventRecord(t0, c->stream));
-    int round = 0;
     std::vector<RoundOut> hout;
+    // rounds of an active set until every block of it is done
+    auto run_rounds = [&](std::vector<int> active, bool allow_graph) -> int {
+    int round = 0;
     while (!active.empty()) {
         RoundPlan p;
         p.round = round;
@@ -791,7 +791,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             c->timing[9] += 1;
         }
         // graph of the first round: key = the sample counts and options that shape it
-        bool try_graph = o.use_graph && round == 0;
+        bool try_graph = allow_graph && o.use_graph && round == 0;
         std::vector<int> key;
         if (try_graph) {
             key = p.r;
@@ -884,6 +884,17 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         }
         active.swap(next);
         ++round;
+    }
+    return PSKEL_OK;
+    };
+    if (o.per_block) {
+        for (int b = 0; b < nb; ++b) PSKEL_TRY(run_rounds(std::vector<int>{b}, false));
+        // each block reused the round arenas: only the last block's factors are still there
+        for (int b = 0; b + 1 < nb; ++b) c->results[b].arena = -1;
+    } else {
+        std::vector<int> all(nb);
+        std::iota(all.begin(), all.end(), 0);
+        PSKEL_TRY(run_rounds(all, true));
     }
     PSKEL_CUDA(cudaEventRecord(t1, c->stream));
     PSKEL_CUDA(cudaEventSynchronize(t1));
@@ -989,6 +1000,12 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         return PSKEL_ERR_ARG;
     }
     const int nb = c->n_blocks;
+    for (int b = 0; b < nb; ++b)
+        if (c->results[b].arena < 0) {
+            set_error(PSKEL_ERR_STATE, "true_errors: block %d has no retained factors (run the "
+                                       "batched mode to keep every block)", b);
+            return PSKEL_ERR_STATE;
+        }
     const bool f32 = c->precision == PSKEL_C64;
     const size_t budget = (size_t)1 << 28;  // complex elements of dense blocks per batch
     int b0 = 0;

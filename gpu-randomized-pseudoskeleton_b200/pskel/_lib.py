@@ -41,7 +41,8 @@ class Opts(ctypes.Structure):
     _fields_ = [("tol", cd), ("tau", cd), ("tau_relative", ci), ("precision", ci),
                 ("start", ci), ("oversample", ci), ("extra_rows", ci), ("extra_cols", ci),
                 ("max_rounds", ci), ("recompress", ci), ("seed", ctypes.c_uint64),
-                ("recompress_tol", cd), ("est_safety", cd), ("use_graph", ci)]
+                ("recompress_tol", cd), ("est_safety", cd), ("use_graph", ci),
+                ("per_block", ci)]
 
 
 class BlockStat(ctypes.Structure):

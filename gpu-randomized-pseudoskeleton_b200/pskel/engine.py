@@ -101,7 +101,7 @@ class Engine:
                  r0=None, oversample: int = 10, extra_rows: int = 16, extra_cols: int = 16,
                  est_safety: float = 2.0, max_rounds: int = 12, seed: int = 0,
                  use_graph: bool = False, recompress: bool = False,
-                 recompress_tol: float = 0.0) -> np.ndarray:
+                 recompress_tol: float = 0.0, per_block: bool = False) -> np.ndarray:
         """Compress every block; returns a structured array of per-block stats
         (m, n, r, rank, rank_recompressed, rounds, status, est)."""
         o = _lib.Opts(tol=tol, tau=tau, tau_relative=int(bool(tau_relative)),
@@ -111,7 +111,7 @@ class Engine:
                       extra_cols=int(extra_cols), max_rounds=int(max_rounds),
                       recompress=int(recompress), seed=int(seed),
                       recompress_tol=float(recompress_tol), est_safety=float(est_safety),
-                      use_graph=int(bool(use_graph)))
+                      use_graph=int(bool(use_graph)), per_block=int(bool(per_block)))
         nb = self.n_blocks
         stats = (_lib.BlockStat * nb)()
         if r0 is not None:

@@ -190,6 +190,11 @@ typedef struct {
     double recompress_tol; /* relative singular-value threshold of the recompression */
     double est_safety;   /* a block is accepted when est <= tol / est_safety (>= 1) */
     int use_graph;       /* 1: replay the first round from a CUDA graph captured on a repeat call */
+    int per_block;       /* 1: drive the blocks one at a time (each block's rounds synchronise
+                            with the host), the way the reference's drivers call its GPU CUR per
+                            block; the kernels, samples and results per block are those of the
+                            batched mode, but only the stats are kept (factors of the last block
+                            only) */
 } pskel_opts_t;
 
 /* Per-block outcome, filled by pskel_compress_blocks. */

@@ -19,6 +19,6 @@ def test_stat_layout_matches_c():
 
 
 def test_opts_layout():
-    # pskel_opts_t: 2 doubles, 8 ints, uint64, 2 doubles, int (+ tail padding)
+    # pskel_opts_t: 2 doubles, 8 ints, uint64, 2 doubles, 2 ints
     assert ctypes.sizeof(_lib.Opts) == 80
     assert ctypes.sizeof(_lib.EM) == 24
