@@ -333,11 +333,16 @@ struct pskel_ctx {
     int n_groups = 0, n_blocks = 0;
     std::vector<int> gptr, gids, gt, gs;
     DevBuf d_gids;
+    // triangle structure of the groups for the triangle-moment fill
+    std::vector<int> h_edges;            // T+, T-, v+, v- per RWG (0-based), host copy
+    std::vector<int> gtri_ptr;           // CSR offsets into gtri / (3x) gadj
+    DevBuf d_gtri, d_gadj;
+    bool use_tri = false;
     std::vector<RoundArena> arenas;
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;
-    int split[2] = {0, 0};  // fill variant (0: two rows per thread; 1, 2, 4: lanes per entry)
+    int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
     double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;
@@ -348,6 +353,16 @@ struct pskel_ctx {
 };
 
 namespace {
+
+// fill variant actually used for a precision: the triangle-moment kernel when asked for and
+// every group fits it, else the per-entry kernel (two rows per thread when 8 was asked for)
+bool tri_for(const pskel_ctx *c, int precision) {
+    return c->split[precision == PSKEL_C64 ? 1 : 0] == 8 && c->use_tri;
+}
+int entry_split_for(const pskel_ctx *c, int precision) {
+    const int s = c->split[precision == PSKEL_C64 ? 1 : 0];
+    return s == 8 ? 0 : s;
+}
 
 int ctx_ok(pskel_ctx *c) {
     if (!c) {
@@ -366,7 +381,9 @@ struct RoundPlan {
     int round = 0;
     // device table views (inside arena.tables)
     BlockWork *d_works = nullptr;
-    FillJob *d_fill = nullptr;
+    FillJob *d_fill = nullptr;            // per-entry fill jobs (groups too large for tri)
+    GroupFillJob *d_gfill = nullptr;      // triangle-moment fill jobs
+    bool tri = false;
     int *d_fill_prefix = nullptr;
     int fill_jobs = 0, fill_tiles = 0;
     SvdJob *d_svd = nullptr;
@@ -414,6 +431,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     std::vector<BlockWork> works(nb);
     std::vector<FillJob> fills;
     fills.reserve(2 * nb);
+    std::vector<GroupFillJob> gfills;
+    if (tri_for(c, o.precision)) gfills.reserve(2 * nb);
     std::vector<SvdJob> svds(nb);
     std::vector<PinvJob> pinvs(nb);
     char *kb = ar.keep.as<char>();
@@ -459,6 +478,16 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         // Rx = Z([I; Ix], group_s) filled as the transpose of Z(group_s, [I; Ix]) (the Galerkin
         // block is symmetric for equal test and source rules), so the long side is on rows
         fills.push_back(FillJob{w.cols_g, w.Ig, w.Rx, w.n, w.r + w.pe, w.r + w.pe, 1});
+        if (tri_for(c, o.precision)) {
+            const int gt = c->gt[b], gs = c->gs[b];
+            const int *tri = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
+            gfills.push_back(GroupFillJob{w.rows_g, tri + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
+                                          w.Jg, w.C, w.m, c->gtri_ptr[gt + 1] - c->gtri_ptr[gt],
+                                          w.r + w.pc, w.m, 0, 0});
+            gfills.push_back(GroupFillJob{w.cols_g, tri + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
+                                          w.Ig, w.Rx, w.n, c->gtri_ptr[gs + 1] - c->gtri_ptr[gs],
+                                          w.r + w.pe, w.r + w.pe, 1, 0});
+        }
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, o.tau, o.tau_relative};
         max_pinv_tiles = std::max(max_pinv_tiles, ((w.r + 31) / 32) * ((w.r + 31) / 32));
@@ -477,10 +506,16 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     }
     // fill tile prefix
     int tm, tn;
-    fill_tile_shape(o.precision, c->em.q_test, c->split[o.precision == PSKEL_C64 ? 1 : 0], &tm, &tn);
+    fill_tile_shape(o.precision, c->em.q_test, entry_split_for(c, o.precision), &tm, &tn);
+    p.tri = tri_for(c, o.precision);
     std::vector<int> prefix(fills.size() + 1, 0);
-    for (size_t i = 0; i < fills.size(); ++i)
-        prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
+    if (p.tri) {
+        for (size_t i = 0; i < gfills.size(); ++i)
+            prefix[i + 1] = prefix[i] + (gfills[i].nc + kTriFillCols - 1) / kTriFillCols;
+    } else {
+        for (size_t i = 0; i < fills.size(); ++i)
+            prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
+    }
     std::vector<int> svd_idx;
     PSKEL_TRY(svd_plan(svds, svd_idx, &p.n_res, &p.max_res_smem));
     p.n_blk = nb - p.n_res;
@@ -488,14 +523,18 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     size_t t = 0;
     auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
     const size_t o_works = slot(sizeof(BlockWork) * nb);
-    const size_t o_fill = slot(sizeof(FillJob) * fills.size());
+    const size_t o_fill = p.tri ? slot(sizeof(GroupFillJob) * gfills.size())
+                                : slot(sizeof(FillJob) * fills.size());
     const size_t o_pref = slot(sizeof(int) * prefix.size());
     const size_t o_svd = slot(sizeof(SvdJob) * nb);
     const size_t o_idx = slot(sizeof(int) * nb);
     const size_t o_pinv = slot(sizeof(PinvJob) * nb);
     ar.h_tables.assign(t, 0);
     std::memcpy(ar.h_tables.data() + o_works, works.data(), sizeof(BlockWork) * nb);
-    std::memcpy(ar.h_tables.data() + o_fill, fills.data(), sizeof(FillJob) * fills.size());
+    if (p.tri)
+        std::memcpy(ar.h_tables.data() + o_fill, gfills.data(), sizeof(GroupFillJob) * gfills.size());
+    else
+        std::memcpy(ar.h_tables.data() + o_fill, fills.data(), sizeof(FillJob) * fills.size());
     std::memcpy(ar.h_tables.data() + o_pref, prefix.data(), sizeof(int) * prefix.size());
     std::memcpy(ar.h_tables.data() + o_svd, svds.data(), sizeof(SvdJob) * nb);
     std::memcpy(ar.h_tables.data() + o_idx, svd_idx.data(), sizeof(int) * nb);
@@ -506,6 +545,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     char *d = ar.tables.as<char>();
     p.d_works = reinterpret_cast<BlockWork *>(d + o_works);
     p.d_fill = reinterpret_cast<FillJob *>(d + o_fill);
+    p.d_gfill = reinterpret_cast<GroupFillJob *>(d + o_fill);
     p.d_fill_prefix = reinterpret_cast<int *>(d + o_pref);
     p.fill_jobs = (int)fills.size();
     p.fill_tiles = prefix.back();
@@ -530,9 +570,13 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.q_test = c->em.q_test;
     fp.q_src = c->em.q_src;
     fp.precision = o.precision;
-    fp.split = c->split[o.precision == PSKEL_C64 ? 1 : 0];
-    PSKEL_TRY(launch_fill(c->mesh, fp, p.d_fill, p.d_fill_prefix, p.fill_jobs, p.fill_tiles,
-                          c->flags.as<int>(), s));
+    fp.split = entry_split_for(c, o.precision);
+    if (p.tri)
+        PSKEL_TRY(launch_tri_fill(c->mesh, fp, p.d_gfill, p.d_fill_prefix, p.fill_jobs,
+                                  p.fill_tiles, s));
+    else
+        PSKEL_TRY(launch_fill(c->mesh, fp, p.d_fill, p.d_fill_prefix, p.fill_jobs, p.fill_tiles,
+                              c->flags.as<int>(), s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
     if (o.precision == PSKEL_C64)
         gather_core_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_works);
@@ -630,6 +674,8 @@ extern "C" int pskel_upload_mesh(pskel_ctx *c, const double *vertex, int nv, con
         set_error(PSKEL_ERR_RANGE, "mesh: triangle or vertex id out of range");
         return PSKEL_ERR_RANGE;
     }
+    c->h_edges.resize(4 * (size_t)ne);
+    for (size_t i = 0; i < 4 * (size_t)ne; ++i) c->h_edges[i] = (int)edges[i] - 1;
     c->em = *em;
     c->have_mesh = true;
     if (c->graph) {
@@ -653,7 +699,7 @@ extern "C" int pskel_fill_device(pskel_ctx *c, const int *rows_dev, int nr, cons
     }
     if ((size_t)nr * nc == 0) return PSKEL_OK;
     int tm, tn;
-    fill_tile_shape(precision, c->em.q_test, c->split[precision == PSKEL_C64 ? 1 : 0], &tm, &tn);
+    fill_tile_shape(precision, c->em.q_test, entry_split_for(c, precision), &tm, &tn);
     FillJob job{rows_dev, cols_dev, Z_dev, nr, nc, ld, 0};
     int prefix[2] = {0, ((nr + tm - 1) / tm) * ((nc + tn - 1) / tn)};
     PSKEL_TRY(c->tmp3.reserve(512));
@@ -667,7 +713,7 @@ extern "C" int pskel_fill_device(pskel_ctx *c, const int *rows_dev, int nr, cons
     fp.q_test = c->em.q_test;
     fp.q_src = c->em.q_src;
     fp.precision = precision;
-    fp.split = c->split[precision == PSKEL_C64 ? 1 : 0];
+    fp.split = entry_split_for(c, precision);
     return launch_fill(c->mesh, fp, c->tmp3.as<FillJob>(),
                        reinterpret_cast<int *>(c->tmp3.as<char>() + 256), 1, prefix[1],
                        c->flags.as<int>(), c->stream);
@@ -712,6 +758,48 @@ extern "C" int pskel_set_blocks(pskel_ctx *c, const int *group_ptr, const int *g
     PSKEL_TRY(c->d_gids.reserve(sizeof(int) * nids));
     PSKEL_CUDA(cudaMemcpyAsync(c->d_gids.ptr, group_ids, sizeof(int) * nids, cudaMemcpyHostToDevice,
                                c->stream));
+    // triangles of each group and, per triangle, the (local RWG, side) pairs that use it
+    {
+        std::vector<int> tri, adj;
+        c->gtri_ptr.assign(n_groups + 1, 0);
+        int max_rows = 0;
+        std::vector<int> local(c->mesh.nt, -1);
+        for (int g = 0; g < n_groups; ++g) {
+            const int b0 = group_ptr[g], b1 = group_ptr[g + 1];
+            max_rows = std::max(max_rows, b1 - b0);
+            const size_t t0 = tri.size();
+            for (int i = b0; i < b1; ++i)
+                for (int side = 0; side < 2; ++side) {
+                    const int t = c->h_edges[4 * (size_t)group_ids[i] + side];
+                    if (t < 0 || t >= c->mesh.nt) {
+                        set_error(PSKEL_ERR_RANGE, "edges: triangle id out of range");
+                        return PSKEL_ERR_RANGE;
+                    }
+                    if (local[t] < 0) {
+                        local[t] = (int)(tri.size() - t0);
+                        tri.push_back(t);
+                        adj.insert(adj.end(), {-1, -1, -1});
+                    }
+                    int *a = &adj[3 * (t0 + local[t])];
+                    int u = 0;
+                    while (u < 3 && a[u] >= 0) ++u;
+                    if (u == 3) {
+                        set_error(PSKEL_ERR_ARG, "triangle %d is used by more than three RWG", t);
+                        return PSKEL_ERR_ARG;
+                    }
+                    a[u] = 2 * (i - b0) + side;
+                }
+            for (size_t q = t0; q < tri.size(); ++q) local[tri[q]] = -1;
+            c->gtri_ptr[g + 1] = (int)tri.size();
+        }
+        c->use_tri = max_rows <= kTriFillMaxRows;
+        PSKEL_TRY(c->d_gtri.reserve(sizeof(int) * (tri.size() + 1)));
+        PSKEL_TRY(c->d_gadj.reserve(sizeof(int) * (adj.size() + 1)));
+        PSKEL_CUDA(cudaMemcpyAsync(c->d_gtri.ptr, tri.data(), sizeof(int) * tri.size(),
+                                   cudaMemcpyHostToDevice, c->stream));
+        PSKEL_CUDA(cudaMemcpyAsync(c->d_gadj.ptr, adj.data(), sizeof(int) * adj.size(),
+                                   cudaMemcpyHostToDevice, c->stream));
+    }
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
     c->results.assign(n_blocks, BlockResult());
     if (c->graph) {
@@ -801,7 +889,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back(o.extra_cols);
             key.push_back((int)std::lround(std::log10(std::max(o.tau, 1e-300)) * 1000));
             key.push_back(o.tau_relative);
-            key.push_back(c->split[0] * 8 + c->split[1]);
+            key.push_back(c->split[0] * 8 + c->split[1] + (c->use_tri ? 1000 : 0));
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -931,9 +1019,9 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
 
 extern "C" int pskel_set_fill_split(pskel_ctx *c, int split_c128, int split_c64) {
     PSKEL_TRY(ctx_ok(c));
-    auto ok = [](int v) { return v == -1 || v == 0 || v == 1 || v == 2 || v == 4; };
+    auto ok = [](int v) { return v == -1 || v == 0 || v == 1 || v == 2 || v == 4 || v == 8; };
     if (!ok(split_c128) || !ok(split_c64)) {
-        set_error(PSKEL_ERR_ARG, "fill variant must be -1 (unchanged), 0, 1, 2 or 4");
+        set_error(PSKEL_ERR_ARG, "fill variant must be -1 (unchanged), 0, 1, 2, 4 or 8");
         return PSKEL_ERR_ARG;
     }
     if (split_c128 >= 0) c->split[0] = split_c128;
@@ -1027,12 +1115,14 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         double2 *Zb = c->tmp.as<double2>();
         double2 *Wb = Zb + dense;
         std::vector<FillJob> fills(nbb);
+        std::vector<GroupFillJob> gfills(nbb);
         std::vector<ZgemmJob> g1, g2;
         std::vector<const double2 *> mats(nbb);
         std::vector<long long> sizes(nbb);
         size_t zo = 0, wo = 0;
         int tm, tn;
-        fill_tile_shape(PSKEL_C128, c->em.q_test, c->split[0], &tm, &tn);
+        fill_tile_shape(PSKEL_C128, c->em.q_test, entry_split_for(c, PSKEL_C128), &tm, &tn);
+        const bool tri = tri_for(c, PSKEL_C128);
         std::vector<int> prefix(nbb + 1, 0);
         for (int i = 0; i < nbb; ++i) {
             const int b = b0 + i;
@@ -1041,7 +1131,14 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
             double2 *Z = Zb + zo;
             fills[i] = FillJob{c->d_gids.as<int>() + c->gptr[c->gt[b]],
                                c->d_gids.as<int>() + c->gptr[c->gs[b]], Z, res.m, res.n, res.m, 0};
-            prefix[i + 1] = prefix[i] + ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn);
+            const int gt = c->gt[b];
+            gfills[i] = GroupFillJob{c->d_gids.as<int>() + c->gptr[gt],
+                                     c->d_gtri.as<int>() + c->gtri_ptr[gt],
+                                     c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt],
+                                     c->d_gids.as<int>() + c->gptr[c->gs[b]], Z, res.m,
+                                     c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], res.n, res.m, 0, 0};
+            prefix[i + 1] = prefix[i] + (tri ? (res.n + kTriFillCols - 1) / kTriFillCols
+                                                     : ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn));
             mats[i] = Z;
             sizes[i] = (long long)res.m * res.n;
             const double2 *Cd;
@@ -1076,7 +1173,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         }
         PSKEL_CUDA(cudaGetLastError());
         // dense FP64 fill of the batch
-        const size_t jb = sizeof(FillJob) * nbb;
+        const size_t jb = std::max(sizeof(FillJob), sizeof(GroupFillJob)) * nbb;
         PSKEL_TRY(c->tmp2.reserve(jb + sizeof(int) * (nbb + 1) + sizeof(void *) * nbb +
                                   sizeof(long long) * nbb + sizeof(double) * 2 * nbb + 8 * 256));
         char *d = c->tmp2.as<char>();
@@ -1088,7 +1185,12 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         long long *d_s = reinterpret_cast<long long *>(slot(sizeof(long long) * nbb));
         double *d_nz = reinterpret_cast<double *>(slot(sizeof(double) * nbb));
         double *d_ne = reinterpret_cast<double *>(slot(sizeof(double) * nbb));
-        PSKEL_CUDA(cudaMemcpyAsync(d_f, fills.data(), jb, cudaMemcpyHostToDevice, c->stream));
+        if (tri)
+            PSKEL_CUDA(cudaMemcpyAsync(d_f, gfills.data(), sizeof(GroupFillJob) * nbb,
+                                       cudaMemcpyHostToDevice, c->stream));
+        else
+            PSKEL_CUDA(cudaMemcpyAsync(d_f, fills.data(), sizeof(FillJob) * nbb,
+                                       cudaMemcpyHostToDevice, c->stream));
         PSKEL_CUDA(cudaMemcpyAsync(d_p, prefix.data(), sizeof(int) * (nbb + 1), cudaMemcpyHostToDevice, c->stream));
         PSKEL_CUDA(cudaMemcpyAsync(d_m, mats.data(), sizeof(void *) * nbb, cudaMemcpyHostToDevice, c->stream));
         PSKEL_CUDA(cudaMemcpyAsync(d_s, sizes.data(), sizeof(long long) * nbb, cudaMemcpyHostToDevice, c->stream));
@@ -1099,8 +1201,12 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         fp.q_test = c->em.q_test;
         fp.q_src = c->em.q_src;
         fp.precision = PSKEL_C128;
-        fp.split = c->split[0];
-        PSKEL_TRY(launch_fill(c->mesh, fp, d_f, d_p, nbb, prefix.back(), c->flags.as<int>(), c->stream));
+        fp.split = entry_split_for(c, PSKEL_C128);
+        if (tri)
+            PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d_f), d_p, nbb,
+                                      prefix.back(), c->stream));
+        else
+            PSKEL_TRY(launch_fill(c->mesh, fp, d_f, d_p, nbb, prefix.back(), c->flags.as<int>(), c->stream));
         block_norm_kernel<<<nbb, 256, 0, c->stream>>>(d_m, d_s, d_nz);
         PSKEL_LAUNCHED(1);
         PSKEL_TRY(launch_zgemm(g1, c->stream, c->tmp3));

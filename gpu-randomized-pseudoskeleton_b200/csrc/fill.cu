@@ -533,6 +533,214 @@ int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
 #undef PSKEL_FILL_CASE
 }
 
+// ============================================================ triangle-moment fill
+// Z(group, cols) for a group of RWG functions with a known triangle list. For far interactions
+// every point pair costs the same Green's function evaluation whichever RWG it is weighted for,
+// and the RWG functions of a group share their triangles (about 2.5 RWG references per
+// triangle on a closed surface). So G is evaluated once per (triangle t of the group, column
+// RWG n) over the Q x 2Q point pairs and reduced to five moments, in coordinates local to the
+// centroid c_t of t (x' = x - c_t) so that nothing cancels in FP32:
+//     A0 = sum_p w_p S0_p,  Bx = sum_p w_p x'_p . S1_p,  Cv = sum_p w_p S1_p,
+//     S0_p = sum_q G(x_p, y_q) e_q,  S1_p = sum_q G(x_p, y_q) v_q   (e, v: source record d, u)
+// and each RWG m of the group that uses t as its side a (sign s_a, free vertex v_a, length l_m)
+// receives   s_a l_m [ A0 / k - (k/2) (Bx - (v_a - c_t) . Cv) ],
+// which is the per-entry sum sum_p sum_q G [d_p e_q / k - k u_p . v_q] regrouped. A CTA owns one
+// job and kTriFillCols columns: it stages the column records, loops over (triangle, column)
+// items, scatters the two to three contributions of each item into a shared-memory tile of the
+// block (shared-memory atomics; each entry receives exactly two) and writes the tile once.
+// Weights of the rule by point class: the centroid (point 0) and the two orbits of three
+// points (1-3, 4-6) of the 7-point rule; Q = 1 uses w0 = 1.
+struct TriWeights {
+    double w0, w1, w2;
+};
+
+template <typename T, int Q, int TN>
+__global__ void __launch_bounds__(256, 2)
+    tri_fill_kernel(const double *__restrict__ tri_rec, const double *__restrict__ rec_s,
+                    const double *__restrict__ edges, const double *__restrict__ vertex,
+                    const double *__restrict__ ln, const GroupFillJob *__restrict__ jobs,
+                    const int *__restrict__ tile_prefix, int njobs, int total_tiles, T k,
+                    T kinv, double kturn, T scale, TriWeights wq) {
+    constexpr int NP = 2 * Q;
+    constexpr int RS = (7 * NP) | 1;
+    constexpr int TS = tri_stride(Q);
+    using C2 = typename Cplx<T>::type;
+    using T4 = typename Vec4<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double2 *s_xy = reinterpret_cast<double2 *>(smem_raw);   // TN x NP
+    double *s_z = reinterpret_cast<double *>(s_xy + TN * NP);  // TN x NP
+    T4 *s_v = reinterpret_cast<T4 *>(s_z + TN * NP);           // TN x NP
+    T *zs = reinterpret_cast<T *>(s_v + TN * NP);              // 2 x kTriFillMaxRows x TN
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const int jb = find_job(tile_prefix, njobs, tile);
+        const GroupFillJob job = jobs[jb];
+        const int j0 = (tile - tile_prefix[jb]) * TN;
+        for (int idx = threadIdx.x; idx < TN * NP; idx += blockDim.x) {
+            const int c = idx / NP, q = idx - c * NP;
+            const int col = j0 + c;
+            const bool ok = col < job.nc;
+            const double *src = rec_s + (size_t)(ok ? job.cols[col] : 0) * RS;
+            s_xy[idx] = make_double2(ok ? src[q] : 0.0, ok ? src[NP + q] : 0.0);
+            s_z[idx] = ok ? src[2 * NP + q] : 0.0;
+            T4 v;
+            v.x = ok ? (T)src[3 * NP + q] : T(0);
+            v.y = ok ? (T)src[4 * NP + q] : T(0);
+            v.z = ok ? (T)src[5 * NP + q] : T(0);
+            v.w = ok ? (T)src[6 * NP + q] : T(0);
+            s_v[idx] = v;
+        }
+        for (int idx = threadIdx.x; idx < 2 * job.m * TN; idx += blockDim.x) zs[idx] = T(0);
+        __syncthreads();
+
+        const int items = job.nt * TN;
+        for (int it = threadIdx.x; it < items; it += blockDim.x) {
+            const int t = it % job.nt, j = it / job.nt;
+            if (j0 + j >= job.nc) continue;
+            const double *tr = tri_rec + (size_t)job.tris[t] * TS;
+            const double cx = tr[3 * Q], cy = tr[3 * Q + 1], cz = tr[3 * Q + 2];
+            const double2 *sxy = s_xy + j * NP;
+            const double *sz = s_z + j * NP;
+            const T4 *sv = s_v + j * NP;
+            T a0r = 0, a0i = 0, bxr = 0, bxi = 0;
+            T cvr[3] = {0, 0, 0}, cvi[3] = {0, 0, 0};
+#pragma unroll 1
+            for (int p = 0; p < Q; ++p) {
+                const double x = tr[3 * p], y = tr[3 * p + 1], z = tr[3 * p + 2];
+                T s0r = 0, s0i = 0, s1r[3] = {0, 0, 0}, s1i[3] = {0, 0, 0};
+#pragma unroll 2
+                for (int q = 0; q < NP; ++q) {
+                    const double2 xy = sxy[q];
+                    const double dx = x - xy.x, dy = y - xy.y, dz = z - sz[q];
+                    const double R2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                    T rinv, sn, cs;
+                    int quad;
+                    if constexpr (sizeof(T) == 8) {
+                        rinv = rsqrt(R2);
+                        const double g = split_quarter(R2 * rinv * kturn, &quad);
+                        sincos_2pi(g, quad, &sn, &cs);
+                    } else {
+                        const float yy = rsqrtf((float)R2);
+                        const double yd = (double)yy;
+                        const double R0 = R2 * yd;
+                        const double R = fma(fma(-R0, R0, R2), 0.5 * yd, R0);
+                        const double g = split_quarter(R * kturn, &quad);
+                        sincos_2pi((float)g, quad, &sn, &cs);
+                        rinv = yy;
+                    }
+                    const T gr = rinv * sn, gi = rinv * cs;  // G = (sin kR + j cos kR) / R
+                    const T4 v = sv[q];
+                    s0r = fma(gr, v.w, s0r);
+                    s0i = fma(gi, v.w, s0i);
+                    s1r[0] = fma(gr, v.x, s1r[0]);
+                    s1i[0] = fma(gi, v.x, s1i[0]);
+                    s1r[1] = fma(gr, v.y, s1r[1]);
+                    s1i[1] = fma(gi, v.y, s1i[1]);
+                    s1r[2] = fma(gr, v.z, s1r[2]);
+                    s1i[2] = fma(gi, v.z, s1i[2]);
+                }
+                const T w = (T)(p == 0 ? wq.w0 : (p < 4 ? wq.w1 : wq.w2));
+                const T xl[3] = {(T)(x - cx), (T)(y - cy), (T)(z - cz)};
+                a0r = fma(w, s0r, a0r);
+                a0i = fma(w, s0i, a0i);
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    cvr[d] = fma(w, s1r[d], cvr[d]);
+                    cvi[d] = fma(w, s1i[d], cvi[d]);
+                    bxr = fma(w * xl[d], s1r[d], bxr);
+                    bxi = fma(w * xl[d], s1i[d], bxi);
+                }
+            }
+            const int *ad = job.adj + 3 * t;
+#pragma unroll
+            for (int u = 0; u < 3; ++u) {
+                const int a = ad[u];
+                if (a < 0) continue;
+                const int ml = a >> 1, side = a & 1;
+                const int e = job.rows[ml];
+                const int vo = (int)edges[4 * (size_t)e + 2 + side] - 1;
+                const T vl[3] = {(T)(vertex[3 * (size_t)vo] - cx), (T)(vertex[3 * (size_t)vo + 1] - cy),
+                                 (T)(vertex[3 * (size_t)vo + 2] - cz)};
+                const T sl = (side ? -1 : 1) * (T)ln[e];
+                const T hk = (T)0.5 * k;
+                T br = bxr, bi = bxi;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    br = fma(-vl[d], cvr[d], br);
+                    bi = fma(-vl[d], cvi[d], bi);
+                }
+                const T vr = sl * fma(a0r, kinv, -hk * br);
+                const T vi = sl * fma(a0i, kinv, -hk * bi);
+                atomicAdd(&zs[2 * (ml + j * job.m)], vr);
+                atomicAdd(&zs[2 * (ml + j * job.m) + 1], vi);
+            }
+        }
+        __syncthreads();
+        C2 *out = reinterpret_cast<C2 *>(job.out);
+        for (int idx = threadIdx.x; idx < job.m * TN; idx += blockDim.x) {
+            const int i = idx % job.m, j = idx / job.m;
+            if (j0 + j >= job.nc) continue;
+            C2 z;
+            z.x = scale * zs[2 * idx];
+            z.y = scale * zs[2 * idx + 1];
+            if (!job.trans) out[i + (size_t)(j0 + j) * job.ld] = z;
+            else out[(j0 + j) + (size_t)i * job.ld] = z;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T, int Q>
+static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillParams &p,
+                        const GroupFillJob *d_jobs, const int *d_prefix, int njobs,
+                        int total_tiles, cudaStream_t stream) {
+    constexpr int NP = 2 * Q;
+    constexpr int TN = kTriFillCols;
+    const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
+                        2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
+    auto kern = tri_fill_kernel<T, Q, TN>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    int per_sm = 0;
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    if (per_sm < 1) per_sm = 1;
+    long long grid = (long long)sm_count() * per_sm;
+    if (grid > total_tiles) grid = total_tiles;
+    if (grid < 1) return PSKEL_OK;
+    double wall[7];
+    quadrature_weights(Q, wall);
+    TriWeights w{wall[0], Q == 7 ? wall[1] : 0.0, Q == 7 ? wall[4] : 0.0};
+    const double pi = 3.14159265358979323846;
+    kern<<<(int)grid, 256, smem, stream>>>(
+        rec.tri.as<double>(), rec.f64.as<double>(), mesh.edges.as<double>(),
+        mesh.vertex.as<double>(), mesh.ln.as<double>(), d_jobs, d_prefix, njobs, total_tiles,
+        (T)p.k, (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)), w);
+    PSKEL_LAUNCHED(1);
+    return PSKEL_OK;
+}
+
+int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob *d_jobs,
+                    const int *d_tile_prefix, int njobs, int total_tiles, cudaStream_t stream) {
+    if (total_tiles <= 0 || njobs <= 0) return PSKEL_OK;
+    if (p.q_test != p.q_src || (p.q_test != 1 && p.q_test != 7)) {
+        set_error(PSKEL_ERR_ARG, "tri fill: q_test and q_src must both be 1 or both be 7");
+        return PSKEL_ERR_ARG;
+    }
+    const MeshRecords &rec = const_cast<DevMesh &>(mesh).records(p.q_test);
+    if (rec.q != p.q_test) {
+        set_error(PSKEL_ERR_STATE, "tri fill: records for Q=%d not built", p.q_test);
+        return PSKEL_ERR_STATE;
+    }
+    if (p.precision == PSKEL_C128)
+        return p.q_test == 7 ? launch_tri_t<double, 7>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
+                             : launch_tri_t<double, 1>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream);
+    return p.q_test == 7 ? launch_tri_t<float, 7>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
+                         : launch_tri_t<float, 1>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream);
+}
+
 // ---------------------------------------------------------------- diagnostics
 // The fill's sin/cos of 2 pi t next to CUDA's sincospi(2 t), for tests of the polynomial.
 __global__ void diag_sincos_kernel(const double *t, int n, double *out) {

@@ -62,6 +62,15 @@ static Rule7 make_rule7() {
     return r;
 }
 
+void quadrature_weights(int q, double *w) {
+    if (q == 1) {
+        w[0] = 1.0;
+        return;
+    }
+    static const Rule7 r7 = make_rule7();
+    for (int i = 0; i < 7; ++i) w[i] = r7.w[i];
+}
+
 struct RuleArg {
     double a[7], b[7], c[7], w[7];
 };
@@ -121,6 +130,32 @@ __global__ void build_records_kernel(const double *__restrict__ vertex,
     if (pp == 0) r64[stride - 1] = 0.0;
 }
 
+// One thread per triangle: its q quadrature points and centroid (q = 1 uses the stored centroid
+// as its point, like the per-RWG records).
+__global__ void build_tri_records_kernel(const double *__restrict__ vertex,
+                                         const double *__restrict__ topol,
+                                         const double *__restrict__ cent, int nt, int nv, int q,
+                                         RuleArg rule, double *__restrict__ out, int *flags) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    double *o = out + (size_t)t * tri_stride(q);
+    const int v1 = (int)topol[3 * (size_t)t + 0] - 1;
+    const int v2 = (int)topol[3 * (size_t)t + 1] - 1;
+    const int v3 = (int)topol[3 * (size_t)t + 2] - 1;
+    const bool ok = v1 >= 0 && v1 < nv && v2 >= 0 && v2 < nv && v3 >= 0 && v3 < nv;
+    if (!ok) atomicOr(flags, 2);
+    for (int p = 0; p < q; ++p)
+        for (int d = 0; d < 3; ++d) {
+            double x = 0.0;
+            if (q == 1) x = cent[3 * (size_t)t + d];
+            else if (ok)
+                x = rule.a[p] * vertex[3 * (size_t)v1 + d] + rule.b[p] * vertex[3 * (size_t)v2 + d] +
+                    rule.c[p] * vertex[3 * (size_t)v3 + d];
+            o[3 * p + d] = x;
+        }
+    for (int d = 0; d < 3; ++d) o[3 * q + d] = cent[3 * (size_t)t + d];
+}
+
 int upload_mesh_arrays(DevMesh &mesh, const double *vertex, int nv, const double *topol, int nt,
                        const double *edges, int ne, const double *ln, const double *cent,
                        cudaStream_t stream) {
@@ -174,6 +209,11 @@ int build_records(DevMesh &mesh, int q, cudaStream_t stream, int *d_flag) {
         mesh.vertex.as<double>(), mesh.topol.as<double>(), mesh.edges.as<double>(),
         mesh.ln.as<double>(), mesh.cent.as<double>(), mesh.ne, mesh.nt, mesh.nv, q, ra,
         rec.f64.as<double>(), d_flag);
+    PSKEL_LAUNCHED(1);
+    PSKEL_TRY(rec.tri.reserve(sizeof(double) * (size_t)mesh.nt * tri_stride(q)));
+    build_tri_records_kernel<<<(mesh.nt + 255) / 256, 256, 0, stream>>>(
+        mesh.vertex.as<double>(), mesh.topol.as<double>(), mesh.cent.as<double>(), mesh.nt,
+        mesh.nv, q, ra, rec.tri.as<double>(), d_flag);
     PSKEL_LAUNCHED(1);
     rec.q = q;
     return PSKEL_OK;

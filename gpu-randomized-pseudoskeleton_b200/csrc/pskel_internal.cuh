@@ -72,7 +72,10 @@ __host__ __device__ constexpr int rec_stride(int q) { return (7 * 2 * q) | 1; }
 struct MeshRecords {
     int q = 0;
     DevBuf f64;  // ne * rec_stride(q) doubles
+    DevBuf tri;  // nt * tri_stride(q) doubles: the q points (x, y, z) of each triangle, then
+                 // its centroid (x, y, z)
 };
+__host__ __device__ constexpr int tri_stride(int q) { return 3 * (q + 1); }
 
 struct DevMesh {
     int ne = 0, nt = 0, nv = 0;
@@ -80,6 +83,9 @@ struct DevMesh {
     MeshRecords rec1, rec7;                 // Q = 1 and Q = 7 records (built on demand)
     MeshRecords &records(int q) { return q == 1 ? rec1 : rec7; }
 };
+
+// Weights of the q-point triangle rule (q = 1: {1}; q = 7: the 7-point rule), summing to 1.
+void quadrature_weights(int q, double *w);
 
 // Build (or rebuild) the Q-point records of a mesh whose raw arrays are on the device.
 int build_records(DevMesh &mesh, int q, cudaStream_t stream, int *d_flag);
@@ -116,6 +122,21 @@ int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
                 const int *d_tile_prefix, int njobs, int total_tiles, int *d_flags,
                 cudaStream_t stream);
 int fill_tile_shape(int precision, int q, int split, int *tm, int *tn);
+
+// Triangle-moment fill of Z(group, cols) for a group of RWG functions whose triangle list and
+// triangle -> (RWG, side) adjacency are known (see tri_fill_kernel in fill.cu).
+struct GroupFillJob {
+    const int *rows;  // global RWG ids of the group (m)
+    const int *tris;  // global triangle ids touched by the group (nt)
+    const int *adj;   // 3 per triangle: 2 * local RWG index + side (0: T+, 1: T-), or -1
+    const int *cols;  // global RWG ids of the columns (nc)
+    void *out;
+    int m, nt, nc, ld, trans, pad;
+};
+constexpr int kTriFillMaxRows = 512;  // largest group the triangle-moment fill accepts
+constexpr int kTriFillCols = 8;       // columns per CTA tile
+int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob *d_jobs,
+                    const int *d_tile_prefix, int njobs, int total_tiles, cudaStream_t stream);
 
 // Convert 1-based double ids to 0-based int32 with a range check (flags bit 1 on error).
 int launch_ids_from_double(const double *d_in, int *d_out, int n, int limit, int *d_flags,

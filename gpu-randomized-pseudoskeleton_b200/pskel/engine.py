@@ -155,8 +155,8 @@ class Engine:
         return err
 
     def set_fill_split(self, split_c128: int = -1, split_c64: int = -1):
-        """Fill-kernel variant: 0 two rows per thread (default), 1/2/4 lanes per entry with a
-        shuffle reduction, -1 unchanged."""
+        """Fill-kernel variant: 8 triangle moments (default), 0 two rows per thread, 1/2/4
+        lanes per entry with a shuffle reduction, -1 unchanged."""
         _lib.check(self._lib.pskel_set_fill_split(self._h, int(split_c128), int(split_c64)))
 
     def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,

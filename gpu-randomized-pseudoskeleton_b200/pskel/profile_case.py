@@ -4,9 +4,9 @@
 
 builds the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions, 0.5-lambda leaves), then
 makes CALLS (default 3) single-round compressions of every far block at a fixed sample count of
-24 with the given precision (c128 or c64) and fill variant (0: two rows per thread, the default;
-1, 2, 4: lanes per entry), printing the fill time and point-pair
-rate of each call. Under a profiler the fill launch of call i is the i-th fill_kernel launch.
+24 with the given precision (c128 or c64) and fill variant (8: triangle moments, the default;
+0: two rows per thread; 1, 2, 4: lanes per entry), printing the fill time and point-pair
+rate of each call. Under a profiler the fill launch of call i is the i-th launch of the chosen fill kernel.
 """
 from __future__ import annotations
 
@@ -26,7 +26,7 @@ from pskel.engine import Engine  # noqa: E402
 def main():
     prec = sys.argv[1] if len(sys.argv) > 1 else "c64"
     calls = int(sys.argv[2]) if len(sys.argv) > 2 else 3
-    split = int(sys.argv[3]) if len(sys.argv) > 3 else 0
+    split = int(sys.argv[3]) if len(sys.argv) > 3 else 8
     m = pmesh.icosphere(2.0, 4)
     part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
     with Engine() as eng:

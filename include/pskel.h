@@ -244,9 +244,11 @@ int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
                     int *I, int *J);
 
-/* Fill-kernel variant used by this context for the complex128 and complex64 fills: 0 = two
-   matrix rows per thread (default), 1, 2 or 4 = lanes per matrix entry with a warp-shuffle
-   reduction over the quadrature points, -1 = keep the current choice. Set by the autotuner. */
+/* Fill-kernel variant used by this context for the complex128 and complex64 fills:
+   8 = triangle-moment kernel (default; used when every group has at most 512 RWG, else 0),
+   0 = per-entry kernel with two matrix rows per thread, 1, 2 or 4 = per-entry kernel with that
+   many lanes per entry and a warp-shuffle reduction over the quadrature points, -1 = keep the
+   current choice. Set by the autotuner. */
 int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
 
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by

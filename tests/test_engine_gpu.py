@@ -98,3 +98,23 @@ def test_adaptive_rounds_match_oracle(small_sphere):
             assert abs(st["est"][b] - o["est"]) <= 1e-6 * o["est"] + 1e-9
             C, U, R, I, J = eng.get_block(b, st)
             assert np.array_equal(I, o["I"]) and np.array_equal(J, o["J"])
+
+
+@pytest.mark.parametrize("prec,bar", [("c128", 1e-12), ("c64", 2e-6)])
+def test_fill_variants_agree(small_sphere, prec, bar):
+    """The triangle-moment fill, the two-rows-per-thread fill and the shuffle-split fill give
+    the same C and R for the same samples."""
+    m, part = small_sphere
+    out = {}
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        for v in (8, 0, 2):
+            eng.set_fill_split(split_c128=v, split_c64=v)
+            st = eng.compress(1.0, precision=prec, r0=np.full(eng.n_blocks, 12), oversample=0,
+                              max_rounds=1, seed=5)
+            out[v] = [eng.get_block(b, st)[:3] for b in (0, eng.n_blocks // 2)]
+    for v in (0, 2):
+        for (C, U, R), (C8, U8, R8) in zip(out[v], out[8]):
+            assert np.abs(C - C8).max() <= bar * np.abs(C8).max()
+            assert np.abs(R - R8).max() <= bar * np.abs(R8).max()
