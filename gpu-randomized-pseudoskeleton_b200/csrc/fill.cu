@@ -167,7 +167,9 @@ __global__ void __launch_bounds__(TM *TN *SPLIT, FillOcc<T>::value)
             C2 z;
             z.x = scale * re;
             z.y = scale * im;
-            reinterpret_cast<C2 *>(job.out)[i + (size_t)j * job.ld] = z;
+            C2 *out = reinterpret_cast<C2 *>(job.out);
+            if (!job.trans) out[i + (size_t)j * job.ld] = z;
+            else out[j + (size_t)i * job.ld] = z;
         }
         __syncthreads();
     }
