@@ -306,13 +306,14 @@ def run_ours(args, rank, world, dev):
                    fill_point_pairs=float(t_plain["point_pairs"]),
                    err_max=None if err_plain is None else float(err_plain.max()),
                    blocks_over_tol=None if err_plain is None else int((err_plain > TOL).sum())),
-        roofline=dict(bound="alu", kernel="fill_kernel<float,7> (c64, FP64 geometry)",
+        roofline=dict(bound="alu", kernel="tri_fill_kernel<float,7> (c64 triangle moments, FP64 geometry)",
                       achieved=round(achieved, 3), peak=round(fp32_peak.value, 3), unit="TFLOP/s",
                       frac=round(achieved / fp32_peak.value, 4), traffic=None,
                       peak_source="measured FP32 FMA microbenchmark on this GPU (pskel_fma_peak); "
                                   f"FP64 FMA {fp64_peak.value:.2f} TFLOP/s",
                       flops="32 flops per point-pair evaluation x point pairs / fill device time",
                       fill_ms=round(tph["fill"], 3), fill_launches=int(tph["fill_launches"])),
+        phases_nograph_ms={k: round(tph[k], 3) for k in ("sample", "fill", "pinv", "estimate", "total")},
         e2e=dict(value=round(e2e_ms, 3), unit="ms", h2d_bytes_per_step=int(h2d),
                  d2h_bytes_per_step=int(d2h)),
         clocks=clocks, gpu_launches=int(launches),

@@ -148,6 +148,7 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 
 __global__ void __launch_bounds__(kSvdThreads)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
+    // blockDim.x is a multiple of 32 chosen by the launcher (enough lane teams for one round)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdJob &job = jobs[idx_map[blockIdx.x]];
     const int m = job.m, n = job.n;
@@ -302,10 +303,20 @@ int svd_resident_attr() {
 }
 
 int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
-               int max_sweeps, cudaStream_t stream) {
+               int max_sweeps, cudaStream_t stream, int max_res_n) {
     PSKEL_TRY(svd_resident_attr());
+    // threads of the resident kernel: one lane team (~two rows per lane, up to a warp) per
+    // column pair of a round, rounded to warps, between 64 and 512
+    int resident_threads = kSvdThreads;
+    if (max_res_n > 0) {
+        int team = 1;
+        while (team < 32 && 4 * team <= max_res_n) team <<= 1;
+        int want = team * ((max_res_n + 1) / 2);
+        want = (want + 31) / 32 * 32;
+        resident_threads = want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
+    }
     if (n_res > 0) {
-        svd_resident_kernel<<<n_res, kSvdThreads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
+        svd_resident_kernel<<<n_res, resident_threads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
     if (n_blk > 0) {
@@ -328,7 +339,9 @@ int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweep
     int *d_idx = scratch.as<int>();
     PSKEL_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
                                stream));
-    return svd_launch(d_jobs, d_idx, n_res, nj - n_res, max_res, max_sweeps, stream);
+    int max_n = 0;
+    for (const SvdJob &j : h_jobs) max_n = std::max(max_n, j.n);
+    return svd_launch(d_jobs, d_idx, n_res, nj - n_res, max_res, max_sweeps, stream, max_n);
 }
 
 // ------------------------------------------------------------------ pseudo-inverse

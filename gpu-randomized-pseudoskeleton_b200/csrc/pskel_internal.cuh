@@ -169,7 +169,7 @@ int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweep
 int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_res,
              size_t *max_res_smem);
 int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
-               int max_sweeps, cudaStream_t stream);
+               int max_sweeps, cudaStream_t stream, int max_res_n = 0);
 // Shared-memory attributes of the SVD kernels (set once per process).
 int svd_resident_attr();
 
