@@ -388,9 +388,7 @@ struct RoundPlan {
     int fill_jobs = 0, fill_tiles = 0;
     SvdJob *d_svd = nullptr;
     int *d_svd_idx = nullptr;
-    int n_res = 0, n_blk = 0;
-    size_t max_res_smem = 0;
-    int max_r = 0;
+    SvdPlan svd;
     PinvJob *d_pinv = nullptr;
     int pinv_tiles = 0;
     int nb = 0;
@@ -517,11 +515,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         for (size_t i = 0; i < fills.size(); ++i)
             prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
     }
-    std::vector<int> svd_idx;
-    PSKEL_TRY(svd_plan(svds, svd_idx, &p.n_res, &p.max_res_smem));
-    p.max_r = 0;
-    for (int i = 0; i < nb; ++i) p.max_r = std::max(p.max_r, p.r[i]);
-    p.n_blk = nb - p.n_res;
+    PSKEL_TRY(svd_plan(svds, p.svd));
+    const std::vector<int> &svd_idx = p.svd.idx;
     // pack tables
     size_t t = 0;
     auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
@@ -586,7 +581,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     else
         gather_core_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.n_res, p.n_blk, p.max_res_smem, 60, s, p.max_r));
+    PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.svd, 60, s));
     PSKEL_TRY(batched_pinv(p.d_pinv, p.nb, p.pinv_tiles, s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));
     if (o.precision == PSKEL_C64)

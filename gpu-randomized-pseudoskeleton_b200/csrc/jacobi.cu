@@ -262,29 +262,52 @@ __global__ void __launch_bounds__(kSvdThreads)
 
 static size_t resident_bytes(int m, int n) { return sizeof(double2) * ((size_t)m * n + (size_t)n * n); }
 
-int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_res,
-             size_t *max_res_smem) {
+// resident size classes: cores of n <= 16, 32, 48, 64, 80 columns get their own launch with a
+// shared-memory size and a thread count fitted to the class, so that one large core does not
+// dictate the occupancy of every CTA
+static int size_class(int n) { return n <= 16 ? 0 : n <= 32 ? 1 : n <= 48 ? 2 : n <= 64 ? 3 : 4; }
+
+static int resident_threads_for(int n) {
+    int team = 1;
+    while (team < 32 && 4 * team <= n) team <<= 1;
+    int want = team * ((n + 1) / 2);
+    want = (want + 31) / 32 * 32;
+    return want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
+}
+
+int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
     const int nj = (int)h_jobs.size();
-    idx.clear();
-    idx.reserve(nj);
-    *n_res = 0;
-    *max_res_smem = 0;
-    for (int pass = 0; pass < 2; ++pass)
-        for (int i = 0; i < nj; ++i) {
-            const SvdJob &j = h_jobs[i];
-            if (j.m < j.n || j.n <= 0 || j.m <= 0) {
-                set_error(PSKEL_ERR_ARG, "svd: job %d has m=%d < n=%d or is empty", i, j.m, j.n);
-                return PSKEL_ERR_ARG;
-            }
-            const bool fits = resident_bytes(j.m, j.n) <= kSmemBudget;
-            if (fits == (pass == 0)) {
-                idx.push_back(i);
-                if (fits) {
-                    ++*n_res;
-                    *max_res_smem = std::max(*max_res_smem, resident_bytes(j.m, j.n));
-                }
-            }
+    plan.idx.clear();
+    plan.idx.reserve(nj);
+    plan.res.clear();
+    std::vector<std::vector<int>> cls(5);
+    std::vector<int> blk;
+    std::vector<size_t> smem(5, 0);
+    std::vector<int> maxn(5, 0);
+    for (int i = 0; i < nj; ++i) {
+        const SvdJob &j = h_jobs[i];
+        if (j.m < j.n || j.n <= 0 || j.m <= 0) {
+            set_error(PSKEL_ERR_ARG, "svd: job %d has m=%d < n=%d or is empty", i, j.m, j.n);
+            return PSKEL_ERR_ARG;
         }
+        if (resident_bytes(j.m, j.n) <= kSmemBudget) {
+            const int c = size_class(j.n);
+            cls[c].push_back(i);
+            smem[c] = std::max(smem[c], resident_bytes(j.m, j.n));
+            maxn[c] = std::max(maxn[c], j.n);
+        } else {
+            blk.push_back(i);
+        }
+    }
+    for (int c = 0; c < 5; ++c) {
+        if (cls[c].empty()) continue;
+        plan.res.push_back(SvdPlan::Cls{(int)plan.idx.size(), (int)cls[c].size(), smem[c],
+                                        resident_threads_for(maxn[c])});
+        plan.idx.insert(plan.idx.end(), cls[c].begin(), cls[c].end());
+    }
+    plan.blk_off = (int)plan.idx.size();
+    plan.blk_count = (int)blk.size();
+    plan.idx.insert(plan.idx.end(), blk.begin(), blk.end());
     return PSKEL_OK;
 }
 
@@ -302,46 +325,40 @@ int svd_resident_attr() {
     return PSKEL_OK;
 }
 
-int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
-               int max_sweeps, cudaStream_t stream, int max_res_n) {
+int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
+               cudaStream_t stream) {
     PSKEL_TRY(svd_resident_attr());
-    // threads of the resident kernel: one lane team (~two rows per lane, up to a warp) per
-    // column pair of a round, rounded to warps, between 64 and 512
-    int resident_threads = kSvdThreads;
-    if (max_res_n > 0) {
-        int team = 1;
-        while (team < 32 && 4 * team <= max_res_n) team <<= 1;
-        int want = team * ((max_res_n + 1) / 2);
-        want = (want + 31) / 32 * 32;
-        resident_threads = want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
-    }
-    if (n_res > 0) {
-        svd_resident_kernel<<<n_res, resident_threads, max_res_smem, stream>>>(d_jobs, d_idx, max_sweeps);
+    for (const SvdPlan::Cls &c : plan.res) {
+        svd_resident_kernel<<<c.count, c.threads, c.smem, stream>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
-    if (n_blk > 0) {
-        svd_blocked_kernel<<<n_blk, kSvdThreads, kSmemBudget, stream>>>(d_jobs, d_idx + n_res,
-                                                                        max_sweeps, (int)kSmemBudget);
+    if (plan.blk_count > 0) {
+        svd_blocked_kernel<<<plan.blk_count, kSvdThreads, kSmemBudget, stream>>>(
+            d_jobs, d_idx + plan.blk_off, max_sweeps, (int)kSmemBudget);
         PSKEL_LAUNCHED(1);
     }
     return PSKEL_OK;
 }
 
+int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
+                               cudaStream_t stream) {
+    SvdPlan plan;
+    plan.res.push_back(SvdPlan::Cls{0, 1, resident_bytes(m, n), resident_threads_for(n)});
+    plan.blk_off = 1;
+    plan.blk_count = 0;
+    return svd_launch(d_job, d_idx0, plan, max_sweeps, stream);
+}
+
 int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
                 cudaStream_t stream, DevBuf &scratch) {
-    const int nj = (int)h_jobs.size();
-    if (nj == 0) return PSKEL_OK;
-    std::vector<int> idx;
-    int n_res = 0;
-    size_t max_res = 0;
-    PSKEL_TRY(svd_plan(h_jobs, idx, &n_res, &max_res));
-    PSKEL_TRY(scratch.reserve(sizeof(int) * idx.size()));
+    if (h_jobs.empty()) return PSKEL_OK;
+    SvdPlan plan;
+    PSKEL_TRY(svd_plan(h_jobs, plan));
+    PSKEL_TRY(scratch.reserve(sizeof(int) * plan.idx.size()));
     int *d_idx = scratch.as<int>();
-    PSKEL_CUDA(cudaMemcpyAsync(d_idx, idx.data(), sizeof(int) * idx.size(), cudaMemcpyHostToDevice,
-                               stream));
-    int max_n = 0;
-    for (const SvdJob &j : h_jobs) max_n = std::max(max_n, j.n);
-    return svd_launch(d_jobs, d_idx, n_res, nj - n_res, max_res, max_sweeps, stream, max_n);
+    PSKEL_CUDA(cudaMemcpyAsync(d_idx, plan.idx.data(), sizeof(int) * plan.idx.size(),
+                               cudaMemcpyHostToDevice, stream));
+    return svd_launch(d_jobs, d_idx, plan, max_sweeps, stream);
 }
 
 // ------------------------------------------------------------------ pseudo-inverse

@@ -161,10 +161,9 @@ extern "C" int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau,
     noalloc_setup_kernel<<<16, 256, 0, s>>>(base, Ad, M, N, tau, relative);
     PSKEL_LAUNCHED(1);
     const int m = M < N ? N : M, n = M < N ? M : N;
-    const size_t smem = sizeof(double2) * ((size_t)m * n + (size_t)n * n);
     SvdJob *sj = reinterpret_cast<SvdJob *>(base + NoAllocLayout::svd);
     const int *idx = reinterpret_cast<const int *>(base + NoAllocLayout::idx);
-    PSKEL_TRY(svd_launch(sj, idx, 1, 0, smem, 60, s));
+    PSKEL_TRY(svd_launch_single_resident(sj, idx, m, n, 60, s));
     const PinvJob *pj = reinterpret_cast<const PinvJob *>(base + NoAllocLayout::pinv);
     PSKEL_TRY(batched_pinv(pj, 1, ((n + 31) / 32) * ((m + 31) / 32), s));
     noalloc_finish_kernel<<<16, 256, 0, s>>>(base, M, N, reinterpret_cast<double2 *>(P), sigma, rank);

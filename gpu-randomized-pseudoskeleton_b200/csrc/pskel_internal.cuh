@@ -164,12 +164,24 @@ struct SvdJob {
 int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
                 cudaStream_t stream, DevBuf &scratch);
 
-// The same split into a host plan (job order: resident jobs first, then blocked ones) and a
-// launch from device tables, so the launches can be captured in a CUDA graph.
-int svd_plan(const std::vector<SvdJob> &h_jobs, std::vector<int> &idx, int *n_res,
-             size_t *max_res_smem);
-int svd_launch(SvdJob *d_jobs, const int *d_idx, int n_res, int n_blk, size_t max_res_smem,
-               int max_sweeps, cudaStream_t stream, int max_res_n = 0);
+// The same work as a host plan (job order: resident jobs by size class, then blocked ones) and
+// launches from device tables, so the launches can be captured in a CUDA graph.
+struct SvdPlan {
+    struct Cls {
+        int off, count;  // range of the index map
+        size_t smem;     // dynamic shared memory of the class
+        int threads;
+    };
+    std::vector<int> idx;  // job order
+    std::vector<Cls> res;  // resident classes
+    int blk_off = 0, blk_count = 0;
+};
+int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan);
+int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
+               cudaStream_t stream);
+// One resident job (m x n fits in shared memory) whose index map entry is d_idx0[0].
+int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
+                               cudaStream_t stream);
 // Shared-memory attributes of the SVD kernels (set once per process).
 int svd_resident_attr();
 
