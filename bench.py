@@ -272,6 +272,7 @@ def run_ours(args, rank, world, dev):
     if args.plain_errors:
         st_plain = eng.compress(TOL, **PLAIN)
         err_plain = eng.true_errors()
+    blockops = run_blockops(eng, st, m, flush)
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush)
     if args.save and rank == 0:
@@ -317,9 +318,67 @@ def run_ours(args, rank, world, dev):
         e2e=dict(value=round(e2e_ms, 3), unit="ms", h2d_bytes_per_step=int(h2d),
                  d2h_bytes_per_step=int(d2h)),
         clocks=clocks, gpu_launches=int(launches),
+        blockops=blockops,
     )
     eng.close()
     return out
+
+
+def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
+    """Compressed far-field matvec (nrhs right-hand sides, complex64 like the stored factors)
+    and FP64 recompression of every block, after the product compression."""
+    import torch
+
+    from pskel import _lib
+    L = _lib.lib()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn((m.N, nrhs), dtype=torch.complex64, device="cuda", generator=g)
+    for _ in range(3):
+        eng.matvec(X)
+    times = []
+    l0 = L.pskel_kernel_launches()
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.matvec(X)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    mv_launches = (L.pskel_kernel_launches() - l0) // reps
+    mv_ms = float(np.mean(times))
+    mm, nn, rr = (st[k].astype(np.float64) for k in ("m", "n", "r"))
+    factor_bytes = float(((mm + nn) * rr * 8 + rr * rr * 16).sum())
+    vec_bytes = float(((mm + nn) * nrhs * 8).sum())
+    flops = float((8 * (mm + nn) * rr * nrhs + 8 * rr * rr * nrhs).sum())
+    peak = _hbm_peak()
+    gbs = (factor_bytes + vec_bytes) / (mv_ms * 1e-3) / 1e9
+    # recompression to the compression tolerance
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ks = eng.recompress(TOL)
+    rc_ms = (time.perf_counter() - t0) * 1e3
+    return dict(
+        matvec=dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),
+                    factor_bytes=factor_bytes, vector_bytes=vec_bytes,
+                    achieved_gbs=round(gbs, 1), peak_gbs=peak, frac=round(gbs / peak, 4),
+                    gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
+                    bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
+                          "once each per call (algorithmic)"),
+        recompress=dict(ms=round(rc_ms, 3), thresh=TOL, r_mean=float(rr.mean()),
+                        k_mean=float(ks.mean()), arithmetic="FP64 (Jacobi on C, R^H and the core)",
+                        timing="host wall clock around the synchronous call"),
+    )
+
+
+def _hbm_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return 6650.0
 
 
 def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush):

@@ -22,28 +22,10 @@
 
 #include "pskel_internal.cuh"
 #include "zgemm.cuh"
+#include "engine_internal.cuh"
 
 namespace pskel {
 
-static constexpr int kMaxGroup = 8192;   // largest m or n the sampler accepts
-static constexpr int kMaxExtra = 32;
-
-struct BlockWork {
-    const int *rows_g;  // global RWG ids of the test group (m)
-    const int *cols_g;  // global RWG ids of the source group (n)
-    int m, n, r, pe, pc;
-    int block_id, round;
-    int *I, *J, *Ix, *Jx;  // local indices (sorted)
-    int *Ig;            // global ids of rows I then Ix (r + pe)
-    int *Jg;            // global ids of columns J then Jx (r + pc)
-    void *C;            // m x (r + pc): C = Z(:, J), then the extra columns Z(:, Jx)
-    void *Rx;           // (r + pe) x n, ld = r + pe: R = Z(I, :), then the extra rows Z(Ix, :)
-    double2 *AV, *V, *U;
-    double2 *T;         // estimator scratch: C(Ix, :) U (pe x r), then U R(:, Jx) (r x pc)
-    double *sigma;
-    int *perm, *rank;
-    double *est;
-};
 
 // ------------------------------------------------------------------ sampler
 __device__ __forceinline__ uint32_t philox_word(uint32_t i, uint32_t block, uint32_t round,
@@ -305,52 +287,6 @@ __global__ void promote_kernel(const S *in, double2 *out, long long n) {
 
 // ====================================================================== context
 using namespace pskel;
-
-struct BlockResult {
-    int m = 0, n = 0, r = 0, pe = 0, pc = 0, round = -1, rank = 0, status = 0;
-    double est = 0;
-    int arena = -1;
-    size_t offC = 0, offRx = 0, offU = 0, offI = 0, offJ = 0;
-};
-
-struct RoundArena {
-    DevBuf keep;     // C, Rx, U, samples, sigma, est ... of the blocks of the round
-    DevBuf work;     // AV, V of the round (scratch, but owned per round so that a captured
-                     // round keeps valid pointers while later rounds grow their own)
-    DevBuf tables;   // device copies of the job tables
-    DevBuf outs;     // RoundOut per block of the round
-    std::vector<char> h_tables;
-};
-
-struct pskel_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaEvent_t ev[6] = {};
-    DevMesh mesh;
-    pskel_em_t em{};
-    bool have_mesh = false;
-    DevBuf flags;
-    int n_groups = 0, n_blocks = 0;
-    std::vector<int> gptr, gids, gt, gs;
-    DevBuf d_gids;
-    // triangle structure of the groups for the triangle-moment fill
-    std::vector<int> h_edges;            // T+, T-, v+, v- per RWG (0-based), host copy
-    std::vector<int> gtri_ptr;           // CSR offsets into gtri / (3x) gadj
-    DevBuf d_gtri, d_gadj;
-    bool use_tri = false;
-    std::vector<RoundArena> arenas;
-    std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
-    std::vector<BlockResult> results;
-    int precision = PSKEL_C128;
-    int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
-    double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    // CUDA graph of the first round
-    cudaGraphExec_t graph = nullptr;
-    long long graph_kernels = 0;  // kernel nodes of the captured graph
-    std::vector<int> graph_key;
-    std::vector<int> last_key;  // round-0 key of the previous call (capture on a repeat)
-    DevBuf tmp, tmp2, tmp3;
-};
 
 namespace {
 
@@ -647,7 +583,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec1.f64.release();
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
-    c->tmp.release(); c->tmp2.release(); c->tmp3.release();
+    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->mv_table.release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -826,6 +762,8 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     PSKEL_TRY(set_kernel_attrs());
     const double safety = o.est_safety >= 1.0 ? o.est_safety : 1.0;
     c->precision = o.precision;
+    ++c->generation;
+    c->recomp_slots.clear();
     for (double &t : c->timing) t = 0;
     const int nb = c->n_blocks;
     // first sample counts

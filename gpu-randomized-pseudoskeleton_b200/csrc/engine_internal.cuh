@@ -1,0 +1,92 @@
+// Internal state of the pskel_* handle API (engine.cu, blockops.cu).
+#pragma once
+
+#include <vector>
+
+#include "pskel_internal.cuh"
+
+namespace pskel {
+
+constexpr int kMaxGroup = 8192;  // largest m or n the sampler accepts
+constexpr int kMaxExtra = 32;
+
+struct BlockWork {
+    const int *rows_g;  // global RWG ids of the test group (m)
+    const int *cols_g;  // global RWG ids of the source group (n)
+    int m, n, r, pe, pc;
+    int block_id, round;
+    int *I, *J, *Ix, *Jx;  // local indices (sorted)
+    int *Ig;            // global ids of rows I then Ix (r + pe)
+    int *Jg;            // global ids of columns J then Jx (r + pc)
+    void *C;            // m x (r + pc): C = Z(:, J), then the extra columns Z(:, Jx)
+    void *Rx;           // (r + pe) x n, ld = r + pe: R = Z(I, :), then the extra rows Z(Ix, :)
+    double2 *AV, *V, *U;
+    double2 *T;         // estimator scratch: C(Ix, :) U (pe x r), then U R(:, Jx) (r x pc)
+    double *sigma;
+    int *perm, *rank;
+    double *est;
+};
+
+}  // namespace pskel
+
+using pskel::BlockWork;
+using pskel::DevBuf;
+using pskel::DevMesh;
+
+struct BlockResult {
+    int m = 0, n = 0, r = 0, pe = 0, pc = 0, round = -1, rank = 0, status = 0;
+    double est = 0;
+    int arena = -1;
+    size_t offC = 0, offRx = 0, offU = 0, offI = 0, offJ = 0;
+};
+
+struct RoundArena {
+    DevBuf keep;     // C, Rx, U, samples, sigma, est ... of the blocks of the round
+    DevBuf work;     // AV, V of the round (scratch, but owned per round so that a captured
+                     // round keeps valid pointers while later rounds grow their own)
+    DevBuf tables;   // device copies of the job tables
+    DevBuf outs;     // RoundOut per block of the round
+    std::vector<char> h_tables;
+};
+
+struct RecompSlot {
+    size_t offCp, offRp, offS;
+    int k;
+};
+
+struct pskel_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[6] = {};
+    DevMesh mesh;
+    pskel_em_t em{};
+    bool have_mesh = false;
+    DevBuf flags;
+    int n_groups = 0, n_blocks = 0;
+    std::vector<int> gptr, gids, gt, gs;
+    DevBuf d_gids;
+    // triangle structure of the groups for the triangle-moment fill
+    std::vector<int> h_edges;            // T+, T-, v+, v- per RWG (0-based), host copy
+    std::vector<int> gtri_ptr;           // CSR offsets into gtri / (3x) gadj
+    DevBuf d_gtri, d_gadj;
+    bool use_tri = false;
+    std::vector<RoundArena> arenas;
+    std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
+    std::vector<BlockResult> results;
+    int precision = PSKEL_C128;
+    int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
+    double timing[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // CUDA graph of the first round
+    cudaGraphExec_t graph = nullptr;
+    long long graph_kernels = 0;  // kernel nodes of the captured graph
+    std::vector<int> graph_key;
+    std::vector<int> last_key;  // round-0 key of the previous call (capture on a repeat)
+    DevBuf tmp, tmp2, tmp3;
+    DevBuf recomp;                          // recompressed factors and their workspace
+    std::vector<RecompSlot> recomp_slots;   // per block: offsets of C', R', S and the rank k
+    long long generation = 0;               // incremented by every compression
+    DevBuf mv_table;                        // matvec block table (built once per compression)
+    long long mv_generation = -1;
+    int mv_max_r = 0;
+};
+

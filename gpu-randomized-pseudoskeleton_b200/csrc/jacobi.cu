@@ -43,7 +43,7 @@ __device__ __forceinline__ int circle_player(int pos, int rho, int nn) {
 // A-part and ldv rows for V-part). Returns (via *rotated) whether any rotation happened.
 // All threads of the CTA must call it.
 __device__ void inner_sweep(double2 *sA, int m, double2 *sV, int nv, int w, int team,
-                            double tol, int *s_rot) {
+                            double tol, double zero2, int *s_rot) {
     const int tid = threadIdx.x;
     const int nteams = blockDim.x / team;
     const int t = tid / team;
@@ -83,7 +83,10 @@ __device__ void inner_sweep(double2 *sA, int m, double2 *sV, int nv, int w, int 
             }
             if (ci >= 0) {
                 const double ag = hypot(gr, gi);
-                if (ag > tol * sqrt(al) * sqrt(be) && ag > 0.0) {
+                // columns with squared norm <= zero2 are numerically zero: rotating them
+                // against anything only moves rounding noise (and on rank-deficient cores
+                // would never satisfy the relative test), so they are left alone
+                if (ag > tol * sqrt(al) * sqrt(be) && ag > 0.0 && al > zero2 && be > zero2) {
                     const double zeta = (be - al) / (2.0 * ag);
                     double tt;
                     if (fabs(zeta) > 1e150) {
@@ -116,6 +119,23 @@ __device__ void inner_sweep(double2 *sA, int m, double2 *sV, int nv, int w, int 
         }
         __syncthreads();
     }
+}
+
+// Squared column norm below which a column counts as zero: (m eps)^2 ||A||_F^2 (the
+// Frobenius norm is invariant under the rotations). All threads of the CTA must call it.
+__device__ double zero_column_norm2(const double2 *A, size_t count, int m) {
+    __shared__ double red[32];
+    double s = 0;
+    for (size_t i = threadIdx.x; i < count; i += blockDim.x) s = fma(A[i].x, A[i].x, fma(A[i].y, A[i].y, s));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    __syncthreads();
+    const double e = (double)m * DBL_EPSILON;
+    return e * e * t;
 }
 
 __device__ int pick_team(int m) {
@@ -161,11 +181,12 @@ __global__ void __launch_bounds__(kSvdThreads)
     __syncthreads();
     const int team = pick_team(m);
     const double tol = (double)(m > 1 ? m : 1) * DBL_EPSILON;
+    const double zero2 = zero_column_norm2(sA, (size_t)m * n, m);
     int sweep = 0, converged = 0;
     for (; sweep < max_sweeps; ++sweep) {
         if (threadIdx.x == 0) s_rot = 0;
         __syncthreads();
-        inner_sweep(sA, m, sV, n, n, team, tol, &s_rot);
+        inner_sweep(sA, m, sV, n, n, team, tol, zero2, &s_rot);
         __syncthreads();
         const int rot = s_rot;
         __syncthreads();
@@ -203,6 +224,7 @@ __global__ void __launch_bounds__(kSvdThreads)
     __syncthreads();
     const int team = pick_team(m);
     const double tol = (double)(m > 1 ? m : 1) * DBL_EPSILON;
+    const double zero2 = zero_column_norm2(job.A, (size_t)m * n, m);
     int sweep = 0, converged = 0;
     if (nb == 1) nb = 2;  // a single block still needs its own inner sweep: pair it with empty
     for (; sweep < max_sweeps; ++sweep) {
@@ -226,7 +248,7 @@ __global__ void __launch_bounds__(kSvdThreads)
                 }
                 if (threadIdx.x == 0) s_rot = 0;
                 __syncthreads();
-                inner_sweep(sA, m, sV, n, w, team, tol, &s_rot);
+                inner_sweep(sA, m, sV, n, w, team, tol, zero2, &s_rot);
                 __syncthreads();
                 if (s_rot) {
                     for (size_t idx = threadIdx.x; idx < (size_t)m * w; idx += blockDim.x) {

@@ -80,6 +80,9 @@ SIGNATURES = {
     "pskel_get_block": (ci, [VP, ci, VP, VP, VP, I32, I32]),
     "pskel_true_errors": (ci, [VP, D]),
     "pskel_set_fill_split": (ci, [VP, ci, ci]),
+    "pskel_matvec": (ci, [VP, VP, ci, VP, ci, ci, ci, VP]),
+    "pskel_recompress": (ci, [VP, cd, I32]),
+    "pskel_get_recompressed": (ci, [VP, ci, VP, D, VP]),
     "pskel_mlp_num_params": (ci, []),
     "pskel_mlp_forward": (ci, [VP, VP, ci, VP, VP]),
     "pskel_mlp_grad": (ci, [VP, VP, VP, ci, VP, VP, VP]),

@@ -154,6 +154,45 @@ class Engine:
         _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
         return err
 
+    def matvec(self, X, precision=None):
+        """Compressed far-field product Y = sum_b C_b U_b R_b X over all blocks of the last
+        compress(). X: torch CUDA tensor (RWG count, nrhs <= 64), complex128 or complex64
+        (the arithmetic precision); returns Y of the same shape and dtype on the same stream."""
+        import torch
+        if X.dim() == 1:
+            return self.matvec(X[:, None], precision)[:, 0]
+        if X.dtype not in (torch.complex128, torch.complex64) or not X.is_cuda:
+            raise ValueError("X must be a complex CUDA tensor")
+        prec = C128 if X.dtype == torch.complex128 else C64
+        ne, nrhs = X.shape
+        Xc = X.t().contiguous()                   # column-major (ne x nrhs), ld = ne
+        Y = torch.empty_like(Xc)
+        s = torch.cuda.current_stream(X.device).cuda_stream
+        _lib.check(self._lib.pskel_matvec(self._h, ctypes.c_void_p(Xc.data_ptr()), ne,
+                                          ctypes.c_void_p(Y.data_ptr()), ne, nrhs, prec,
+                                          ctypes.c_void_p(s)))
+        return Y.t()
+
+    def recompress(self, thresh: float) -> np.ndarray:
+        """SVD-truncate every block's C U R to C' diag(S) R' (S > thresh * S_max, FP64);
+        returns the kept rank per block."""
+        k = np.zeros(self.n_blocks, dtype=np.int32)
+        _lib.check(self._lib.pskel_recompress(self._h, float(thresh), k.ctypes.data_as(_lib.I32)))
+        self._recomp_k = k
+        return k
+
+    def get_recompressed(self, b: int):
+        """(C', S, R') of block b after recompress()."""
+        rows, cols = self.block_ids(b)
+        k = int(self._recomp_k[b])
+        Cp = np.zeros((len(rows), k), dtype=np.complex128, order="F")
+        S = np.zeros(k)
+        Rp = np.zeros((k, len(cols)), dtype=np.complex128, order="F")
+        vp = lambda x: ctypes.c_void_p(x.ctypes.data)
+        _lib.check(self._lib.pskel_get_recompressed(self._h, b, vp(Cp), S.ctypes.data_as(_lib.D),
+                                                    vp(Rp)))
+        return Cp, S, Rp
+
     def set_fill_split(self, split_c128: int = -1, split_c64: int = -1):
         """Fill-kernel variant: 8 triangle moments (default), 0 two rows per thread, 1/2/4
         lanes per entry with a shuffle reduction, -1 unchanged."""

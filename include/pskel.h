@@ -255,6 +255,30 @@ int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
 
+/* Compressed far-field matvec over every block of the last compression:
+   Y(:, j) = sum_b P_t(b) C_b U_b R_b P_s(b)^T X(:, j), j < nrhs <= 64, with P_t, P_s the
+   scatter/gather of the blocks' test and source groups (the near field is not included).
+   Replaces, for all blocks and many right-hand sides at once, the per-block C(U(R v)) of
+   codes/GPU_implementation/seed/user_impedance_for_julia_cuda.cu:1929-1960 (cuda_complete_
+   compression's error check). X (ldx >= RWG count) and Y (ldy >= RWG count) are DEVICE
+   arrays, column-major, interleaved complex of the arithmetic precision (PSKEL_C128: double,
+   PSKEL_C64: float); Y is overwritten. Enqueued on stream (NULL: the legacy default stream),
+   returns without waiting; the first call after a compression also uploads the block table
+   (synchronously). */
+int pskel_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int nrhs,
+                 int precision, void *stream);
+
+/* Recompression of every block's C U R into an SVD-truncated C' diag(S) R' (k terms kept,
+   S > thresh * S_max), in FP64: the restatement of codes/ACA_vs_CUR/seed/svd_compress.m:19-33
+   with its two QR factorisations replaced by one-sided Jacobi on C and R^H. ranks (host,
+   n_blocks, may be NULL) receives k per block. The factors stay on the device until the next
+   compression. */
+int pskel_recompress(pskel_ctx *ctx, double thresh, int *ranks);
+
+/* Copy block b's recompressed factors to host buffers: C' m x k, S (k, descending),
+   R' k x n (complex128, column-major). Any pointer may be NULL. */
+int pskel_get_recompressed(pskel_ctx *ctx, int b, pskel_c128 *Cp, double *S, pskel_c128 *Rp);
+
 /* ================================================= 3. rank / sample-count predictor (MLP) */
 /* 8 -> 64 -> 64 -> 1 MLP with GELU in FP32 (parameter layout W1[64x8] b1[64] W2[64x64] b2[64]
    W3[1x64] b3[1], row-major, contiguous). All pointers are DEVICE pointers; stream may be
