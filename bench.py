@@ -243,6 +243,13 @@ def run_ours(args, rank, world, dev):
         ms, st, launches, times = timed(step, args.steps, args.warmup)
     clocks = clk.summary()
     tinfo = eng.timing()
+    if args.product_only:
+        eng.close()
+        return dict(metric=METRIC, value=round(ms, 3), unit="ms", n_gpus=world, steps=args.steps,
+                    warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=False,
+                    mode="product steps only", gpu_launches=int(launches), clocks=clocks,
+                    sweeps=dict(mean=tinfo["sweeps_mean"], max=tinfo["sweeps_max"]),
+                    config=dict(workload=args.workload, blocks=int(part.n_blocks)))
     # plain FP64 GPU pseudoskeleton (the drop-in baseline): start at min(m,n)/10 and double,
     # driven one block at a time as the reference's drivers call its GPU CUR; same kernels,
     # samples and estimator as the batched modes
@@ -446,6 +453,9 @@ def main():
     ap.add_argument("--save", default=None, help="write per-block stats (npz)")
     ap.add_argument("--plain-errors", action="store_true", help="also check the plain run's errors")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--product-only", action="store_true",
+                    help="time the product steps only (no baselines, ablations, checks): the "
+                         "command the kernel launch list is captured from")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -477,7 +487,7 @@ def main():
         import datetime
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     out = run_ours(args, rank, world, local)
-    if world == 1 and rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and rank == 0 and not (args.no_cpu_baseline or args.product_only):
         out["cpu_baseline"] = cpu_baseline(args.workload)
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -251,6 +251,8 @@ struct RoundOut {
     double est;
     int rank;
     int status;
+    int sweeps;  // Jacobi sweeps of the core SVD
+    int pad;
 };
 __global__ void collect_kernel(const BlockWork *__restrict__ works, const SvdJob *__restrict__ svd,
                                int nb, RoundOut *out) {
@@ -259,6 +261,7 @@ __global__ void collect_kernel(const BlockWork *__restrict__ works, const SvdJob
     out[b].est = *works[b].est;
     out[b].rank = *works[b].rank;
     out[b].status = svd[b].status;
+    out[b].sweeps = svd[b].sweeps;
 }
 
 // ------------------------------------------------------------------ true errors
@@ -900,6 +903,9 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             res.est = hout[i].est;
             res.rank = hout[i].rank;
             res.status = hout[i].status;
+            c->timing[10] += hout[i].sweeps;
+            c->timing[11] = std::max(c->timing[11], (double)hout[i].sweeps);
+            c->timing[12] += 1;
             rounds_used[b] = round + 1;
             const bool ok = hout[i].status == PSKEL_OK && hout[i].est <= o.tol / safety;
             if (ok || r_cur[b] >= Dmin[b] || round + 1 >= o.max_rounds) continue;
@@ -925,6 +931,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     float total = 0;
     cudaEventElapsedTime(&total, t0, t1);
     c->timing[5] = total;
+    if (c->timing[12] > 0) c->timing[10] /= c->timing[12];
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     int h = 0;
@@ -971,7 +978,7 @@ extern "C" int pskel_last_timing(pskel_ctx *c, double *out, int n) {
         set_error(PSKEL_ERR_ARG, "null output");
         return PSKEL_ERR_ARG;
     }
-    for (int i = 0; i < n && i < 10; ++i) out[i] = c->timing[i];
+    for (int i = 0; i < n && i < 12; ++i) out[i] = c->timing[i];
     return PSKEL_OK;
 }
 

@@ -128,10 +128,11 @@ class Engine:
 
     def timing(self) -> dict:
         """Device ms per phase of the last compress() and its work counters."""
-        t = np.zeros(10)
-        _lib.check(self._lib.pskel_last_timing(self._h, t.ctypes.data_as(_lib.D), 10))
+        t = np.zeros(12)
+        _lib.check(self._lib.pskel_last_timing(self._h, t.ctypes.data_as(_lib.D), 12))
         return dict(zip(("sample", "fill", "pinv", "estimate", "recompress", "total",
-                         "fill_entries", "point_pairs", "fill_launches", "rounds"), t.tolist()))
+                         "fill_entries", "point_pairs", "fill_launches", "rounds",
+                         "sweeps_mean", "sweeps_max"), t.tolist()))
 
     def get_block(self, b: int, stats=None):
         rows, cols = self.block_ids(b)

@@ -41,7 +41,9 @@ def main():
                          max_rounds=1, seed=i)
             t = eng.timing()
             print(f"{prec} split {split} call {i}: fill {t['fill']:.3f} ms, "
-                  f"{t['point_pairs'] / t['fill'] / 1e6:.1f} G point pairs/s", flush=True)
+                  f"{t['point_pairs'] / t['fill'] / 1e6:.1f} G point pairs/s, pinv "
+                  f"{t['pinv']:.3f} ms, Jacobi sweeps mean {t['sweeps_mean']:.2f} "
+                  f"max {t['sweeps_max']:.0f}", flush=True)
 
 
 if __name__ == "__main__":

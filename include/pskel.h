@@ -236,7 +236,8 @@ int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r
 /* Timing and work counters of the last pskel_compress_blocks call: out[0..5] = device ms of
    the phases sample, fill, pinv, estimate, recompress and the whole call (a round replayed
    from a CUDA graph is booked under fill as a whole); out[6] = entries filled, out[7] =
-   point pairs evaluated, out[8] = fill launches, out[9] = rounds. n = length of out (<= 10). */
+   point pairs evaluated, out[8] = fill launches, out[9] = rounds, out[10] = mean and out[11] =
+   maximum Jacobi sweeps of the core SVDs. n = length of out (<= 12). */
 int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 
 /* Copy block b's factors to host buffers (complex128): C m x r, U r x r, R r x n, 0-based
