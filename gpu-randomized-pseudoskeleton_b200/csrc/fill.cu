@@ -557,7 +557,7 @@ struct TriWeights {
 };
 
 template <typename T, int Q, int TN>
-__global__ void __launch_bounds__(256, 2)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     tri_fill_kernel(const double *__restrict__ tri_rec, const double *__restrict__ rec_s,
                     const double *__restrict__ edges, const double *__restrict__ vertex,
                     const double *__restrict__ ln, const GroupFillJob *__restrict__ jobs,

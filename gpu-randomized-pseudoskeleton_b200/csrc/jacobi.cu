@@ -83,21 +83,25 @@ __device__ void inner_sweep(double2 *sA, int m, double2 *sV, int nv, int w, int 
                 }
             }
             if (ci >= 0) {
-                const double ag = hypot(gr, gi);
+                const double ag2 = fma(gr, gr, gi * gi);
                 // columns with squared norm <= zero2 are numerically zero: rotating them
                 // against anything only moves rounding noise (and on rank-deficient cores
                 // would never satisfy the relative test), so they are left alone
-                if (ag > tol * sqrt(al) * sqrt(be) && ag > 0.0 && al > zero2 && be > zero2) {
-                    const double zeta = (be - al) / (2.0 * ag);
+                if (ag2 > tol * tol * al * be && ag2 > 0.0 && al > zero2 && be > zero2) {
+                    // rotation from reciprocal square roots: 1/|gamma|, sqrt(1 + zeta^2) and
+                    // c = 1/sqrt(1 + t^2), plus one reciprocal for t
+                    const double iag = rsqrt(ag2);
+                    const double zeta = (be - al) * 0.5 * iag;
                     double tt;
                     if (fabs(zeta) > 1e150) {
                         tt = 0.5 / zeta;
                     } else {
-                        tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+                        const double w1 = fma(zeta, zeta, 1.0);
+                        tt = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + w1 * rsqrt(w1));
                     }
-                    const double c = 1.0 / sqrt(1.0 + tt * tt);
+                    const double c = rsqrt(fma(tt, tt, 1.0));
                     const double s = c * tt;
-                    const double2 e = make_double2(gr / ag, -gi / ag);  // e^{-i phi}
+                    const double2 e = make_double2(gr * iag, -gi * iag);  // e^{-i phi}
                     double2 *ai = sA + (size_t)ci * m;
                     double2 *aj = sA + (size_t)cj * m;
                     for (int r = g; r < m; r += team) {
@@ -137,6 +141,15 @@ __device__ double zero_column_norm2(const double2 *A, size_t count, int m) {
     __syncthreads();
     const double e = (double)m * DBL_EPSILON;
     return e * e * t;
+}
+
+// Lanes per column pair in a Jacobi round over w columns of m rows: as many as keep at least
+// two rows per lane while all w/2 pairs of a round still run at once in the CTA.
+__device__ int jacobi_team(int m, int w, int threads) {
+    const int npairs = (w + 1) / 2;
+    int t = 1;
+    while (t < 32 && 2 * t * 2 <= m && 2 * t * npairs <= threads) t <<= 1;
+    return t;
 }
 
 __device__ int pick_team(int m) {
@@ -312,7 +325,7 @@ __global__ void __launch_bounds__(kSvdThreads)
         sW[idx] = make_double2(i == j ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    const int team = pick_team(n);
+    const int team = jacobi_team(n, n, blockDim.x);
     const double tol = (double)(n > 1 ? n : 1) * DBL_EPSILON;
     const double zero2 = zero_column_norm2(sX, (size_t)n * n, n);
     int sweep = 0, converged = 0;
@@ -510,7 +523,7 @@ static int size_class(int n) { return n <= 16 ? 0 : n <= 32 ? 1 : n <= 48 ? 2 : 
 
 static int resident_threads_for(int n) {
     int team = 1;
-    while (team < 32 && 4 * team <= n) team <<= 1;
+    while (team < 32 && 4 * team <= n) team <<= 1;  // jacobi_team without the thread cap
     int want = team * ((n + 1) / 2);
     want = (want + 31) / 32 * 32;
     return want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
