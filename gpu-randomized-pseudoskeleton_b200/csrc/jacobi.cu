@@ -199,10 +199,13 @@ __global__ void __launch_bounds__(kSvdThreads)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SvdJob &job = jobs[idx_map[blockIdx.x]];
     const int m = job.m, n = job.n;
+    // square cores (m == n) park the reflectors in job.V during the Jacobi sweeps and let W
+    // take their place, so that a CTA needs 2 n^2 complex values of shared memory, not 3 n^2
+    const bool compact = m == n;
     double2 *sA = reinterpret_cast<double2 *>(smem_raw);  // m x n: R and the reflectors
     double2 *sX = sA + (size_t)m * n;                      // n x n: R^H, then B
-    double2 *sW = sX + (size_t)n * n;                      // n x n: rotations
-    double2 *sv0 = sW + (size_t)n * n;                     // n: first entry of each reflector
+    double2 *sW = compact ? sA : sX + (size_t)n * n;       // n x n: rotations
+    double2 *sv0 = sX + (size_t)n * n + (compact ? 0 : (size_t)n * n);  // n: first entry of each reflector
     double *scoef = reinterpret_cast<double *>(sv0 + n);   // n: 2 / |v|^2
     double *snrm = scoef + n;                              // n
     int *spiv = reinterpret_cast<int *>(snrm + n);         // n
@@ -322,6 +325,15 @@ __global__ void __launch_bounds__(kSvdThreads)
         const int i = idx % n, j = idx / n;
         const double2 r = sA[j + (size_t)i * m];  // R(j, i)
         sX[idx] = j <= i ? make_double2(r.x, -r.y) : make_double2(0.0, 0.0);
+    }
+    const double2 *refl = sA;  // reflector k: v0 = sv0[k], tail refl[k+1 .. m-1 + k m]
+    if (compact) {
+        for (int idx = tid; idx < m * n; idx += blockDim.x) job.V[idx] = sA[idx];
+        refl = job.V;
+        __syncthreads();
+    }
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;
         sW[idx] = make_double2(i == j ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
@@ -351,13 +363,6 @@ __global__ void __launch_bounds__(kSvdThreads)
         snrm[j] = sqrt(s2);
     }
     __syncthreads();
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
-        const int i = idx % n, j = idx / n;
-        const double sg = snrm[j];
-        const double f = sg > 0 ? 1.0 / sg : 0.0;
-        const double2 b = sX[idx];
-        job.V[spiv[i] + (size_t)j * n] = make_double2(b.x * f, b.y * f);
-    }
     // A V column j by one team: y = [W(:, j) sigma_j; 0], then y <- H_k y for k = n-1 .. 0;
     // the team's lanes hold rows qg, qg + qteam, ... (at most kQrRowsPerLane each)
     for (int j0 = 0; j0 < n; j0 += qteams) {
@@ -379,7 +384,7 @@ __global__ void __launch_bounds__(kSvdThreads)
             for (int e = 0; e < kQrRowsPerLane; ++e) {
                 const int i = qg + e * qteam;
                 if (i >= k && i < m) {
-                    const double2 x = i == k ? v0 : sA[i + (size_t)k * m];
+                    const double2 x = i == k ? v0 : refl[i + (size_t)k * m];
                     dr = fma(x.x, y[e].x, fma(x.y, y[e].y, dr));
                     di = fma(x.x, y[e].y, fma(-x.y, y[e].x, di));
                 }
@@ -393,7 +398,7 @@ __global__ void __launch_bounds__(kSvdThreads)
             for (int e = 0; e < kQrRowsPerLane; ++e) {
                 const int i = qg + e * qteam;
                 if (i >= k && i < m) {
-                    const double2 x = i == k ? v0 : sA[i + (size_t)k * m];
+                    const double2 x = i == k ? v0 : refl[i + (size_t)k * m];
                     y[e].x -= fr * x.x - fi * x.y;
                     y[e].y -= fr * x.y + fi * x.x;
                 }
@@ -406,6 +411,14 @@ __global__ void __launch_bounds__(kSvdThreads)
                 if (i < m) job.A[i + (size_t)j * m] = y[e];
             }
         }
+    }
+    __syncthreads();  // the reflectors in job.V are read until here
+    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;
+        const double sg = snrm[j];
+        const double f = sg > 0 ? 1.0 / sg : 0.0;
+        const double2 b = sX[idx];
+        job.V[spiv[i] + (size_t)j * n] = make_double2(b.x * f, b.y * f);
     }
     for (int j = tid; j < n; j += blockDim.x) job.sigma[j] = snrm[j];
     if (job.perm) {
@@ -504,7 +517,8 @@ __global__ void __launch_bounds__(kSvdThreads)
 }
 
 static size_t resident_bytes(int m, int n) {
-    return sizeof(double2) * ((size_t)m * n + 2 * (size_t)n * n + n) +
+    const size_t w = m == n ? 0 : (size_t)n * n;  // square cores keep W over the QR workspace
+    return sizeof(double2) * ((size_t)m * n + (size_t)n * n + w + n) +
            (2 * sizeof(double) + sizeof(int)) * (size_t)n;
 }
 
