@@ -367,6 +367,30 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     t0 = time.perf_counter()
     ks = eng.recompress(TOL)
     rc_ms = (time.perf_counter() - t0) * 1e3
+    # compressed store and the tensor-core matvec over it
+    t0 = time.perf_counter()
+    store_bytes = eng.build_store()
+    build_ms = (time.perf_counter() - t0) * 1e3
+    for _ in range(3):
+        eng.store_matvec(X)
+    st_times = []
+    l0 = L.pskel_kernel_launches()
+    for _ in range(reps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.store_matvec(X)
+        e1.record()
+        torch.cuda.synchronize()
+        st_times.append(e0.elapsed_time(e1))
+    st_launches = (L.pskel_kernel_launches() - l0) // reps
+    st_ms = float(np.mean(st_times))
+    st_status = eng.store_status()
+    kk = ks.astype(np.float64)
+    st_alg_bytes = float(((mm + nn) * kk * 2 * 4).sum())  # bf16 hi + lo of [re | im] per entry
+    st_gbs = (st_alg_bytes + vec_bytes) / (st_ms * 1e-3) / 1e9
     return dict(
         matvec=dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),
                     factor_bytes=factor_bytes, vector_bytes=vec_bytes,
@@ -374,6 +398,13 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
                     gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
                     bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
                           "once each per call (algorithmic)"),
+        store_matvec=dict(ms=round(st_ms, 4), nrhs=nrhs, launches=int(st_launches),
+                          status=int(st_status), store_bytes=store_bytes,
+                          build_ms=round(build_ms, 3), algorithmic_bytes=st_alg_bytes,
+                          achieved_gbs=round(st_gbs, 1), peak_gbs=peak, frac=round(st_gbs / peak, 4),
+                          arithmetic="tcgen05 kind::f16, bf16 hi/lo split (3 products), FP32 accumulation",
+                          bytes="C' and diag(S) R' as bf16 hi + lo of [re | im] (8 bytes per complex "
+                                "entry), gathered X and scattered Y (algorithmic; tile padding excluded)"),
         recompress=dict(ms=round(rc_ms, 3), thresh=TOL, r_mean=float(rr.mean()),
                         k_mean=float(ks.mean()), arithmetic="FP64 (Jacobi on C, R^H and the core)",
                         timing="host wall clock around the synchronous call"),

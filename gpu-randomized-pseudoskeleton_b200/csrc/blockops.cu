@@ -174,6 +174,7 @@ struct RecompBlock {
     double2 *Bc, *Vc, *Br, *Vr, *T, *M, *Vm, *Tc, *Tr, *Cp, *RpH, *Rp;
     double *sc, *sr, *sm, *S;
     int *pc, *pr, *pm, *k;
+    int *kout;  // the kept rank, in a table of all blocks
     int m, n, r, ldr;
     double thresh;
 };
@@ -243,6 +244,7 @@ __global__ void __launch_bounds__(256) recomp_factors_kernel(const RecompBlock *
         int k = 0;
         for (int t = 0; t < w.r; ++t) k += w.sm[w.pm[t]] > w.thresh * smax;
         *w.k = k;
+        *w.kout = k;
     }
 }
 
@@ -337,11 +339,13 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     // device job tables
     const size_t jb = sizeof(RecompBlock) * nb, s1 = sizeof(SvdJob) * svd1.size(),
                  s2 = sizeof(SvdJob) * svd2.size();
-    PSKEL_TRY(c->tmp.reserve(jb + s1 + s2 + 1024));
+    PSKEL_TRY(c->tmp.reserve(jb + s1 + s2 + sizeof(int) * nb + 1024));
     char *d = c->tmp.as<char>();
     RecompBlock *d_jobs = reinterpret_cast<RecompBlock *>(d);
     SvdJob *d_s1 = reinterpret_cast<SvdJob *>(d + ((jb + 255) & ~size_t(255)));
     SvdJob *d_s2 = reinterpret_cast<SvdJob *>(reinterpret_cast<char *>(d_s1) + ((s1 + 255) & ~size_t(255)));
+    int *d_k = reinterpret_cast<int *>(reinterpret_cast<char *>(d_s2) + ((s2 + 255) & ~size_t(255)));
+    for (int b = 0; b < nb; ++b) jobs[b].kout = d_k + b;
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_s1, svd1.data(), s1, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_s2, svd2.data(), s2, cudaMemcpyHostToDevice, c->stream));
@@ -364,8 +368,7 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     PSKEL_CUDA(cudaMemcpyAsync(h1.data(), d_s1, s1, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
     std::vector<int> ks(nb);
-    for (int b = 0; b < nb; ++b)
-        PSKEL_CUDA(cudaMemcpyAsync(&ks[b], jobs[b].k, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PSKEL_CUDA(cudaMemcpyAsync(ks.data(), d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
     for (const SvdJob &j : h1)
         if (j.status != PSKEL_OK) {

@@ -587,6 +587,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
     c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->mv_table.release();
+    for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;

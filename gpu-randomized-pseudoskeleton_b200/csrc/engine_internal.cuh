@@ -54,6 +54,30 @@ struct RecompSlot {
     int k;
 };
 
+// Compressed store of the recompressed blocks (csrc/store.cu): host copy of its layout.
+struct StoreTile {
+    long long a_off, b_off;  // A and B offsets (bf16 elements) within the phase's region
+    int kc, rows, out0;      // K chunks, valid rows, first T row (phase 1) or first group row
+    int phase;
+};
+struct StoreGroup {
+    long long b_base;  // B offset within the phase's region
+    int kc, K;         // chunks, real K
+    int ids0;          // phase 1: offset of the group's ids in the group id list
+    int map0;          // phase 2: offset of the group's T-row map
+};
+struct StoreLayout {
+    std::vector<StoreTile> tiles1, tiles2;
+    std::vector<StoreGroup> groups1, groups2;
+    std::vector<int> trow_map;
+    long long a1 = 0, a2 = 0, b1 = 0, b2 = 0;
+    int trows = 0;
+    int n_items1 = 0, n_items2 = 0;  // GEMM work items per phase
+    void *d_t1 = nullptr, *d_t2 = nullptr, *d_g1 = nullptr, *d_g2 = nullptr;
+    bool ready = false;
+    long long generation = -1;
+};
+
 struct pskel_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -88,5 +112,7 @@ struct pskel_ctx {
     DevBuf mv_table;                        // matvec block table (built once per compression)
     long long mv_generation = -1;
     int mv_max_r = 0;
+    StoreLayout store;                      // compressed store (bf16 hi/lo planes, tiled)
+    DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
 };
 

@@ -1,0 +1,657 @@
+// Compressed store and its far-field matvec on the 5th-generation tensor cores.
+//
+// After the recompression every far block is C'_b diag(S_b) R'_b. The store regroups the
+// factors so that the matvec Y = sum_b P_t(b) C'_b S_b R'_b P_s(b)^T X (16 complex right-hand
+// sides) becomes two grouped GEMMs:
+//   phase 1, per source group s:  T_s = [S_b R'_b ; b with gs(b) = s] X(ids_s)
+//   phase 2, per test group t:    Y(ids_t) = [C'_b ; b with gt(b) = t] [T_b ; b with gt(b) = t]
+// (the reference's C(U(R v)) of codes/GPU_implementation/seed/user_impedance_for_julia_cuda.cu:
+// 1929-1960, for all blocks and 16 vectors, on the recompressed form of
+// codes/ACA_vs_CUR/seed/svd_compress.m:19-33).
+//
+// Complex products run as real GEMMs: A' = [Re A | Im A] (K doubled) times
+// B' = [[Re X, Im X]; [-Im X, Re X]] gives [Re(AX) | Im(AX)] (N = 2 x 16 = 32).
+// Precision: every real operand is split into bf16 hi + lo (hi = bf16(x), lo = bf16(x - hi));
+// the tensor cores accumulate hi*hi + hi*lo + lo*hi in FP32 (relative error about 1e-5).
+//
+// Layout: both operands are stored K-major in the canonical no-swizzle UMMA layout: chunks of
+// 8 consecutive K values (16 bytes) for all rows of a 128-row tile (A) or of the 32 columns (B),
+// so that one pipeline stage (64 K values) of a tile is one contiguous range of global memory,
+// fetched with one bulk copy (cp.async.bulk, the TMA engine's linear mode) per plane. The hi and
+// lo planes are two arrays of the same shape.
+//
+// Kernel: one CTA of 128 threads per 128-row output tile. Warp 0 allocates 32 TMEM columns
+// (the 128 x 32 FP32 accumulator) and its lane 0 issues the bulk copies of a 4-stage ring;
+// lane 0 of warp 1 issues tcgen05.mma (kind::f16, bf16 in, FP32 accumulate, M = 128, N = 32,
+// K = 16) and commits each stage back to the producer through an mbarrier; after the last
+// stage all four warps read their 32 TMEM lanes (tcgen05.ld 32x32b) and write the rows. Every
+// mbarrier wait is bounded: a wait that runs out sets the error word, the CTA stops issuing,
+// waits (bounded) for what it issued, frees its TMEM and returns.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include <cuda_bf16.h>
+
+#include "engine_internal.cuh"
+
+namespace pskel {
+
+constexpr int kStTileM = 128;      // rows per output tile (UMMA M)
+constexpr int kStN = 32;           // real columns: 16 right-hand sides x (re, im)
+constexpr int kStRhs = 16;
+constexpr int kStStageK = 64;      // K values per pipeline stage (8 chunks of 8)
+constexpr int kStStages = 4;
+constexpr int kStChunkA = kStTileM * 8;  // bf16 elements per A chunk (128 rows x 8 K)
+constexpr int kStChunkB = kStN * 8;      // bf16 elements per B chunk (32 columns x 8 K)
+constexpr int kStStageABytes = 8 * kStChunkA * 2;  // 16 KB per plane
+constexpr int kStStageBBytes = 8 * kStChunkB * 2;  // 4 KB per plane
+constexpr int kStStageBytes = 2 * kStStageABytes + 2 * kStStageBBytes;
+constexpr size_t kStSmem = (size_t)kStStages * kStStageBytes + 1024;
+constexpr long long kStWaitLimit = 1ll << 22;  // try_wait polls before a wait counts as lost
+constexpr int kStSliceStages = 8;             // phase-2 K slice per work item (512 K values)
+
+// canonical offset (bf16 elements) of A(row, k) inside a group whose tiles have kc chunks each
+__host__ __device__ __forceinline__ long long st_a_off(long long base, int kc, int row, int k) {
+    return base + (((long long)(row >> 7) * kc + (k >> 3)) * kStTileM + (row & 127)) * 8 + (k & 7);
+}
+// canonical offset of B(col, k) (col < 32)
+__host__ __device__ __forceinline__ long long st_b_off(long long base, int col, int k) {
+    return base + ((long long)(k >> 3) * kStN + col) * 8 + (k & 7);
+}
+
+__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(x);
+    *hi = h;
+    *lo = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+
+// ---------------------------------------------------------------- pack (once per recompression)
+struct PackBlock {
+    const double2 *Cp;  // m x r (ld m), first k columns
+    const double2 *Rp;  // r x n (ld r), first k rows
+    const double *S;    // k
+    int m, n, r, k;
+    long long a1_base;  // phase-1 group base (elements) and the block's first row in it
+    int a1_kc, a1_row0;
+    long long a2_base;  // phase-2 group base and the block's first K column (real part)
+    int a2_kc, a2_col0, a2_K;  // a2_K: real K of the test group (imag parts start there)
+};
+
+__global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__ blocks,
+                                                   __nv_bfloat16 *A1h, __nv_bfloat16 *A1l,
+                                                   __nv_bfloat16 *A2h, __nv_bfloat16 *A2l) {
+    const PackBlock w = blocks[blockIdx.x];
+    // phase 1: rows S_i R'(i, :) of the source group's stack, [re | im] along K
+    for (int e = threadIdx.x; e < w.k * w.n; e += blockDim.x) {
+        const int i = e % w.k, j = e / w.k;
+        const double2 v = w.Rp[i + (size_t)j * w.r];
+        const double s = w.S[i];
+        const int row = w.a1_row0 + i;
+        const long long o_re = st_a_off(w.a1_base, w.a1_kc, row, j);
+        const long long o_im = st_a_off(w.a1_base, w.a1_kc, row, w.n + j);
+        split_bf16((float)(s * v.x), A1h + o_re, A1l + o_re);
+        split_bf16((float)(s * v.y), A1h + o_im, A1l + o_im);
+    }
+    // phase 2: columns C'(:, i) in the test group's stack
+    for (int e = threadIdx.x; e < w.m * w.k; e += blockDim.x) {
+        const int i = e % w.m, j = e / w.m;
+        const double2 v = w.Cp[i + (size_t)j * w.m];
+        const long long o_re = st_a_off(w.a2_base, w.a2_kc, i, w.a2_col0 + j);
+        const long long o_im = st_a_off(w.a2_base, w.a2_kc, i, w.a2_K + w.a2_col0 + j);
+        split_bf16((float)v.x, A2h + o_re, A2l + o_re);
+        split_bf16((float)v.y, A2h + o_im, A2l + o_im);
+    }
+}
+
+// ---------------------------------------------------------------- B operands (every matvec)
+struct StGroupB {
+    long long b_base;  // B buffer offset (elements)
+    int kc;            // chunks of the group's K (padded)
+    int K;             // real K (phase 1: group size; phase 2: sum of the blocks' ranks)
+    const int *src;    // phase 1: RWG ids of the group; phase 2: T row of each real K index
+};
+
+// phase 1: B'(k, c) from X (complex64, column-major, ldx), columns >= nrhs are zero. One thread
+// per K index writes its 32 columns: eight consecutive K indices fill one 16-byte chunk row.
+__global__ void __launch_bounds__(256) build_b1_kernel(const StGroupB *__restrict__ groups,
+                                                       const float2 *__restrict__ X, int ldx,
+                                                       int nrhs, __nv_bfloat16 *Bh,
+                                                       __nv_bfloat16 *Bl) {
+    const StGroupB g = groups[blockIdx.x];
+    const int kpad = g.kc * 8;
+    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
+        const bool in = k < 2 * g.K;
+        const bool re_half = k < g.K;
+        const int id = in ? g.src[re_half ? k : k - g.K] : 0;
+#pragma unroll 4
+        for (int rhs = 0; rhs < kStRhs; ++rhs) {
+            float2 x = make_float2(0.f, 0.f);
+            if (in && rhs < nrhs) x = X[id + (size_t)rhs * ldx];
+            const float v0 = re_half ? x.x : -x.y;  // column rhs:      [re X; -im X]
+            const float v1 = re_half ? x.y : x.x;   // column 16 + rhs: [im X;  re X]
+            const long long o0 = st_b_off(g.b_base, rhs, k), o1 = st_b_off(g.b_base, rhs + kStRhs, k);
+            split_bf16(v0, Bh + o0, Bl + o0);
+            split_bf16(v1, Bh + o1, Bl + o1);
+        }
+    }
+}
+
+// phase 2: B'(k, c) from the phase-1 rows T (32 floats per row: re of the 16 sides, then im);
+// one thread per K index reads its T row once
+__global__ void __launch_bounds__(256) build_b2_kernel(const StGroupB *__restrict__ groups,
+                                                       const float *__restrict__ T,
+                                                       __nv_bfloat16 *Bh, __nv_bfloat16 *Bl) {
+    const StGroupB g = groups[blockIdx.x];
+    const int kpad = g.kc * 8;
+    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
+        const bool in = k < 2 * g.K;
+        const bool re_half = k < g.K;
+        float t[kStN];
+        if (in) {
+            const float4 *row = reinterpret_cast<const float4 *>(T + (size_t)g.src[re_half ? k : k - g.K] * kStN);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 a = row[q];
+                t[4 * q] = a.x;
+                t[4 * q + 1] = a.y;
+                t[4 * q + 2] = a.z;
+                t[4 * q + 3] = a.w;
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < kStN; ++c) t[c] = 0.f;
+        }
+#pragma unroll
+        for (int c = 0; c < kStN; ++c) {
+            // [re T | im T] on the first K rows, [-im T | re T] on the second
+            const float v = re_half ? t[c] : (c < kStRhs ? -t[c + kStRhs] : t[c - kStRhs]);
+            const long long o = st_b_off(g.b_base, c, k);
+            split_bf16(v, Bh + o, Bl + o);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tcgen05 grouped GEMM
+// One work item of the grouped GEMM: a 128-row output tile and a range of its K stages.
+struct StItem {
+    long long a_off;  // first A chunk of the item (bf16 elements)
+    long long b_off;  // first B chunk of the item
+    int nst;          // stages (64 K values each)
+    int rows;         // valid rows of the tile
+    int out0;         // phase 1: first T row of the tile
+    const int *ids;   // phase 2: RWG ids of the tile's rows (null in phase 1)
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// no-swizzle K-major UMMA shared-memory descriptor: start, leading byte offset (distance of the
+// two 16-byte K chunks of one K = 16 step), stride byte offset (distance of 8-row core matrices)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
+    return d;                // base offset 0, absolute LBO mode, layout type 0 (no swizzle)
+}
+
+// instruction descriptor: kind::f16 with bf16 A and B, FP32 D, both K-major, M = 128, N = 32
+constexpr uint32_t kStIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kStN >> 3) << 17) |
+                              ((uint32_t)(kStTileM >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait; false when it ran out or the CTA aborted
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
+    for (long long i = 0; i < kStWaitLimit; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t accumulate) {
+    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kStIdesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
+        "r"(mask3));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Persistent grouped GEMM, one CTA per SM, warp-specialised:
+//   warp 0 lane 0   producer: bulk copies of the A and B planes into a 4-stage ring;
+//   warp 1 lane 0   MMA issuer: 3 x 4 tcgen05.mma per stage into one of two TMEM accumulators;
+//   warps 2-5       epilogue: tcgen05.ld of their TMEM lane quadrant, then the rows go out
+//                   (phase 1: stores into T; phase 2: FP32 atomics into Y, the items of a tile
+//                   being K slices of it).
+// The two accumulators let the epilogue of one item overlap the MMAs of the next.
+__global__ void __launch_bounds__(192, 1)
+    store_gemm_kernel(const StItem *__restrict__ items, int nitems,
+                      const __nv_bfloat16 *__restrict__ Ah, const __nv_bfloat16 *__restrict__ Al,
+                      const __nv_bfloat16 *__restrict__ Bh, const __nv_bfloat16 *__restrict__ Bl,
+                      float *T, float *Y, int ldy, int nrhs, int *err) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t full_bar[kStStages], empty_bar[kStStages];
+    __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], final_bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int s_abort;
+    unsigned char *ring = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStStages; ++s) {
+            mbar_init(&full_bar[s], 1);
+            mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&tfull_bar[a], 1);
+            mbar_init(&tempty_bar[a], 4);  // one arrival per epilogue warp
+        }
+        mbar_init(&final_bar, 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(2 * kStN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            long long g = 0;  // stages issued by this CTA
+            for (int it = blockIdx.x; it < nitems && !s_abort; it += gridDim.x) {
+                const StItem w = items[it];
+                for (int s = 0; s < w.nst; ++s, ++g) {
+                    const int slot = (int)(g % kStStages);
+                    if (g >= kStStages &&
+                        !mbar_wait(&empty_bar[slot], (uint32_t)(((g / kStStages) - 1) & 1), &s_abort)) {
+                        atomicExch(err, 1);
+                        s_abort = 1;
+                        break;
+                    }
+                    unsigned char *st = ring + (size_t)slot * kStStageBytes;
+                    mbar_expect_tx(&full_bar[slot], kStStageBytes);
+                    const long long ao = w.a_off + (long long)s * 8 * kStChunkA;
+                    const long long bo = w.b_off + (long long)s * 8 * kStChunkB;
+                    bulk_g2s(st, Ah + ao, kStStageABytes, &full_bar[slot]);
+                    bulk_g2s(st + kStStageABytes, Al + ao, kStStageABytes, &full_bar[slot]);
+                    bulk_g2s(st + 2 * kStStageABytes, Bh + bo, kStStageBBytes, &full_bar[slot]);
+                    bulk_g2s(st + 2 * kStStageABytes + kStStageBBytes, Bl + bo, kStStageBBytes, &full_bar[slot]);
+                }
+            }
+            // no copy may still be in flight when the CTA leaves
+            for (long long q = (g > kStStages ? g - kStStages : 0); q < g; ++q)
+                mbar_wait(&full_bar[q % kStStages], (uint32_t)((q / kStStages) & 1), &s_abort);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            long long g = 0;
+            int n = 0;  // items handled
+            for (int it = blockIdx.x; it < nitems && !s_abort; it += gridDim.x, ++n) {
+                const StItem w = items[it];
+                const int acc = n & 1;
+                if (n >= 2 && !mbar_wait(&tempty_bar[acc], (uint32_t)(((n >> 1) - 1) & 1), &s_abort)) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t d = tmem + (uint32_t)(acc * kStN);
+                for (int s = 0; s < w.nst; ++s, ++g) {
+                    const int slot = (int)(g % kStStages);
+                    if (!mbar_wait(&full_bar[slot], (uint32_t)((g / kStStages) & 1), &s_abort)) {
+                        atomicExch(err, 1);
+                        s_abort = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    unsigned char *st = ring + (size_t)slot * kStStageBytes;
+                    const uint32_t a_hi = smem_u32(st), a_lo = smem_u32(st + kStStageABytes);
+                    const uint32_t b_hi = smem_u32(st + 2 * kStStageABytes);
+                    const uint32_t b_lo = smem_u32(st + 2 * kStStageABytes + kStStageBBytes);
+#pragma unroll
+                    for (int ks = 0; ks < 4; ++ks) {  // K = 16 per MMA: two chunks
+                        const uint32_t ao = ks * 2 * kStChunkA * 2, bo = ks * 2 * kStChunkB * 2;
+                        const uint64_t dah = umma_desc(a_hi + ao, kStChunkA * 2, 128);
+                        const uint64_t dal = umma_desc(a_lo + ao, kStChunkA * 2, 128);
+                        const uint64_t dbh = umma_desc(b_hi + bo, kStChunkB * 2, 128);
+                        const uint64_t dbl = umma_desc(b_lo + bo, kStChunkB * 2, 128);
+                        umma_bf16(d, dah, dbh, (s > 0 || ks > 0) ? 1u : 0u);
+                        umma_bf16(d, dah, dbl, 1u);
+                        umma_bf16(d, dal, dbh, 1u);
+                    }
+                    umma_commit(&empty_bar[slot]);  // the slot is free once these MMAs have read it
+                }
+                if (s_abort) break;
+                umma_commit(&tfull_bar[acc]);  // the accumulator is complete
+            }
+            // every MMA issued has finished before TMEM may be released
+            umma_commit(&final_bar);
+            if (!mbar_wait(&final_bar, 0, &s_abort)) atomicExch(err, 1);
+        }
+    } else {
+        const int quad = warp & 3;  // TMEM lanes 32 quad .. 32 quad + 31
+        int n = 0;
+        for (int it = blockIdx.x; it < nitems; it += gridDim.x, ++n) {
+            const StItem w = items[it];
+            const int acc = n & 1;
+            int okw = mbar_wait(&tfull_bar[acc], (uint32_t)((n >> 1) & 1), &s_abort) ? 1 : 0;
+            okw = __all_sync(0xffffffffu, okw);
+            if (!okw) {
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    s_abort = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t v[32];
+            const uint32_t taddr = tmem + (uint32_t)(acc * kStN) + ((uint32_t)(quad * 32) << 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+                "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+                "%28, %29, %30, %31}, [%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+                  "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+                  "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty_bar[acc]);  // the accumulator may be reused
+            const int row = quad * 32 + lane;
+            if (row < w.rows) {
+                if (!w.ids) {
+                    float4 *t = reinterpret_cast<float4 *>(T + (size_t)(w.out0 + row) * kStN);
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        t[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                           __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+                } else {
+                    const int id = w.ids[row];
+#pragma unroll
+                    for (int c = 0; c < kStRhs; ++c)
+                        if (c < nrhs) {
+                            float *y = Y + 2 * ((size_t)id + (size_t)c * ldy);
+                            atomicAdd(y, __uint_as_float(v[c]));
+                            atomicAdd(y + 1, __uint_as_float(v[c + kStRhs]));
+                        }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kStN));
+}
+
+}  // namespace pskel
+
+using namespace pskel;
+
+// ---------------------------------------------------------------- host side
+extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
+    if (!c || c->n_blocks <= 0 || (int)c->recomp_slots.size() != c->n_blocks) {
+        set_error(PSKEL_ERR_STATE, "store_build: run pskel_recompress first");
+        return PSKEL_ERR_STATE;
+    }
+    PSKEL_CUDA(cudaSetDevice(c->device));
+    const int nb = c->n_blocks, ng = c->n_groups;
+    StoreLayout &L = c->store;
+    L = StoreLayout();
+    std::vector<std::vector<int>> by_src(ng), by_test(ng);
+    for (int b = 0; b < nb; ++b) {
+        by_src[c->gs[b]].push_back(b);
+        by_test[c->gt[b]].push_back(b);
+    }
+    auto gsize = [&](int g) { return c->gptr[g + 1] - c->gptr[g]; };
+    auto pad = [](long long x, long long a) { return (x + a - 1) / a * a; };
+    std::vector<PackBlock> pb(nb);
+    const char *rbase = c->recomp.as<char>();
+    // phase 1: per source group
+    long long a1 = 0, b1 = 0;
+    int trow = 0;
+    std::vector<int> t_row0(nb);  // first T row of each block
+    for (int g = 0; g < ng; ++g) {
+        if (by_src[g].empty()) continue;
+        int K = 0;
+        for (int b : by_src[g]) K += c->recomp_slots[b].k;
+        if (K == 0) continue;
+        const int n = gsize(g);
+        const int kc = (int)(pad(2 * (long long)n, kStStageK) / 8);
+        const int mpad = (int)pad(K, kStTileM);
+        int row = 0;
+        for (int b : by_src[g]) {
+            PackBlock &w = pb[b];
+            w.a1_base = a1;
+            w.a1_kc = kc;
+            w.a1_row0 = row;
+            t_row0[b] = trow + row;
+            row += c->recomp_slots[b].k;
+        }
+        for (int mt = 0; mt < mpad / kStTileM; ++mt)
+            L.tiles1.push_back(StoreTile{a1 + (long long)mt * kc * kStChunkA, b1, kc,
+                                         std::min(kStTileM, K - mt * kStTileM), trow + mt * kStTileM, -1});
+        L.groups1.push_back(StoreGroup{b1, kc, n, c->gptr[g], -1});
+        a1 += (long long)mpad * kc * 8;
+        b1 += (long long)kc * kStChunkB;
+        trow += mpad;
+    }
+    // phase 2: per test group; the T row of every real K index
+    long long a2 = 0, b2 = 0;
+    for (int g = 0; g < ng; ++g) {
+        if (by_test[g].empty()) continue;
+        int K = 0;
+        for (int b : by_test[g]) K += c->recomp_slots[b].k;
+        if (K == 0) continue;
+        const int m = gsize(g);
+        const int kc = (int)(pad(2 * (long long)K, kStStageK) / 8);
+        const int mpad = (int)pad(m, kStTileM);
+        const int map0 = (int)L.trow_map.size();
+        int col = 0;
+        for (int b : by_test[g]) {
+            PackBlock &w = pb[b];
+            w.a2_base = a2;
+            w.a2_kc = kc;
+            w.a2_col0 = col;
+            w.a2_K = K;
+            for (int i = 0; i < c->recomp_slots[b].k; ++i) L.trow_map.push_back(t_row0[b] + i);
+            col += c->recomp_slots[b].k;
+        }
+        for (int mt = 0; mt < mpad / kStTileM; ++mt)
+            L.tiles2.push_back(StoreTile{a2 + (long long)mt * kc * kStChunkA, b2, kc,
+                                         std::min(kStTileM, m - mt * kStTileM), c->gptr[g] + mt * kStTileM, 1});
+        L.groups2.push_back(StoreGroup{b2, kc, K, -1, map0});
+        a2 += (long long)mpad * kc * 8;
+        b2 += (long long)kc * kStChunkB;
+    }
+    for (int b = 0; b < nb; ++b) {
+        const RecompSlot &sl = c->recomp_slots[b];
+        const BlockResult &res = c->results[b];
+        PackBlock &w = pb[b];
+        w.Cp = reinterpret_cast<const double2 *>(rbase + sl.offCp);
+        w.Rp = reinterpret_cast<const double2 *>(rbase + sl.offRp);
+        w.S = reinterpret_cast<const double *>(rbase + sl.offS);
+        w.m = res.m;
+        w.n = res.n;
+        w.r = res.r;
+        w.k = sl.k;
+    }
+    L.a1 = a1;
+    L.a2 = a2;
+    L.b1 = b1;
+    L.b2 = b2;
+    L.trows = trow;
+    // device buffers: A planes (phase 1 then phase 2), B planes, T, tables
+    const size_t abytes = (size_t)(a1 + a2) * 2;
+    PSKEL_TRY(c->st_ah.reserve(abytes));
+    PSKEL_TRY(c->st_al.reserve(abytes));
+    PSKEL_TRY(c->st_bh.reserve((size_t)(b1 + b2) * 2 + 256));
+    PSKEL_TRY(c->st_bl.reserve((size_t)(b1 + b2) * 2 + 256));
+    PSKEL_TRY(c->st_t.reserve((size_t)std::max(trow, 1) * kStN * sizeof(float)));
+    PSKEL_CUDA(cudaMemsetAsync(c->st_ah.ptr, 0, abytes, c->stream));
+    PSKEL_CUDA(cudaMemsetAsync(c->st_al.ptr, 0, abytes, c->stream));
+    PSKEL_TRY(c->st_tab.reserve(sizeof(PackBlock) * nb + 256));
+    PSKEL_CUDA(cudaMemcpyAsync(c->st_tab.ptr, pb.data(), sizeof(PackBlock) * nb, cudaMemcpyHostToDevice,
+                               c->stream));
+    __nv_bfloat16 *ah = c->st_ah.as<__nv_bfloat16>(), *al = c->st_al.as<__nv_bfloat16>();
+    pack_kernel<<<nb, 256, 0, c->stream>>>(c->st_tab.as<PackBlock>(), ah, al, ah + a1, al + a1);
+    PSKEL_LAUNCHED(1);
+    // device tile and group tables (pointers resolved here)
+    const int *gids = c->d_gids.as<int>();
+    PSKEL_TRY(c->st_map.reserve(sizeof(int) * std::max<size_t>(L.trow_map.size(), 1)));
+    if (!L.trow_map.empty())
+        PSKEL_CUDA(cudaMemcpyAsync(c->st_map.ptr, L.trow_map.data(), sizeof(int) * L.trow_map.size(),
+                                   cudaMemcpyHostToDevice, c->stream));
+    // work items: phase-1 tiles whole (their K is one source group); phase-2 tiles cut into K
+    // slices of at most kStSliceStages stages, accumulated with atomics
+    std::vector<StItem> t1, t2;
+    for (const StoreTile &t : L.tiles1)
+        t1.push_back(StItem{t.a_off, t.b_off, t.kc / 8, t.rows, t.out0, nullptr});
+    for (const StoreTile &t : L.tiles2)
+        for (int s0 = 0; s0 < t.kc / 8; s0 += kStSliceStages)
+            t2.push_back(StItem{a1 + t.a_off + (long long)s0 * 8 * kStChunkA,
+                                b1 + t.b_off + (long long)s0 * 8 * kStChunkB,
+                                std::min(kStSliceStages, t.kc / 8 - s0), t.rows, 0, gids + t.out0});
+    L.n_items1 = (int)t1.size();
+    L.n_items2 = (int)t2.size();
+    std::vector<StGroupB> g1, g2;
+    for (const StoreGroup &g : L.groups1) g1.push_back(StGroupB{g.b_base, g.kc, g.K, gids + g.ids0});
+    for (const StoreGroup &g : L.groups2)
+        g2.push_back(StGroupB{b1 + g.b_base, g.kc, g.K, c->st_map.as<int>() + g.map0});
+    const size_t s1 = sizeof(StItem) * t1.size(), s2 = sizeof(StItem) * t2.size();
+    const size_t s3 = sizeof(StGroupB) * g1.size(), s4 = sizeof(StGroupB) * g2.size();
+    auto al256 = [](size_t x) { return (x + 255) & ~size_t(255); };
+    PSKEL_TRY(c->st_tiles.reserve(al256(s1) + al256(s2) + al256(s3) + al256(s4) + 256));
+    char *d = c->st_tiles.as<char>();
+    L.d_t1 = d;
+    L.d_t2 = d + al256(s1);
+    L.d_g1 = d + al256(s1) + al256(s2);
+    L.d_g2 = d + al256(s1) + al256(s2) + al256(s3);
+    if (s1) PSKEL_CUDA(cudaMemcpyAsync(L.d_t1, t1.data(), s1, cudaMemcpyHostToDevice, c->stream));
+    if (s2) PSKEL_CUDA(cudaMemcpyAsync(L.d_t2, t2.data(), s2, cudaMemcpyHostToDevice, c->stream));
+    if (s3) PSKEL_CUDA(cudaMemcpyAsync(L.d_g1, g1.data(), s3, cudaMemcpyHostToDevice, c->stream));
+    if (s4) PSKEL_CUDA(cudaMemcpyAsync(L.d_g2, g2.data(), s4, cudaMemcpyHostToDevice, c->stream));
+    PSKEL_CUDA(cudaStreamSynchronize(c->stream));
+    L.ready = true;
+    L.generation = c->generation;
+    if (bytes) *bytes = (long long)(2 * abytes);
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
+                                  void *stream) {
+    if (!c || !X || !Y || nrhs <= 0 || nrhs > kStRhs || ldx < c->mesh.ne || ldy < c->mesh.ne) {
+        set_error(PSKEL_ERR_ARG, "store_matvec: bad arguments (nrhs=%d, at most %d)", nrhs, kStRhs);
+        return PSKEL_ERR_ARG;
+    }
+    const StoreLayout &L = c->store;
+    if (!L.ready || L.generation != c->generation) {
+        set_error(PSKEL_ERR_STATE, "store_matvec: build the store after the last compression");
+        return PSKEL_ERR_STATE;
+    }
+    PSKEL_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    static bool attr = false;
+    if (!attr) {
+        PSKEL_CUDA(cudaFuncSetAttribute(store_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)kStSmem));
+        attr = true;
+    }
+    PSKEL_TRY(c->st_err.reserve(256));
+    PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
+    PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));
+    __nv_bfloat16 *ah = c->st_ah.as<__nv_bfloat16>(), *al = c->st_al.as<__nv_bfloat16>();
+    __nv_bfloat16 *bh = c->st_bh.as<__nv_bfloat16>(), *bl = c->st_bl.as<__nv_bfloat16>();
+    int *err = c->st_err.as<int>();
+    const int n1 = L.n_items1, n2 = L.n_items2;
+    const int ng1 = (int)L.groups1.size(), ng2 = (int)L.groups2.size();
+    const int sms = sm_count();
+    if (ng1 > 0) {
+        build_b1_kernel<<<ng1, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g1),
+                                             reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl);
+        PSKEL_LAUNCHED(1);
+    }
+    if (n1 > 0) {
+        store_gemm_kernel<<<std::min(n1, sms), 192, kStSmem, st>>>(
+            reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<float>(), nullptr, 0,
+            kStRhs, err);
+        PSKEL_LAUNCHED(1);
+    }
+    if (ng2 > 0) {
+        build_b2_kernel<<<ng2, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g2),
+                                             c->st_t.as<float>(), bh, bl);
+        PSKEL_LAUNCHED(1);
+    }
+    if (n2 > 0) {
+        store_gemm_kernel<<<std::min(n2, sms), 192, kStSmem, st>>>(
+            reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr,
+            reinterpret_cast<float *>(Y), ldy, nrhs, err);
+        PSKEL_LAUNCHED(1);
+    }
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_store_status(pskel_ctx *c, int *error_word) {
+    if (!c || !error_word) {
+        set_error(PSKEL_ERR_ARG, "store_status: null argument");
+        return PSKEL_ERR_ARG;
+    }
+    PSKEL_CUDA(cudaSetDevice(c->device));
+    *error_word = 0;
+    if (c->st_err.ptr) PSKEL_CUDA(cudaMemcpy(error_word, c->st_err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+    return PSKEL_OK;
+}

@@ -83,6 +83,9 @@ SIGNATURES = {
     "pskel_matvec": (ci, [VP, VP, ci, VP, ci, ci, ci, VP]),
     "pskel_recompress": (ci, [VP, cd, I32]),
     "pskel_get_recompressed": (ci, [VP, ci, VP, D, VP]),
+    "pskel_store_build": (ci, [VP, ctypes.POINTER(ctypes.c_longlong)]),
+    "pskel_store_matvec": (ci, [VP, VP, ci, VP, ci, ci, VP]),
+    "pskel_store_status": (ci, [VP, I32]),
     "pskel_mlp_num_params": (ci, []),
     "pskel_mlp_forward": (ci, [VP, VP, ci, VP, VP]),
     "pskel_mlp_grad": (ci, [VP, VP, VP, ci, VP, VP, VP]),

@@ -194,6 +194,35 @@ class Engine:
                                                     vp(Rp)))
         return Cp, S, Rp
 
+    def build_store(self) -> int:
+        """Compressed store of the recompressed blocks (after recompress()); returns its bytes."""
+        nbytes = ctypes.c_longlong()
+        _lib.check(self._lib.pskel_store_build(self._h, ctypes.byref(nbytes)))
+        return int(nbytes.value)
+
+    def store_matvec(self, X):
+        """Tensor-core matvec over the compressed store: X is a complex64 CUDA tensor
+        (RWG count, nrhs <= 16); returns Y of the same shape on the current stream."""
+        import torch
+        if X.dim() == 1:
+            return self.store_matvec(X[:, None])[:, 0]
+        if X.dtype != torch.complex64 or not X.is_cuda:
+            raise ValueError("X must be a complex64 CUDA tensor")
+        ne, nrhs = X.shape
+        Xc = X.t().contiguous()
+        Y = torch.empty_like(Xc)
+        s = torch.cuda.current_stream(X.device).cuda_stream
+        _lib.check(self._lib.pskel_store_matvec(self._h, ctypes.c_void_p(Xc.data_ptr()), ne,
+                                                ctypes.c_void_p(Y.data_ptr()), ne, nrhs,
+                                                ctypes.c_void_p(s)))
+        return Y.t()
+
+    def store_status(self) -> int:
+        """Error word of the last store_matvec (0 = every pipeline wait completed)."""
+        w = np.zeros(1, dtype=np.int32)
+        _lib.check(self._lib.pskel_store_status(self._h, w.ctypes.data_as(_lib.I32)))
+        return int(w[0])
+
     def set_fill_split(self, split_c128: int = -1, split_c64: int = -1):
         """Fill-kernel variant: 8 triangle moments (default), 0 two rows per thread, 1/2/4
         lanes per entry with a shuffle reduction, -1 unchanged."""

@@ -1,12 +1,15 @@
 """One small, repeatable compression workload for kernel profiling and variant timing.
 
     python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py PRECISION [CALLS] [SPLIT]
+    python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py store [CALLS]
 
 builds the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions, 0.5-lambda leaves), then
 makes CALLS (default 3) single-round compressions of every far block at a fixed sample count of
 24 with the given precision (c128 or c64) and fill variant (8: triangle moments, the default;
 0: two rows per thread; 1, 2, 4: lanes per entry), printing the fill time and point-pair
 rate of each call. Under a profiler the fill launch of call i is the i-th launch of the chosen fill kernel.
+The store form compresses the same sphere, recompresses it, builds the compressed store and runs
+CALLS tensor-core matvecs of 16 right-hand sides.
 """
 from __future__ import annotations
 
@@ -23,7 +26,34 @@ from pskel import octree  # noqa: E402
 from pskel.engine import Engine  # noqa: E402
 
 
+def store_case(calls):
+    """Compress the same sphere at tol 1e-4 (c64), recompress to 1e-4, build the compressed
+    store and run CALLS tensor-core matvecs with 16 right-hand sides."""
+    import torch
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        eng.recompress(1e-4)
+        nbytes = eng.build_store()
+        X = torch.randn((m.N, 16), dtype=torch.complex64, device="cuda")
+        for i in range(calls):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.store_matvec(X)
+            e1.record()
+            torch.cuda.synchronize()
+            print(f"store matvec call {i}: {e0.elapsed_time(e1):.4f} ms, store {nbytes / 1e6:.1f} MB, "
+                  f"status {eng.store_status()}", flush=True)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "store":
+        store_case(int(sys.argv[2]) if len(sys.argv) > 2 else 3)
+        return
     prec = sys.argv[1] if len(sys.argv) > 1 else "c64"
     calls = int(sys.argv[2]) if len(sys.argv) > 2 else 3
     split = int(sys.argv[3]) if len(sys.argv) > 3 else 8

@@ -280,6 +280,26 @@ int pskel_recompress(pskel_ctx *ctx, double thresh, int *ranks);
    R' k x n (complex128, column-major). Any pointer may be NULL. */
 int pskel_get_recompressed(pskel_ctx *ctx, int b, pskel_c128 *Cp, double *S, pskel_c128 *Rp);
 
+/* Compressed store of the recompressed blocks for the tensor-core matvec: diag(S) R' of the
+   blocks stacked per source group and C' stacked per test group, each real value split into a
+   bf16 hi + lo pair, in 128-row tiles laid out for the tensor cores. Requires pskel_recompress
+   after the last compression. bytes (may be NULL) receives the size of the two planes. No
+   reference counterpart (the reference keeps each block's C, U, R apart). */
+int pskel_store_build(pskel_ctx *ctx, long long *bytes);
+
+/* Y = sum over far blocks of C' diag(S) R' X for nrhs <= 16 right-hand sides, as two grouped
+   GEMMs on the tensor cores (tcgen05, bf16 hi/lo split, FP32 accumulation; relative error about
+   1e-5). X (ldx >= RWG count) and Y (ldy >= RWG count) are DEVICE arrays of pskel_c64,
+   column-major; Y is overwritten. Enqueued on stream (NULL: the legacy default stream);
+   returns without waiting. Replaces, for the recompressed blocks, the per-block C(U(R v)) of
+   user_impedance_for_julia_cuda.cu:1929-1960. */
+int pskel_store_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int nrhs,
+                       void *stream);
+
+/* Error word of the last pskel_store_matvec (0: every pipeline wait completed; 1: a bounded
+   wait ran out and the affected tiles were skipped). Waits for the device. */
+int pskel_store_status(pskel_ctx *ctx, int *error_word);
+
 /* ================================================= 3. rank / sample-count predictor (MLP) */
 /* 8 -> 64 -> 64 -> 1 MLP with GELU in FP32 (parameter layout W1[64x8] b1[64] W2[64x64] b2[64]
    W3[1x64] b3[1], row-major, contiguous). All pointers are DEVICE pointers; stream may be
