@@ -159,22 +159,21 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
 }
 
 // ============================================================== recompression (FP64)
-// For each block (C m x r, U r x r, R r x n):
-//   one-sided Jacobi  C V_c = B_c,  R^H V_r = B_r   (B orthogonal columns, sigma = column norms)
-//   core              M = diag(s_c) V_c^H U V_r diag(s_r)          (singular values of C U R)
-//   Jacobi            M V_m = B_m,  s_m = column norms, u_m = B_m / s_m
-//   C' = B_c diag(1/s_c) u_m,  R'^H = B_r diag(1/s_r) V_m,  S = s_m   (sorted, k kept where
-//   s_m > thresh * max s_m, the rule of svd_compress.m:25-28)
-// Columns of B_c, B_r below 1e-14 of their largest are dropped (they carry no part of C U R).
+// The restatement of svd_compress.m:19-33 for every block (C m x r, U r x r, R r x n):
+//   [Q_c, R_c] = qr(C),  [Q_r, R_r] = qr(R^H)           (Householder, batched)
+//   M = R_c U R_r^H = u s v^H                              (QR-preconditioned Jacobi SVD)
+//   keep the k values s > thresh * max s:  C' = Q_c u_k,  S = s_k,  R' = (Q_r v_k)^H
+// with C' and R'^H formed by applying the reflectors to [u_k; 0] and [v_k; 0].
 namespace pskel {
 
 struct RecompBlock {
     const void *C, *R;   // stored factors (storage type of the compression)
     const double2 *U;
-    double2 *Bc, *Vc, *Br, *Vr, *T, *M, *Vm, *Tc, *Tr, *Cp, *RpH, *Rp;
-    double *sc, *sr, *sm, *S;
-    int *pc, *pr, *pm, *k;
-    int *kout;  // the kept rank, in a table of all blocks
+    double2 *Bc, *Br;    // working copies of C (m x r) and R^H (n x r): reflectors after the QR
+    double2 *Rc, *Rr, *T, *M, *Vm, *Zc, *Zr, *Cp, *RpH, *Rp;
+    double2 *v0c, *v0r;
+    double *cc, *cr, *sm, *S;
+    int *pm, *kout;
     int m, n, r, ldr;
     double thresh;
 };
@@ -192,63 +191,29 @@ __global__ void recomp_load_kernel(const RecompBlock *__restrict__ jobs) {
     }
 }
 
-__device__ double block_max(const double *v, int n, double *red) {
-    double mx = 0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) mx = fmax(mx, v[i]);
-    red[threadIdx.x] = mx;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
-        __syncthreads();
-    }
-    const double r = red[0];
-    __syncthreads();
-    return r;
-}
-
-// M <- diag(s_c) M diag(s_r) with the small singular values of C and R dropped
-__global__ void __launch_bounds__(256) recomp_scale_kernel(const RecompBlock *__restrict__ jobs) {
-    __shared__ double red[256];
-    const RecompBlock w = jobs[blockIdx.x];
-    const double mc = block_max(w.sc, w.r, red), mr = block_max(w.sr, w.r, red);
-    for (int e = threadIdx.x; e < w.r * w.r; e += blockDim.x) {
-        const int i = e % w.r, j = e / w.r;
-        const double a = w.sc[i] > 1e-14 * mc ? w.sc[i] : 0.0;
-        const double b = w.sr[j] > 1e-14 * mr ? w.sr[j] : 0.0;
-        const double2 v = w.M[e];
-        w.M[e] = make_double2(v.x * a * b, v.y * a * b);
-    }
-}
-
-// Tc(:, t) = diag(1/s_c) B_m(:, pm[t]) / s_m[pm[t]],  Tr(:, t) = diag(1/s_r) V_m(:, pm[t]),
-// S[t] = s_m[pm[t]], k = #{s_m > thresh s_m,max}
+// u_k, v_k in the order of decreasing s: Zc(:, t) = (M V)(:, p_t) / s_{p_t}, Zr(:, t) = V(:, p_t),
+// S[t] = s_{p_t}; k = #{s > thresh s_max}
 __global__ void __launch_bounds__(256) recomp_factors_kernel(const RecompBlock *__restrict__ jobs) {
-    __shared__ double red[256];
     const RecompBlock w = jobs[blockIdx.x];
-    const double mc = block_max(w.sc, w.r, red), mr = block_max(w.sr, w.r, red);
     const double smax = w.sm[w.pm[0]];
     for (int e = threadIdx.x; e < w.r * w.r; e += blockDim.x) {
         const int i = e % w.r, t = e / w.r;
         const int c = w.pm[t];
         const double s = w.sm[c];
-        const double ic = w.sc[i] > 1e-14 * mc ? 1.0 / w.sc[i] : 0.0;
-        const double ir = w.sr[i] > 1e-14 * mr ? 1.0 / w.sr[i] : 0.0;
-        const double f = s > 0 ? ic / s : 0.0;
-        const double2 bm = w.M[i + (size_t)c * w.r];  // M holds B_m after the SVD
-        const double2 vm = w.Vm[i + (size_t)c * w.r];
-        w.Tc[e] = make_double2(bm.x * f, bm.y * f);
-        w.Tr[e] = make_double2(vm.x * ir, vm.y * ir);
+        const double f = s > 0 ? 1.0 / s : 0.0;
+        const double2 mv = w.M[i + (size_t)c * w.r];  // M holds M V after the SVD
+        w.Zc[e] = make_double2(mv.x * f, mv.y * f);
+        w.Zr[e] = w.Vm[i + (size_t)c * w.r];
     }
     for (int t = threadIdx.x; t < w.r; t += blockDim.x) w.S[t] = w.sm[w.pm[t]];
     if (threadIdx.x == 0) {
         int k = 0;
         for (int t = 0; t < w.r; ++t) k += w.sm[w.pm[t]] > w.thresh * smax;
-        *w.k = k;
         *w.kout = k;
     }
 }
 
-// R' = (R'^H)^H : r x n from n x r
+// R' = (R'^H)^H : r x n (first k rows valid) from n x r
 __global__ void recomp_rp_kernel(const RecompBlock *__restrict__ jobs) {
     const RecompBlock w = jobs[blockIdx.x];
     for (int e = threadIdx.x; e < w.r * w.n; e += blockDim.x) {
@@ -268,10 +233,8 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     PSKEL_CUDA(cudaSetDevice(c->device));
     const int nb = c->n_blocks;
     const bool f32 = c->precision == PSKEL_C64;
-    // workspace (all FP64 complex): Bc m r, Br n r, Vc Vr T M Vm Tc Tr r r each, Cp m r, RpH n r,
-    // Rp r n, plus real vectors
-    std::vector<size_t> off(nb + 1, 0);
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
+    std::vector<size_t> off(nb + 1, 0);
     for (int b = 0; b < nb; ++b) {
         const BlockResult &res = c->results[b];
         if (res.arena < 0) {
@@ -279,18 +242,27 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
             return PSKEL_ERR_STATE;
         }
         const size_t m = res.m, n = res.n, r = res.r;
-        size_t s = al(16 * m * r) * 2 + al(16 * n * r) * 2 + al(16 * r * n) + 7 * al(16 * r * r) +
-                   4 * al(8 * r) + 4 * al(4 * r) + 256;
-        off[b + 1] = off[b] + s;
+        off[b + 1] = off[b] + 2 * al(16 * m * r) + 3 * al(16 * n * r) + 8 * al(16 * r * r) +
+                     2 * al(16 * r) + 4 * al(8 * r) + al(4 * r) + 256;
     }
     PSKEL_TRY(c->recomp.reserve(off[nb] + 256));
     char *base = c->recomp.as<char>();
     std::vector<RecompBlock> jobs(nb);
-    std::vector<SvdJob> svd1, svd2;
-    svd1.reserve(2 * nb);
-    svd2.reserve(nb);
-    std::vector<ZgemmJob> g1, g2, g3;
+    std::vector<QrJob> qrs;
+    qrs.reserve(2 * nb);
+    std::vector<SvdJob> svds;
+    svds.reserve(nb);
+    std::vector<ZgemmJob> g1, g2;
+    std::vector<ApplyQJob> aps;
+    aps.reserve(2 * nb);
     c->recomp_slots.assign(nb, {});
+    // device job tables (the k table is referenced by the apply jobs)
+    const size_t jb = sizeof(RecompBlock) * nb, s2 = sizeof(SvdJob) * nb;
+    PSKEL_TRY(c->tmp.reserve(al(jb) + al(s2) + sizeof(int) * nb + 1024));
+    char *d = c->tmp.as<char>();
+    RecompBlock *d_jobs = reinterpret_cast<RecompBlock *>(d);
+    SvdJob *d_s2 = reinterpret_cast<SvdJob *>(d + al(jb));
+    int *d_k = reinterpret_cast<int *>(d + al(jb) + al(s2));
     for (int b = 0; b < nb; ++b) {
         const BlockResult &res = c->results[b];
         const char *kb = c->arenas[res.arena].keep.as<char>();
@@ -306,75 +278,58 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         w.Br = reinterpret_cast<double2 *>(take(16 * n * r));
         w.RpH = reinterpret_cast<double2 *>(take(16 * n * r));
         w.Rp = reinterpret_cast<double2 *>(take(16 * r * n));
-        w.Vc = reinterpret_cast<double2 *>(take(16 * r * r));
-        w.Vr = reinterpret_cast<double2 *>(take(16 * r * r));
+        w.Rc = reinterpret_cast<double2 *>(take(16 * r * r));
+        w.Rr = reinterpret_cast<double2 *>(take(16 * r * r));
         w.T = reinterpret_cast<double2 *>(take(16 * r * r));
         w.M = reinterpret_cast<double2 *>(take(16 * r * r));
         w.Vm = reinterpret_cast<double2 *>(take(16 * r * r));
-        w.Tc = reinterpret_cast<double2 *>(take(16 * r * r));
-        w.Tr = reinterpret_cast<double2 *>(take(16 * r * r));
-        w.sc = reinterpret_cast<double *>(take(8 * r));
-        w.sr = reinterpret_cast<double *>(take(8 * r));
+        w.Zc = reinterpret_cast<double2 *>(take(16 * r * r));
+        w.Zr = reinterpret_cast<double2 *>(take(16 * r * r));
+        take(16 * r * r);  // spare
+        w.v0c = reinterpret_cast<double2 *>(take(16 * r));
+        w.v0r = reinterpret_cast<double2 *>(take(16 * r));
+        w.cc = reinterpret_cast<double *>(take(8 * r));
+        w.cr = reinterpret_cast<double *>(take(8 * r));
         w.sm = reinterpret_cast<double *>(take(8 * r));
         w.S = reinterpret_cast<double *>(take(8 * r));
-        w.pc = reinterpret_cast<int *>(take(4 * r));
-        w.pr = reinterpret_cast<int *>(take(4 * r));
         w.pm = reinterpret_cast<int *>(take(4 * r));
-        w.k = reinterpret_cast<int *>(take(4 * r));
+        w.kout = d_k + b;
         w.m = res.m;
         w.n = res.n;
         w.r = res.r;
         w.ldr = res.r + res.pe;
         w.thresh = thresh;
-        svd1.push_back(SvdJob{w.Bc, w.Vc, w.sc, w.pc, res.m, res.r, 0, 0});
-        svd1.push_back(SvdJob{w.Br, w.Vr, w.sr, w.pr, res.n, res.r, 0, 0});
-        svd2.push_back(SvdJob{w.M, w.Vm, w.sm, w.pm, res.r, res.r, 0, 0});
-        g1.push_back(zjob(w.U, res.r, ZOP_N, w.Vr, res.r, ZOP_N, w.T, res.r, res.r, res.r, res.r));
-        g2.push_back(zjob(w.Vc, res.r, ZOP_C, w.T, res.r, ZOP_N, w.M, res.r, res.r, res.r, res.r));
-        g3.push_back(zjob(w.Bc, res.m, ZOP_N, w.Tc, res.r, ZOP_N, w.Cp, res.m, res.m, res.r, res.r));
-        g3.push_back(zjob(w.Br, res.n, ZOP_N, w.Tr, res.r, ZOP_N, w.RpH, res.n, res.n, res.r, res.r));
+        qrs.push_back(QrJob{w.Bc, w.Rc, w.v0c, w.cc, res.m, res.r});
+        qrs.push_back(QrJob{w.Br, w.Rr, w.v0r, w.cr, res.n, res.r});
+        // M = R_c (U R_r^H)
+        g1.push_back(zjob(w.U, res.r, ZOP_N, w.Rr, res.r, ZOP_C, w.T, res.r, res.r, res.r, res.r));
+        g2.push_back(zjob(w.Rc, res.r, ZOP_N, w.T, res.r, ZOP_N, w.M, res.r, res.r, res.r, res.r));
+        svds.push_back(SvdJob{w.M, w.Vm, w.sm, w.pm, res.r, res.r, 0, 0});
+        aps.push_back(ApplyQJob{w.Bc, w.v0c, w.cc, res.m, res.r, w.Zc, res.r, w.Cp, res.m, res.r, w.kout});
+        aps.push_back(ApplyQJob{w.Br, w.v0r, w.cr, res.n, res.r, w.Zr, res.r, w.RpH, res.n, res.r, w.kout});
         c->recomp_slots[b] = RecompSlot{(size_t)((char *)w.Cp - base), (size_t)((char *)w.Rp - base),
                                         (size_t)((char *)w.S - base), 0};
     }
-    // device job tables
-    const size_t jb = sizeof(RecompBlock) * nb, s1 = sizeof(SvdJob) * svd1.size(),
-                 s2 = sizeof(SvdJob) * svd2.size();
-    PSKEL_TRY(c->tmp.reserve(jb + s1 + s2 + sizeof(int) * nb + 1024));
-    char *d = c->tmp.as<char>();
-    RecompBlock *d_jobs = reinterpret_cast<RecompBlock *>(d);
-    SvdJob *d_s1 = reinterpret_cast<SvdJob *>(d + ((jb + 255) & ~size_t(255)));
-    SvdJob *d_s2 = reinterpret_cast<SvdJob *>(reinterpret_cast<char *>(d_s1) + ((s1 + 255) & ~size_t(255)));
-    int *d_k = reinterpret_cast<int *>(reinterpret_cast<char *>(d_s2) + ((s2 + 255) & ~size_t(255)));
-    for (int b = 0; b < nb; ++b) jobs[b].kout = d_k + b;
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
-    PSKEL_CUDA(cudaMemcpyAsync(d_s1, svd1.data(), s1, cudaMemcpyHostToDevice, c->stream));
-    PSKEL_CUDA(cudaMemcpyAsync(d_s2, svd2.data(), s2, cudaMemcpyHostToDevice, c->stream));
+    PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, c->stream));
     if (f32) recomp_load_kernel<float2><<<nb, 256, 0, c->stream>>>(d_jobs);
     else recomp_load_kernel<double2><<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(batched_svd(d_s1, svd1, 60, c->stream, c->tmp2));
+    PSKEL_TRY(batched_qr(qrs, c->stream, c->tmp2));
     PSKEL_TRY(launch_zgemm(g1, c->stream, c->tmp3));
     PSKEL_TRY(launch_zgemm(g2, c->stream, c->tmp3));
-    recomp_scale_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
-    PSKEL_LAUNCHED(1);
-    PSKEL_TRY(batched_svd(d_s2, svd2, 60, c->stream, c->tmp2));
+    PSKEL_TRY(batched_svd(d_s2, svds, 60, c->stream, c->tmp2));
     recomp_factors_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(launch_zgemm(g3, c->stream, c->tmp3));
+    PSKEL_TRY(batched_apply_q(aps, c->stream, c->tmp3));
     recomp_rp_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
     // ranks and SVD statuses back to the host
-    std::vector<SvdJob> h1(svd1.size()), h2(svd2.size());
-    PSKEL_CUDA(cudaMemcpyAsync(h1.data(), d_s1, s1, cudaMemcpyDeviceToHost, c->stream));
-    PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<SvdJob> h2(nb);
     std::vector<int> ks(nb);
+    PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(ks.data(), d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
-    for (const SvdJob &j : h1)
-        if (j.status != PSKEL_OK) {
-            set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a factor did not converge");
-            return PSKEL_ERR_NOCONV;
-        }
     for (const SvdJob &j : h2)
         if (j.status != PSKEL_OK) {
             set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a core did not converge");

@@ -199,6 +199,34 @@ struct PinvJob {
 };
 int batched_pinv(const PinvJob *d_jobs, int njobs, int max_n, cudaStream_t stream);
 
+// Householder QR of m x n complex matrices (m >= n), in place: the reflector tails below the
+// diagonal of A, v(0) and coef = 2 / |v|^2 of each reflector in v0 / coef, R (n x n, zero below
+// the diagonal) in R. Job tables go through scratch.
+struct QrJob {
+    double2 *A;
+    double2 *R;
+    double2 *v0;
+    double *coef;
+    int m, n;
+};
+int batched_qr(const std::vector<QrJob> &h_jobs, cudaStream_t stream, DevBuf &scratch);
+
+// Y (m x kcols, ld ldy) = Q [Z; 0] for the Q of a batched_qr job (reflectors A, v0, coef; Z is
+// n x kcols, ld ldz); kcols = min(k, *kp) when kp is given (a device count).
+struct ApplyQJob {
+    const double2 *A;
+    const double2 *v0;
+    const double *coef;
+    int m, n;
+    const double2 *Z;
+    int ldz;
+    double2 *Y;
+    int ldy;
+    int k;
+    const int *kp;
+};
+int batched_apply_q(const std::vector<ApplyQJob> &h_jobs, cudaStream_t stream, DevBuf &scratch);
+
 // ------------------------------------------------------------------ small dense helpers
 // y = C (U (R x)) and the successive-estimate error of the reference (complex128).
 int cur_matvec_error(const double2 *C, const double2 *U, const double2 *R, const double2 *x,
