@@ -34,10 +34,11 @@ for _p in (ROOT, PKG):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
+from pskel import roofline  # noqa: E402
+
 METRIC = "far-block CUR compress time @ rel err 1e-4: learned+mixed+batched vs plain GPU"
 K_WAVE, ETA = 2 * np.pi, 376.73
 TOL = 1e-4
-FLOPS_PER_PAIR = 32  # fixed convention for one point-pair evaluation (see roofline.py)
 
 WORKLOADS = {
     "sphere30k": dict(R=2.0, sub=5, leaf=0.5, min_group=40,
@@ -271,7 +272,7 @@ def run_ours(args, rank, world, dev):
     fp32_peak = ctypes.c_double()
     fp64_peak = ctypes.c_double()
     _lib.check(L.pskel_fma_peak(ctypes.byref(fp32_peak), ctypes.byref(fp64_peak)))
-    achieved = tph["point_pairs"] * FLOPS_PER_PAIR / (tph["fill"] * 1e-3) / 1e12
+    achieved = roofline.fill_flops(tph["point_pairs"]) / (tph["fill"] * 1e-3) / 1e12
     # accuracy of the timed product and of the plain baseline against dense FP64 fills
     st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     err = eng.true_errors()
@@ -357,9 +358,9 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     mv_launches = (L.pskel_kernel_launches() - l0) // reps
     mv_ms = float(np.mean(times))
     mm, nn, rr = (st[k].astype(np.float64) for k in ("m", "n", "r"))
-    factor_bytes = float(((mm + nn) * rr * 8 + rr * rr * 16).sum())
-    vec_bytes = float(((mm + nn) * nrhs * 8).sum())
-    flops = float((8 * (mm + nn) * rr * nrhs + 8 * rr * rr * nrhs).sum())
+    factor_bytes = roofline.matvec_bytes(mm, nn, rr, 0, 8.0, 16.0)
+    vec_bytes = roofline.matvec_bytes(mm, nn, 0 * rr, nrhs, 0.0)
+    flops = roofline.matvec_flops(mm, nn, rr, nrhs)
     peak = _hbm_peak()
     gbs = (factor_bytes + vec_bytes) / (mv_ms * 1e-3) / 1e9
     # recompression to the compression tolerance
@@ -389,7 +390,7 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     st_ms = float(np.mean(st_times))
     st_status = eng.store_status()
     kk = ks.astype(np.float64)
-    st_alg_bytes = float(((mm + nn) * kk * 2 * 4).sum())  # bf16 hi + lo of [re | im] per entry
+    st_alg_bytes = roofline.matvec_bytes(mm, nn, kk, 0, 8.0)  # bf16 hi + lo of re and im
     st_gbs = (st_alg_bytes + vec_bytes) / (st_ms * 1e-3) / 1e9
     return dict(
         matvec=dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),

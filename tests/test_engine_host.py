@@ -22,3 +22,15 @@ def test_opts_layout():
     # pskel_opts_t: 2 doubles, 8 ints, uint64, 2 doubles, 2 ints
     assert ctypes.sizeof(_lib.Opts) == 80
     assert ctypes.sizeof(_lib.EM) == 24
+
+
+def test_roofline_work_counts():
+    """The fixed work conventions of the roofline numerators."""
+    from pskel import roofline
+    assert roofline.FLOPS_PER_PAIR == 32
+    assert roofline.fill_flops(10) == 320
+    assert roofline.pinv_flops([2]) == 92 * 8
+    assert roofline.matvec_flops([4], [5], [3], 2) == 8 * 2 * (12 + 9 + 15)
+    # 30 factor entries of 8 bytes, 9 core entries of 16 bytes, 2 x 9 vector entries of 8 bytes
+    assert roofline.matvec_bytes([4], [6], [3], 2, 8.0, 16.0) == 30 * 8 + 9 * 16 + 2 * 10 * 8
+    assert roofline.recompress_flops([4], [6], [2], [1]) == 8 * (2 * 4 * 4 + 2 * 6 * 4) + 84 * 8 + 8 * 10 * 2
