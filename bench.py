@@ -51,6 +51,10 @@ WORKLOADS = {
                             "octree leaf 0.5 lambda"),
 }
 
+# DRAM bytes (read + write) of the round-1 fill launch of the product step on sphere30k, from
+# one ncu capture (profiles/tri_fill_traffic_sphere30k.md)
+FILL_TRAFFIC_BYTES = 5.534e9
+
 PRODUCT = dict(precision="c64", tau=1e-7, extra_rows=16, extra_cols=16, est_safety=2.0,
                oversample=0, max_rounds=12, seed=0)
 PLAIN = dict(precision="c128", tau=1e-7, extra_rows=16, extra_cols=16, est_safety=2.0,
@@ -317,7 +321,11 @@ def run_ours(args, rank, world, dev):
                    blocks_over_tol=None if err_plain is None else int((err_plain > TOL).sum())),
         roofline=dict(bound="alu", kernel="tri_fill_kernel<float,7> (c64 triangle moments, FP64 geometry)",
                       achieved=round(achieved, 3), peak=round(fp32_peak.value, 3), unit="TFLOP/s",
-                      frac=round(achieved / fp32_peak.value, 4), traffic=None,
+                      frac=round(achieved / fp32_peak.value, 4),
+                      traffic=FILL_TRAFFIC_BYTES if args.workload == "sphere30k" else None,
+                      traffic_source="dram__bytes_read.sum + dram__bytes_write.sum of the round-1 fill "
+                                     "launch, one ncu capture of this workload "
+                                     "(profiles/tri_fill_traffic_sphere30k.md)",
                       peak_source="measured FP32 FMA microbenchmark on this GPU (pskel_fma_peak); "
                                   f"FP64 FMA {fp64_peak.value:.2f} TFLOP/s",
                       flops="32 flops per point-pair evaluation x point pairs / fill device time",

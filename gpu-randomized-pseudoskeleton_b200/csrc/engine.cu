@@ -197,36 +197,64 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
         }
     }
     __syncthreads();
+    // residuals on the extra rows (Z(Ix, j) - Tr R(:, j)) and the extra columns
+    // (Z(i, Jx) - C(i, :) Sc): each thread keeps up to kEstChunk independent complex accumulators,
+    // reading each factor value once per k
+    constexpr int kEstChunk = 8;
     double nr_ = 0, dr_ = 0, nc_ = 0, dc_ = 0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {  // extra rows, column j
         const S *col = Rx + (size_t)j * ldr;
-        for (int e = 0; e < pe; ++e) {
-            double zx = 0, zy = 0;
+        for (int e0 = 0; e0 < pe; e0 += kEstChunk) {
+            double zx[kEstChunk], zy[kEstChunk];
+#pragma unroll
+            for (int q = 0; q < kEstChunk; ++q) zx[q] = zy[q] = 0.0;
             for (int k = 0; k < r; ++k) {
-                const double2 t = Tr[e + k * pe];
                 const double2 rv = promote(col[k]);
-                zx = fma(t.x, rv.x, fma(-t.y, rv.y, zx));
-                zy = fma(t.x, rv.y, fma(t.y, rv.x, zy));
+#pragma unroll
+                for (int q = 0; q < kEstChunk; ++q) {
+                    if (e0 + q < pe) {
+                        const double2 t = Tr[e0 + q + k * pe];
+                        zx[q] = fma(t.x, rv.x, fma(-t.y, rv.y, zx[q]));
+                        zy[q] = fma(t.x, rv.y, fma(t.y, rv.x, zy[q]));
+                    }
+                }
             }
-            const double2 x = promote(col[r + e]);
-            const double dx = x.x - zx, dy = x.y - zy;
-            nr_ = fma(dx, dx, fma(dy, dy, nr_));
-            dr_ = fma(x.x, x.x, fma(x.y, x.y, dr_));
+#pragma unroll
+            for (int q = 0; q < kEstChunk; ++q) {
+                if (e0 + q < pe) {
+                    const double2 x = promote(col[r + e0 + q]);
+                    const double dx = x.x - zx[q], dy = x.y - zy[q];
+                    nr_ = fma(dx, dx, fma(dy, dy, nr_));
+                    dr_ = fma(x.x, x.x, fma(x.y, x.y, dr_));
+                }
+            }
         }
     }
     for (int i = threadIdx.x; i < m; i += blockDim.x) {  // extra columns, row i
-        for (int cc = 0; cc < pc; ++cc) {
-            double zx = 0, zy = 0;
+        for (int c0 = 0; c0 < pc; c0 += kEstChunk) {
+            double zx[kEstChunk], zy[kEstChunk];
+#pragma unroll
+            for (int q = 0; q < kEstChunk; ++q) zx[q] = zy[q] = 0.0;
             for (int k = 0; k < r; ++k) {
-                const double2 c = promote(C[i + (size_t)k * m]);
-                const double2 t = Sc[k + cc * r];
-                zx = fma(c.x, t.x, fma(-c.y, t.y, zx));
-                zy = fma(c.x, t.y, fma(c.y, t.x, zy));
+                const double2 cv = promote(C[i + (size_t)k * m]);
+#pragma unroll
+                for (int q = 0; q < kEstChunk; ++q) {
+                    if (c0 + q < pc) {
+                        const double2 t = Sc[k + (c0 + q) * r];
+                        zx[q] = fma(cv.x, t.x, fma(-cv.y, t.y, zx[q]));
+                        zy[q] = fma(cv.x, t.y, fma(cv.y, t.x, zy[q]));
+                    }
+                }
             }
-            const double2 x = promote(C[i + (size_t)(r + cc) * m]);
-            const double dx = x.x - zx, dy = x.y - zy;
-            nc_ = fma(dx, dx, fma(dy, dy, nc_));
-            dc_ = fma(x.x, x.x, fma(x.y, x.y, dc_));
+#pragma unroll
+            for (int q = 0; q < kEstChunk; ++q) {
+                if (c0 + q < pc) {
+                    const double2 x = promote(C[i + (size_t)(r + c0 + q) * m]);
+                    const double dx = x.x - zx[q], dy = x.y - zy[q];
+                    nc_ = fma(dx, dx, fma(dy, dy, nc_));
+                    dc_ = fma(x.x, x.x, fma(x.y, x.y, dc_));
+                }
+            }
         }
     }
     s_red[0][threadIdx.x] = nr_;
