@@ -477,7 +477,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     std::vector<int> prefix(fills.size() + 1, 0);
     if (p.tri) {
         for (size_t i = 0; i < gfills.size(); ++i)
-            prefix[i + 1] = prefix[i] + (gfills[i].nc + kTriFillCols - 1) / kTriFillCols;
+            prefix[i + 1] = prefix[i] + (gfills[i].nc + c->tri_cols - 1) / c->tri_cols;
     } else {
         for (size_t i = 0; i < fills.size(); ++i)
             prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
@@ -536,6 +536,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.q_src = c->em.q_src;
     fp.precision = o.precision;
     fp.split = entry_split_for(c, o.precision);
+    fp.tri_cols = c->tri_cols;
     if (p.tri)
         PSKEL_TRY(launch_tri_fill(c->mesh, fp, p.d_gfill, p.d_fill_prefix, p.fill_jobs,
                                   p.fill_tiles, s));
@@ -858,6 +859,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back((int)std::lround(std::log10(std::max(o.tau, 1e-300)) * 1000));
             key.push_back(o.tau_relative);
             key.push_back(c->split[0] * 8 + c->split[1] + (c->use_tri ? 1000 : 0));
+            key.push_back(c->tri_cols);
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -1001,6 +1003,16 @@ extern "C" int pskel_set_fill_split(pskel_ctx *c, int split_c128, int split_c64)
     return PSKEL_OK;
 }
 
+extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
+    PSKEL_TRY(ctx_ok(c));
+    if (cols != 4 && cols != 8 && cols != 16) {
+        set_error(PSKEL_ERR_ARG, "triangle-moment fill: %d columns per tile (4, 8 or 16)", cols);
+        return PSKEL_ERR_ARG;
+    }
+    c->tri_cols = cols;
+    return PSKEL_OK;
+}
+
 extern "C" int pskel_last_timing(pskel_ctx *c, double *out, int n) {
     PSKEL_TRY(ctx_ok(c));
     if (!out || n < 0) {
@@ -1109,7 +1121,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
                                      c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt],
                                      c->d_gids.as<int>() + c->gptr[c->gs[b]], Z, res.m,
                                      c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], res.n, res.m, 0, 0};
-            prefix[i + 1] = prefix[i] + (tri ? (res.n + kTriFillCols - 1) / kTriFillCols
+            prefix[i + 1] = prefix[i] + (tri ? (res.n + c->tri_cols - 1) / c->tri_cols
                                                      : ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn));
             mats[i] = Z;
             sizes[i] = (long long)res.m * res.n;
@@ -1174,6 +1186,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         fp.q_src = c->em.q_src;
         fp.precision = PSKEL_C128;
         fp.split = entry_split_for(c, PSKEL_C128);
+        fp.tri_cols = c->tri_cols;
         if (tri)
             PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d_f), d_p, nbb,
                                       prefix.back(), c->stream));

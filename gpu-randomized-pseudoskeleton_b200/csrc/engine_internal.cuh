@@ -99,6 +99,7 @@ struct pskel_ctx {
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;
     int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
+    int tri_cols = pskel::kTriFillColsDefault;  // columns per CTA of the triangle-moment fill
     double timing[13] = {};  // [0..11] as reported by pskel_last_timing, [12] core SVD count
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;

@@ -692,12 +692,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     }
 }
 
-template <typename T, int Q>
+template <typename T, int Q, int TN>
 static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillParams &p,
                         const GroupFillJob *d_jobs, const int *d_prefix, int njobs,
                         int total_tiles, cudaStream_t stream) {
     constexpr int NP = 2 * Q;
-    constexpr int TN = kTriFillCols;
     const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
                         2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
     auto kern = tri_fill_kernel<T, Q, TN>;
@@ -736,11 +735,26 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
         set_error(PSKEL_ERR_STATE, "tri fill: records for Q=%d not built", p.q_test);
         return PSKEL_ERR_STATE;
     }
-    if (p.precision == PSKEL_C128)
-        return p.q_test == 7 ? launch_tri_t<double, 7>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
-                             : launch_tri_t<double, 1>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream);
-    return p.q_test == 7 ? launch_tri_t<float, 7>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
-                         : launch_tri_t<float, 1>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream);
+#define PSKEL_TRI(T, Q, TN) \
+    return launch_tri_t<T, Q, TN>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
+#define PSKEL_TRI_TN(T, Q)                     \
+    do {                                       \
+        if (p.tri_cols == 4) PSKEL_TRI(T, Q, 4);   \
+        if (p.tri_cols == 16) PSKEL_TRI(T, Q, 16); \
+        PSKEL_TRI(T, Q, 8);                    \
+    } while (0)
+    if (p.tri_cols != 4 && p.tri_cols != 8 && p.tri_cols != 16) {
+        set_error(PSKEL_ERR_ARG, "tri fill: %d columns per tile (4, 8 or 16)", p.tri_cols);
+        return PSKEL_ERR_ARG;
+    }
+    if (p.precision == PSKEL_C128) {
+        if (p.q_test == 7) PSKEL_TRI_TN(double, 7);
+        PSKEL_TRI_TN(double, 1);
+    }
+    if (p.q_test == 7) PSKEL_TRI_TN(float, 7);
+    PSKEL_TRI_TN(float, 1);
+#undef PSKEL_TRI_TN
+#undef PSKEL_TRI
 }
 
 // ---------------------------------------------------------------- diagnostics

@@ -107,12 +107,16 @@ struct FillJob {
                 // caller fill Z(a, b) as the transpose of Z(b, a) with the long side on rows)
 };
 
+constexpr int kTriFillCols = 16;        // most columns per CTA tile (variants 4, 8, 16)
+constexpr int kTriFillColsDefault = 8;
+
 struct FillParams {
     double k, eta;
     double r_near;     // > 0: flag triangle pairs whose centroids are closer than this
     int q_test, q_src;
     int precision;     // PSKEL_C128 / PSKEL_C64
     int split;         // 0: two rows per thread (default kernel); 1, 2, 4: lanes per entry
+    int tri_cols = kTriFillColsDefault;  // columns per CTA of the triangle-moment fill (4, 8, 16)
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the
@@ -134,7 +138,6 @@ struct GroupFillJob {
     int m, nt, nc, ld, trans, pad;
 };
 constexpr int kTriFillMaxRows = 512;  // largest group the triangle-moment fill accepts
-constexpr int kTriFillCols = 8;       // columns per CTA tile
 int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob *d_jobs,
                     const int *d_tile_prefix, int njobs, int total_tiles, cudaStream_t stream);
 

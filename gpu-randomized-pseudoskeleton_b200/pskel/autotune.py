@@ -1,0 +1,80 @@
+"""Autotuner of the fill launch: times the fill variants on the engine's own block list and
+keeps the fastest.
+
+The variants are the triangle-moment kernel with 4, 8 or 16 columns per CTA tile (usable while
+every group has at most 512 RWG) and the per-entry kernels (two rows per thread; 1, 2 or 4 lanes
+per entry with a shuffle reduction over the quadrature points). Each candidate runs one
+single-round compression of every block at a fixed sample count (the first round's fill, the
+launch that dominates a compression) and is timed by the engine's own device events
+(`Engine.timing()['fill']`); the best of `repeats` runs counts. The choice is applied to the
+engine and returned with the timings, and can be cached in a JSON file keyed by the GPU name and
+a signature of the workload.
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+
+TRI_VARIANTS = [("tri", 4), ("tri", 8), ("tri", 16)]
+ENTRY_VARIANTS = [("entry", 0), ("entry", 1), ("entry", 2), ("entry", 4)]
+
+
+def _apply(eng, precision, variant):
+    kind, v = variant
+    if kind == "tri":
+        eng.set_tri_cols(v)
+        split = 8
+    else:
+        split = v
+    if precision == "c128":
+        eng.set_fill_split(split_c128=split)
+    else:
+        eng.set_fill_split(split_c64=split)
+
+
+def signature(eng, precision: str, q: int) -> str:
+    sizes = np.diff(np.asarray(eng._gp))
+    return f"{precision}-q{q}-rwg{eng.mesh.N}-blocks{eng.n_blocks}-gmax{int(sizes.max())}"
+
+
+def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int = 2,
+                  include_entry: bool = False, cache: str | None = None, gpu_name: str = "",
+                  q: int = 7) -> dict:
+    """Time the fill variants on eng's blocks and apply the fastest; returns
+    {"choice": (kind, value), "ms": {variant: fill ms}, "cached": bool}."""
+    key = f"{gpu_name}|{signature(eng, precision, q)}"
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            table = json.load(f)
+        if key in table:
+            choice = tuple(table[key]["choice"])
+            _apply(eng, precision, choice)
+            return {"choice": choice, "ms": table[key]["ms"], "cached": True}
+    sizes = np.diff(np.asarray(eng._gp))
+    variants = list(TRI_VARIANTS) if sizes.max() <= 512 else []
+    if include_entry or not variants:
+        variants += ENTRY_VARIANTS
+    r0 = np.minimum(samples, np.minimum(sizes[eng._gt], sizes[eng._gs])).astype(np.int32)
+    timings = {}
+    for variant in variants:
+        _apply(eng, precision, variant)
+        best = float("inf")
+        for rep in range(repeats + 1):  # the first run sets kernel attributes and warms up
+            eng.compress(1.0, precision=precision, r0=r0, oversample=0, max_rounds=1, seed=rep)
+            if rep > 0:
+                best = min(best, eng.timing()["fill"])
+        timings[f"{variant[0]}{variant[1]}"] = round(best, 4)
+    best_name = min(timings, key=timings.get)
+    choice = next(v for v in variants if f"{v[0]}{v[1]}" == best_name)
+    _apply(eng, precision, choice)
+    if cache:
+        table = {}
+        if os.path.exists(cache):
+            with open(cache) as f:
+                table = json.load(f)
+        table[key] = {"choice": list(choice), "ms": timings}
+        with open(cache, "w") as f:
+            json.dump(table, f, indent=1)
+    return {"choice": choice, "ms": timings, "cached": False}

@@ -228,6 +228,10 @@ class Engine:
         lanes per entry with a shuffle reduction, -1 unchanged."""
         _lib.check(self._lib.pskel_set_fill_split(self._h, int(split_c128), int(split_c64)))
 
+    def set_tri_cols(self, cols: int):
+        """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
+        _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
+
     def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,
                     precision="c128"):
         """Fill into device buffers given as raw device pointers (e.g. torch data_ptr())."""

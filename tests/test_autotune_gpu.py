@@ -1,0 +1,60 @@
+"""Fill-variant autotuner: the triangle-moment fill gives the same entries for every tile width,
+and the autotuner picks one of the timed variants and leaves the engine compressing correctly."""
+import json
+
+import numpy as np
+import pytest
+
+from pskel import autotune
+from pskel import mesh as pmesh
+from pskel import octree
+from pskel.engine import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sphere():
+    m = pmesh.icosphere(2.0, 3)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=20)
+    return m, part
+
+
+@pytest.mark.parametrize("prec", ["c64", "c128"])
+def test_tile_widths_agree(sphere, prec):
+    m, part = sphere
+    out = {}
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        r0 = np.full(eng.n_blocks, 12, dtype=np.int32)
+        for cols in (4, 8, 16):
+            eng.set_tri_cols(cols)
+            st = eng.compress(1.0, precision=prec, r0=r0, oversample=0, max_rounds=1, seed=9)
+            out[cols] = [eng.get_block(b, st)[0] for b in (0, eng.n_blocks // 2, eng.n_blocks - 1)]
+        with pytest.raises(RuntimeError):
+            eng.set_tri_cols(5)
+    bar = 1e-6 if prec == "c64" else 1e-13
+    for cols in (4, 16):
+        for a, b in zip(out[cols], out[8]):
+            assert np.abs(a - b).max() <= bar * np.abs(b).max()
+
+
+def test_autotune_picks_a_variant(sphere, tmp_path):
+    m, part = sphere
+    cache = str(tmp_path / "tune.json")
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        rep = autotune.autotune_fill(eng, "c64", samples=16, repeats=1, include_entry=True,
+                                     cache=cache, gpu_name="test")
+        assert not rep["cached"]
+        assert set(rep["ms"]) == {"tri4", "tri8", "tri16", "entry0", "entry1", "entry2", "entry4"}
+        best = min(rep["ms"], key=rep["ms"].get)
+        assert f"{rep['choice'][0]}{rep['choice'][1]}" == best
+        st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        err = eng.true_errors()
+        assert np.median(err) < 1e-4 and np.all(st["status"] == 0)
+        rep2 = autotune.autotune_fill(eng, "c64", cache=cache, gpu_name="test")
+        assert rep2["cached"] and tuple(rep2["choice"]) == tuple(rep["choice"])
+    assert "test|" in next(iter(json.load(open(cache))))
