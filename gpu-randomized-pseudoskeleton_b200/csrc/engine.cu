@@ -537,6 +537,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.precision = o.precision;
     fp.split = entry_split_for(c, o.precision);
     fp.tri_cols = c->tri_cols;
+    fp.geom32 = c->geom32;
     if (p.tri)
         PSKEL_TRY(launch_tri_fill(c->mesh, fp, p.d_gfill, p.d_fill_prefix, p.fill_jobs,
                                   p.fill_tiles, s));
@@ -859,7 +860,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back((int)std::lround(std::log10(std::max(o.tau, 1e-300)) * 1000));
             key.push_back(o.tau_relative);
             key.push_back(c->split[0] * 8 + c->split[1] + (c->use_tri ? 1000 : 0));
-            key.push_back(c->tri_cols);
+            key.push_back(c->tri_cols + 100 * c->geom32);
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -1010,6 +1011,16 @@ extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
         return PSKEL_ERR_ARG;
     }
     c->tri_cols = cols;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_set_fill_geometry(pskel_ctx *c, int fp32_offsets) {
+    PSKEL_TRY(ctx_ok(c));
+    if (fp32_offsets != 0 && fp32_offsets != 1) {
+        set_error(PSKEL_ERR_ARG, "fill geometry: 0 (FP64) or 1 (FP32 offsets)");
+        return PSKEL_ERR_ARG;
+    }
+    c->geom32 = fp32_offsets;
     return PSKEL_OK;
 }
 

@@ -100,6 +100,7 @@ struct pskel_ctx {
     int precision = PSKEL_C128;
     int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
     int tri_cols = pskel::kTriFillColsDefault;  // columns per CTA of the triangle-moment fill
+    int geom32 = 0;  // complex-FP32 fill: 1 = FP32 pair geometry from per-item offsets
     double timing[13] = {};  // [0..11] as reported by pskel_last_timing, [12] core SVD count
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;

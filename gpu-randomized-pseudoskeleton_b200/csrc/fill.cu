@@ -556,7 +556,12 @@ struct TriWeights {
     double w0, w1, w2;
 };
 
-template <typename T, int Q, int TN>
+// OFS (complex-FP32 variant only): the point-pair geometry in FP32 offsets instead of FP64. Per
+// item the vector D = c_t - y_0 from the source RWG's first point to the triangle centroid, |D|
+// and the phase of |D| reduced to a fraction of a turn are FP64; per pair, with e = x'_p - (y_q - y_0)
+// (both small), R^2 = |D|^2 + u with u = e . (2 D + e), and R - |D| = u / (R + |D|), all FP32:
+// the phase keeps an absolute error of ~1e-7 turn without FP64 arithmetic in the pair loop.
+template <typename T, int Q, int TN, bool OFS = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     tri_fill_kernel(const double *__restrict__ tri_rec, const double *__restrict__ rec_s,
                     const double *__restrict__ edges, const double *__restrict__ vertex,
@@ -572,7 +577,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     double2 *s_xy = reinterpret_cast<double2 *>(smem_raw);   // TN x NP
     double *s_z = reinterpret_cast<double *>(s_xy + TN * NP);  // TN x NP
     T4 *s_v = reinterpret_cast<T4 *>(s_z + TN * NP);           // TN x NP
-    T *zs = reinterpret_cast<T *>(s_v + TN * NP);              // 2 x kTriFillMaxRows x TN
+    float4 *s_d = reinterpret_cast<float4 *>(s_v + TN * NP);   // TN x NP (OFS: y_q - y_0)
+    T *zs = reinterpret_cast<T *>(s_d + (OFS ? TN * NP : 0));   // 2 x kTriFillMaxRows x TN
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const int jb = find_job(tile_prefix, njobs, tile);
@@ -591,6 +597,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
             v.z = ok ? (T)src[5 * NP + q] : T(0);
             v.w = ok ? (T)src[6 * NP + q] : T(0);
             s_v[idx] = v;
+            if (OFS)
+                s_d[idx] = make_float4(ok ? (float)(src[q] - src[0]) : 0.f,
+                                       ok ? (float)(src[NP + q] - src[NP]) : 0.f,
+                                       ok ? (float)(src[2 * NP + q] - src[2 * NP]) : 0.f, 0.f);
         }
         for (int idx = threadIdx.x; idx < 2 * job.m * TN; idx += blockDim.x) zs[idx] = T(0);
         __syncthreads();
@@ -606,17 +616,48 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
             const T4 *sv = s_v + j * NP;
             T a0r = 0, a0i = 0, bxr = 0, bxi = 0;
             T cvr[3] = {0, 0, 0}, cvi[3] = {0, 0, 0};
+            // OFS: item-level FP64 geometry from the source RWG's first point y_0
+            float D2x = 0.f, D2y = 0.f, D2z = 0.f, DDf = 0.f, Dnf = 0.f, ph0 = 0.f;
+            if constexpr (OFS) {
+                const double Dx = cx - sxy[0].x, Dy = cy - sxy[0].y, Dz = cz - sz[0];
+                const double DD = fma(Dx, Dx, fma(Dy, Dy, Dz * Dz));
+                const double Dn = sqrt(DD);
+                const double ph = Dn * kturn;
+                D2x = (float)(2.0 * Dx);
+                D2y = (float)(2.0 * Dy);
+                D2z = (float)(2.0 * Dz);
+                DDf = (float)DD;
+                Dnf = (float)Dn;
+                ph0 = (float)(ph - floor(ph));
+            }
+            const float kturnf = (float)kturn;
+            const float4 *sd = s_d + j * NP;
 #pragma unroll 1
             for (int p = 0; p < Q; ++p) {
                 const double x = tr[3 * p], y = tr[3 * p + 1], z = tr[3 * p + 2];
                 T s0r = 0, s0i = 0, s1r[3] = {0, 0, 0}, s1i[3] = {0, 0, 0};
+                const float ex0 = (float)(x - cx), ey0 = (float)(y - cy), ez0 = (float)(z - cz);
 #pragma unroll 2
                 for (int q = 0; q < NP; ++q) {
+                    T rinv, sn, cs;
+                    int quad;
+                    if constexpr (OFS) {
+                        const float4 d = sd[q];
+                        const float ex = ex0 - d.x, ey = ey0 - d.y, ez = ez0 - d.z;
+                        const float u = fmaf(ex, D2x + ex, fmaf(ey, D2y + ey, ez * (D2z + ez)));
+                        const float R2f = DDf + u;
+                        const float ri = rsqrtf(R2f);
+                        const float corr = __fdividef(u, fmaf(R2f, ri, Dnf));  // R - |D|
+                        const float turns = fmaf(corr, kturnf, ph0);
+                        const float tm = fmaf(turns, 4.0f, 12582912.0f);     // 1.5 * 2^23
+                        quad = __float_as_int(tm);
+                        const float g = fmaf(tm - 12582912.0f, -0.25f, turns);
+                        sincos_2pi(g, quad, &sn, &cs);
+                        rinv = ri;
+                    } else {
                     const double2 xy = sxy[q];
                     const double dx = x - xy.x, dy = y - xy.y, dz = z - sz[q];
                     const double R2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                    T rinv, sn, cs;
-                    int quad;
                     if constexpr (sizeof(T) == 8) {
                         rinv = rsqrt(R2);
                         const double g = split_quarter(R2 * rinv * kturn, &quad);
@@ -629,6 +670,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
                         const double g = split_quarter(R * kturn, &quad);
                         sincos_2pi((float)g, quad, &sn, &cs);
                         rinv = yy;
+                    }
                     }
                     const T gr = rinv * sn, gi = rinv * cs;  // G = (sin kR + j cos kR) / R
                     const T4 v = sv[q];
@@ -692,14 +734,15 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     }
 }
 
-template <typename T, int Q, int TN>
+template <typename T, int Q, int TN, bool OFS = false>
 static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillParams &p,
                         const GroupFillJob *d_jobs, const int *d_prefix, int njobs,
                         int total_tiles, cudaStream_t stream) {
     constexpr int NP = 2 * Q;
-    const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
+    const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T) + (OFS ? sizeof(float4) : 0)) *
+                            (size_t)TN * NP +
                         2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
-    auto kern = tri_fill_kernel<T, Q, TN>;
+    auto kern = tri_fill_kernel<T, Q, TN, OFS>;
     static bool attr_set = false;
     if (!attr_set) {
         PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -737,6 +780,8 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
     }
 #define PSKEL_TRI(T, Q, TN) \
     return launch_tri_t<T, Q, TN>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
+#define PSKEL_TRI_OFS(Q, TN) \
+    return launch_tri_t<float, Q, TN, true>(mesh, rec, p, d_jobs, d_tile_prefix, njobs, total_tiles, stream)
 #define PSKEL_TRI_TN(T, Q)                     \
     do {                                       \
         if (p.tri_cols == 4) PSKEL_TRI(T, Q, 4);   \
@@ -751,9 +796,20 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
         if (p.q_test == 7) PSKEL_TRI_TN(double, 7);
         PSKEL_TRI_TN(double, 1);
     }
+    if (p.geom32) {  // complex-FP32 fill with FP32 pair geometry
+        if (p.q_test == 7) {
+            if (p.tri_cols == 4) PSKEL_TRI_OFS(7, 4);
+            if (p.tri_cols == 16) PSKEL_TRI_OFS(7, 16);
+            PSKEL_TRI_OFS(7, 8);
+        }
+        if (p.tri_cols == 4) PSKEL_TRI_OFS(1, 4);
+        if (p.tri_cols == 16) PSKEL_TRI_OFS(1, 16);
+        PSKEL_TRI_OFS(1, 8);
+    }
     if (p.q_test == 7) PSKEL_TRI_TN(float, 7);
     PSKEL_TRI_TN(float, 1);
 #undef PSKEL_TRI_TN
+#undef PSKEL_TRI_OFS
 #undef PSKEL_TRI
 }
 

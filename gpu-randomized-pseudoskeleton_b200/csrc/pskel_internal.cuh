@@ -117,6 +117,7 @@ struct FillParams {
     int precision;     // PSKEL_C128 / PSKEL_C64
     int split;         // 0: two rows per thread (default kernel); 1, 2, 4: lanes per entry
     int tri_cols = kTriFillColsDefault;  // columns per CTA of the triangle-moment fill (4, 8, 16)
+    int geom32 = 0;    // complex-FP32 triangle-moment fill: FP32 pair geometry from item offsets
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the

@@ -2,7 +2,8 @@
 keeps the fastest.
 
 The variants are the triangle-moment kernel with 4, 8 or 16 columns per CTA tile (usable while
-every group has at most 512 RWG) and the per-entry kernels (two rows per thread; 1, 2 or 4 lanes
+every group has at most 512 RWG; in complex FP32 also with the FP32 pair geometry) and the
+per-entry kernels (two rows per thread; 1, 2 or 4 lanes
 per entry with a shuffle reduction over the quadrature points). Each candidate runs one
 single-round compression of every block at a fixed sample count (the first round's fill, the
 launch that dominates a compression) and is timed by the engine's own device events
@@ -18,12 +19,16 @@ import os
 import numpy as np
 
 TRI_VARIANTS = [("tri", 4), ("tri", 8), ("tri", 16)]
+# complex-FP32 only: the triangle-moment fill with FP32 pair geometry from per-item offsets
+TRI32_VARIANTS = [("tri32_", 4), ("tri32_", 8), ("tri32_", 16)]
 ENTRY_VARIANTS = [("entry", 0), ("entry", 1), ("entry", 2), ("entry", 4)]
 
 
 def _apply(eng, precision, variant):
     kind, v = variant
-    if kind == "tri":
+    if precision != "c128":
+        eng.set_fill_geometry(kind == "tri32_")
+    if kind in ("tri", "tri32_"):
         eng.set_tri_cols(v)
         split = 8
     else:
@@ -54,6 +59,8 @@ def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int =
             return {"choice": choice, "ms": table[key]["ms"], "cached": True}
     sizes = np.diff(np.asarray(eng._gp))
     variants = list(TRI_VARIANTS) if sizes.max() <= 512 else []
+    if variants and precision != "c128":
+        variants += TRI32_VARIANTS
     if include_entry or not variants:
         variants += ENTRY_VARIANTS
     r0 = np.minimum(samples, np.minimum(sizes[eng._gt], sizes[eng._gs])).astype(np.int32)

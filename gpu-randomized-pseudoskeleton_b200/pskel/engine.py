@@ -232,6 +232,11 @@ class Engine:
         """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
+    def set_fill_geometry(self, fp32_offsets: bool):
+        """Complex-FP32 triangle-moment fill: FP32 pair geometry from per-item offsets (True)
+        or FP64 differences and phase (False, default)."""
+        _lib.check(self._lib.pskel_set_fill_geometry(self._h, int(bool(fp32_offsets))))
+
     def fill_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int, ld: int,
                     precision="c128"):
         """Fill into device buffers given as raw device pointers (e.g. torch data_ptr())."""

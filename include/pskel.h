@@ -256,6 +256,12 @@ int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
    workload by the autotuner (pskel/autotune.py), which times the variants on the block list. */
 int pskel_set_tri_cols(pskel_ctx *ctx, int cols);
 
+/* Pair geometry of the complex-FP32 triangle-moment fill: 0 = differences, distance and phase
+   in FP64 (default); 1 = FP64 only per (triangle, column) item (the distance from the column's
+   first point to the triangle centroid and its phase), FP32 per point pair from the two small
+   offsets (phase error ~1e-7 turn). Selected by the autotuner. */
+int pskel_set_fill_geometry(pskel_ctx *ctx, int fp32_offsets);
+
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);

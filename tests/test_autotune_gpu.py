@@ -49,7 +49,8 @@ def test_autotune_picks_a_variant(sphere, tmp_path):
         rep = autotune.autotune_fill(eng, "c64", samples=16, repeats=1, include_entry=True,
                                      cache=cache, gpu_name="test")
         assert not rep["cached"]
-        assert set(rep["ms"]) == {"tri4", "tri8", "tri16", "entry0", "entry1", "entry2", "entry4"}
+        assert set(rep["ms"]) == {"tri4", "tri8", "tri16", "tri32_4", "tri32_8", "tri32_16",
+                                  "entry0", "entry1", "entry2", "entry4"}
         best = min(rep["ms"], key=rep["ms"].get)
         assert f"{rep['choice'][0]}{rep['choice'][1]}" == best
         st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
@@ -58,3 +59,30 @@ def test_autotune_picks_a_variant(sphere, tmp_path):
         rep2 = autotune.autotune_fill(eng, "c64", cache=cache, gpu_name="test")
         assert rep2["cached"] and tuple(rep2["choice"]) == tuple(rep["choice"])
     assert "test|" in next(iter(json.load(open(cache))))
+
+
+def test_fp32_geometry_matches_fp64_geometry(sphere):
+    """The complex-FP32 fill with FP32 pair geometry against the FP64-geometry fill and the
+    errors of a compression that uses it."""
+    m, part = sphere
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        r0 = np.full(eng.n_blocks, 12, dtype=np.int32)
+        picks = (0, eng.n_blocks // 3, eng.n_blocks // 2, eng.n_blocks - 1)
+        out = {}
+        for g in (False, True):
+            eng.set_fill_geometry(g)
+            st = eng.compress(1.0, precision="c64", r0=r0, oversample=0, max_rounds=1, seed=4)
+            out[g] = [eng.get_block(b, st)[0] for b in picks]
+        ref = {}
+        st = eng.compress(1.0, precision="c128", r0=r0, oversample=0, max_rounds=1, seed=4)
+        ref = [eng.get_block(b, st)[0] for b in picks]
+        for a, b, c in zip(out[True], out[False], ref):
+            ea = np.linalg.norm(a - c) / np.linalg.norm(c)
+            eb = np.linalg.norm(b - c) / np.linalg.norm(c)
+            assert ea < 3e-6 and eb < 3e-6, (ea, eb)
+        eng.set_fill_geometry(True)
+        st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        err = eng.true_errors()
+        assert np.median(err) < 2e-5 and err.max() < 3e-4
