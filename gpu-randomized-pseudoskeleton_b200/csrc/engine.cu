@@ -321,6 +321,13 @@ using namespace pskel;
 
 namespace {
 
+// columns per tile of a triangle-moment fill job: the context's fixed width, or (width 0) the
+// balanced width of tri_tile_cols up to the widest variant
+int tri_cols_for(const pskel_ctx *c, int nt) {
+    return c->tri_cols > 0 ? c->tri_cols : tri_tile_cols(nt, kTriFillCols);
+}
+
+
 // fill variant actually used for a precision: the triangle-moment kernel when asked for and
 // every group fits it, else the per-entry kernel (two rows per thread when 8 was asked for)
 bool tri_for(const pskel_ctx *c, int precision) {
@@ -351,6 +358,7 @@ struct RoundPlan {
     FillJob *d_fill = nullptr;            // per-entry fill jobs (groups too large for tri)
     GroupFillJob *d_gfill = nullptr;      // triangle-moment fill jobs
     bool tri = false;
+    int tri_rows = 0;                     // largest group among the triangle-moment jobs
     int *d_fill_prefix = nullptr;
     int fill_jobs = 0, fill_tiles = 0;
     SvdJob *d_svd = nullptr;
@@ -447,12 +455,11 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         if (tri_for(c, o.precision)) {
             const int gt = c->gt[b], gs = c->gs[b];
             const int *tri = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
+            const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
             gfills.push_back(GroupFillJob{w.rows_g, tri + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                          w.Jg, w.C, w.m, c->gtri_ptr[gt + 1] - c->gtri_ptr[gt],
-                                          w.r + w.pc, w.m, 0, 0});
+                                          w.Jg, w.C, w.m, ntt, w.r + w.pc, w.m, 0, tri_cols_for(c, ntt)});
             gfills.push_back(GroupFillJob{w.cols_g, tri + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                          w.Ig, w.Rx, w.n, c->gtri_ptr[gs + 1] - c->gtri_ptr[gs],
-                                          w.r + w.pe, w.r + w.pe, 1, 0});
+                                          w.Ig, w.Rx, w.n, nts, w.r + w.pe, w.r + w.pe, 1, tri_cols_for(c, nts)});
         }
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, o.tau, o.tau_relative};
@@ -476,8 +483,11 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.tri = tri_for(c, o.precision);
     std::vector<int> prefix(fills.size() + 1, 0);
     if (p.tri) {
-        for (size_t i = 0; i < gfills.size(); ++i)
-            prefix[i + 1] = prefix[i] + (gfills[i].nc + c->tri_cols - 1) / c->tri_cols;
+        p.tri_rows = 0;
+        for (size_t i = 0; i < gfills.size(); ++i) {
+            prefix[i + 1] = prefix[i] + (gfills[i].nc + gfills[i].tc - 1) / gfills[i].tc;
+            p.tri_rows = std::max(p.tri_rows, gfills[i].m);
+        }
     } else {
         for (size_t i = 0; i < fills.size(); ++i)
             prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
@@ -538,6 +548,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.split = entry_split_for(c, o.precision);
     fp.tri_cols = c->tri_cols;
     fp.geom32 = c->geom32;
+    fp.max_rows = p.tri_rows;
     if (p.tri)
         PSKEL_TRY(launch_tri_fill(c->mesh, fp, p.d_gfill, p.d_fill_prefix, p.fill_jobs,
                                   p.fill_tiles, s));
@@ -1006,8 +1017,8 @@ extern "C" int pskel_set_fill_split(pskel_ctx *c, int split_c128, int split_c64)
 
 extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
     PSKEL_TRY(ctx_ok(c));
-    if (cols != 4 && cols != 8 && cols != 16) {
-        set_error(PSKEL_ERR_ARG, "triangle-moment fill: %d columns per tile (4, 8 or 16)", cols);
+    if (cols != 0 && cols != 4 && cols != 8 && cols != 16) {
+        set_error(PSKEL_ERR_ARG, "triangle-moment fill: %d columns per tile (0 = balanced, 4, 8 or 16)", cols);
         return PSKEL_ERR_ARG;
     }
     c->tri_cols = cols;
@@ -1131,8 +1142,9 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
                                      c->d_gtri.as<int>() + c->gtri_ptr[gt],
                                      c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt],
                                      c->d_gids.as<int>() + c->gptr[c->gs[b]], Z, res.m,
-                                     c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], res.n, res.m, 0, 0};
-            prefix[i + 1] = prefix[i] + (tri ? (res.n + c->tri_cols - 1) / c->tri_cols
+                                     c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], res.n, res.m, 0,
+                                     tri_cols_for(c, c->gtri_ptr[gt + 1] - c->gtri_ptr[gt])};
+            prefix[i + 1] = prefix[i] + (tri ? (res.n + gfills[i].tc - 1) / gfills[i].tc
                                                      : ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn));
             mats[i] = Z;
             sizes[i] = (long long)res.m * res.n;

@@ -578,13 +578,14 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     double *s_z = reinterpret_cast<double *>(s_xy + TN * NP);  // TN x NP
     T4 *s_v = reinterpret_cast<T4 *>(s_z + TN * NP);           // TN x NP
     float4 *s_d = reinterpret_cast<float4 *>(s_v + TN * NP);   // TN x NP (OFS: y_q - y_0)
-    T *zs = reinterpret_cast<T *>(s_d + (OFS ? TN * NP : 0));   // 2 x kTriFillMaxRows x TN
+    T *zs = reinterpret_cast<T *>(s_d + (OFS ? TN * NP : 0));   // 2 x (largest m) x TN
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const int jb = find_job(tile_prefix, njobs, tile);
         const GroupFillJob job = jobs[jb];
-        const int j0 = (tile - tile_prefix[jb]) * TN;
-        for (int idx = threadIdx.x; idx < TN * NP; idx += blockDim.x) {
+        const int tcols = job.tc > 0 && job.tc < TN ? job.tc : TN;  // this job's tile width
+        const int j0 = (tile - tile_prefix[jb]) * tcols;
+        for (int idx = threadIdx.x; idx < tcols * NP; idx += blockDim.x) {
             const int c = idx / NP, q = idx - c * NP;
             const int col = j0 + c;
             const bool ok = col < job.nc;
@@ -602,10 +603,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
                                        ok ? (float)(src[NP + q] - src[NP]) : 0.f,
                                        ok ? (float)(src[2 * NP + q] - src[2 * NP]) : 0.f, 0.f);
         }
-        for (int idx = threadIdx.x; idx < 2 * job.m * TN; idx += blockDim.x) zs[idx] = T(0);
+        for (int idx = threadIdx.x; idx < 2 * job.m * tcols; idx += blockDim.x) zs[idx] = T(0);
         __syncthreads();
 
-        const int items = job.nt * TN;
+        const int items = job.nt * tcols;
         for (int it = threadIdx.x; it < items; it += blockDim.x) {
             const int t = it % job.nt, j = it / job.nt;
             if (j0 + j >= job.nc) continue;
@@ -721,7 +722,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
         }
         __syncthreads();
         C2 *out = reinterpret_cast<C2 *>(job.out);
-        for (int idx = threadIdx.x; idx < job.m * TN; idx += blockDim.x) {
+        for (int idx = threadIdx.x; idx < job.m * tcols; idx += blockDim.x) {
             const int i = idx % job.m, j = idx / job.m;
             if (j0 + j >= job.nc) continue;
             C2 z;
@@ -739,13 +740,15 @@ static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillP
                         const GroupFillJob *d_jobs, const int *d_prefix, int njobs,
                         int total_tiles, cudaStream_t stream) {
     constexpr int NP = 2 * Q;
-    const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T) + (OFS ? sizeof(float4) : 0)) *
-                            (size_t)TN * NP +
-                        2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
+    const size_t rec_bytes =
+        (sizeof(double2) + sizeof(double) + 4 * sizeof(T) + (OFS ? sizeof(float4) : 0)) * (size_t)TN * NP;
+    const int rows = p.max_rows > 0 && p.max_rows < kTriFillMaxRows ? p.max_rows : kTriFillMaxRows;
+    const size_t smem = rec_bytes + 2 * sizeof(T) * (size_t)rows * TN + 16;
     auto kern = tri_fill_kernel<T, Q, TN, OFS>;
     static bool attr_set = false;
     if (!attr_set) {
-        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const size_t most = rec_bytes + 2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
+        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
         attr_set = true;
     }
     int per_sm = 0;
@@ -785,11 +788,11 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
 #define PSKEL_TRI_TN(T, Q)                     \
     do {                                       \
         if (p.tri_cols == 4) PSKEL_TRI(T, Q, 4);   \
-        if (p.tri_cols == 16) PSKEL_TRI(T, Q, 16); \
+        if (p.tri_cols == 16 || p.tri_cols == 0) PSKEL_TRI(T, Q, 16); \
         PSKEL_TRI(T, Q, 8);                    \
     } while (0)
-    if (p.tri_cols != 4 && p.tri_cols != 8 && p.tri_cols != 16) {
-        set_error(PSKEL_ERR_ARG, "tri fill: %d columns per tile (4, 8 or 16)", p.tri_cols);
+    if (p.tri_cols != 0 && p.tri_cols != 4 && p.tri_cols != 8 && p.tri_cols != 16) {
+        set_error(PSKEL_ERR_ARG, "tri fill: %d columns per tile (0 = balanced per job, 4, 8 or 16)", p.tri_cols);
         return PSKEL_ERR_ARG;
     }
     if (p.precision == PSKEL_C128) {
@@ -799,11 +802,11 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
     if (p.geom32) {  // complex-FP32 fill with FP32 pair geometry
         if (p.q_test == 7) {
             if (p.tri_cols == 4) PSKEL_TRI_OFS(7, 4);
-            if (p.tri_cols == 16) PSKEL_TRI_OFS(7, 16);
+            if (p.tri_cols == 16 || p.tri_cols == 0) PSKEL_TRI_OFS(7, 16);
             PSKEL_TRI_OFS(7, 8);
         }
         if (p.tri_cols == 4) PSKEL_TRI_OFS(1, 4);
-        if (p.tri_cols == 16) PSKEL_TRI_OFS(1, 16);
+        if (p.tri_cols == 16 || p.tri_cols == 0) PSKEL_TRI_OFS(1, 16);
         PSKEL_TRI_OFS(1, 8);
     }
     if (p.q_test == 7) PSKEL_TRI_TN(float, 7);

@@ -109,6 +109,7 @@ struct FillJob {
 
 constexpr int kTriFillCols = 16;        // most columns per CTA tile (variants 4, 8, 16)
 constexpr int kTriFillColsDefault = 8;
+constexpr int kTriFillMaxRowsDefaultForParams = 512;
 
 struct FillParams {
     double k, eta;
@@ -118,6 +119,7 @@ struct FillParams {
     int split;         // 0: two rows per thread (default kernel); 1, 2, 4: lanes per entry
     int tri_cols = kTriFillColsDefault;  // columns per CTA of the triangle-moment fill (4, 8, 16)
     int geom32 = 0;    // complex-FP32 triangle-moment fill: FP32 pair geometry from item offsets
+    int max_rows = kTriFillMaxRowsDefaultForParams;  // largest group in a triangle-moment launch
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the
@@ -136,9 +138,28 @@ struct GroupFillJob {
     const int *adj;   // 3 per triangle: 2 * local RWG index + side (0: T+, 1: T-), or -1
     const int *cols;  // global RWG ids of the columns (nc)
     void *out;
-    int m, nt, nc, ld, trans, pad;
+    int m, nt, nc, ld, trans;
+    int tc;           // columns per CTA tile for this job (<= the launch's tile width)
 };
 constexpr int kTriFillMaxRows = 512;  // largest group the triangle-moment fill accepts
+// Columns per tile for a job of nt triangles: the width in [4, max_cols] whose (triangle, column)
+// item count fills the 256 threads of a CTA best (the last round of items is the idle part),
+// the widest among equals. max_cols < 4 returns max_cols.
+inline int tri_tile_cols(int nt, int max_cols) {
+    if (max_cols < 4) return max_cols < 1 ? 1 : max_cols;
+    int best = max_cols;
+    double best_eff = -1.0;
+    for (int c = max_cols; c >= 4; --c) {
+        const long long items = (long long)nt * c;
+        const long long slots = (items + 255) / 256 * 256;
+        const double eff = (double)items / (double)slots;
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = c;
+        }
+    }
+    return best;
+}
 int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob *d_jobs,
                     const int *d_tile_prefix, int njobs, int total_tiles, cudaStream_t stream);
 

@@ -18,9 +18,11 @@ import os
 
 import numpy as np
 
-TRI_VARIANTS = [("tri", 4), ("tri", 8), ("tri", 16)]
+# tile width 0: per job, the width in [4, 16] whose (triangle, column) item count fills the
+# CTA's 256 threads best
+TRI_VARIANTS = [("tri", 0), ("tri", 4), ("tri", 8), ("tri", 16)]
 # complex-FP32 only: the triangle-moment fill with FP32 pair geometry from per-item offsets
-TRI32_VARIANTS = [("tri32_", 4), ("tri32_", 8), ("tri32_", 16)]
+TRI32_VARIANTS = [("tri32_", 0), ("tri32_", 4), ("tri32_", 8), ("tri32_", 16)]
 ENTRY_VARIANTS = [("entry", 0), ("entry", 1), ("entry", 2), ("entry", 4)]
 
 

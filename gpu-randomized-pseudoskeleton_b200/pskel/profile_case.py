@@ -1,12 +1,13 @@
 """One small, repeatable compression workload for kernel profiling and variant timing.
 
-    python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py PRECISION [CALLS] [SPLIT]
+    python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py PRECISION [CALLS] [SPLIT] [GEOM32]
     python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py store [CALLS]
 
 builds the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions, 0.5-lambda leaves), then
 makes CALLS (default 3) single-round compressions of every far block at a fixed sample count of
 24 with the given precision (c128 or c64) and fill variant (8: triangle moments, the default;
-0: two rows per thread; 1, 2, 4: lanes per entry), printing the fill time and point-pair
+0: two rows per thread; 1, 2, 4: lanes per entry; GEOM32 = 1: complex-FP32 fill with FP32 pair
+geometry), printing the fill time and point-pair
 rate of each call. Under a profiler the fill launch of call i is the i-th launch of the chosen fill kernel.
 The store form compresses the same sphere, recompresses it, builds the compressed store and runs
 CALLS tensor-core matvecs of 16 right-hand sides.
@@ -57,6 +58,7 @@ def main():
     prec = sys.argv[1] if len(sys.argv) > 1 else "c64"
     calls = int(sys.argv[2]) if len(sys.argv) > 2 else 3
     split = int(sys.argv[3]) if len(sys.argv) > 3 else 8
+    geom32 = int(sys.argv[4]) if len(sys.argv) > 4 else 0
     m = pmesh.icosphere(2.0, 4)
     part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
     with Engine() as eng:
@@ -66,6 +68,7 @@ def main():
             eng.set_fill_split(split_c128=split)
         else:
             eng.set_fill_split(split_c64=split)
+            eng.set_fill_geometry(bool(geom32))
         for i in range(calls):
             eng.compress(1.0, precision=prec, r0=np.full(part.n_blocks, 24), oversample=0,
                          max_rounds=1, seed=i)

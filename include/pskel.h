@@ -252,8 +252,10 @@ int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c
    current choice. Set by the autotuner. */
 int pskel_set_fill_split(pskel_ctx *ctx, int split_c128, int split_c64);
 
-/* Columns per CTA tile of the triangle-moment fill: 4, 8 (default) or 16. Chosen per GPU and
-   workload by the autotuner (pskel/autotune.py), which times the variants on the block list. */
+/* Columns per CTA tile of the triangle-moment fill: 4, 8 (default) or 16, or 0 for a width per
+   job (in [4, 16], the one whose triangle x column item count best fills a CTA's 256 threads).
+   Chosen per GPU and workload by the autotuner (pskel/autotune.py), which times the variants
+   on the block list. */
 int pskel_set_tri_cols(pskel_ctx *ctx, int cols);
 
 /* Pair geometry of the complex-FP32 triangle-moment fill: 0 = differences, distance and phase

@@ -28,14 +28,14 @@ def test_tile_widths_agree(sphere, prec):
         eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
         eng.set_blocks(part)
         r0 = np.full(eng.n_blocks, 12, dtype=np.int32)
-        for cols in (4, 8, 16):
+        for cols in (0, 4, 8, 16):
             eng.set_tri_cols(cols)
             st = eng.compress(1.0, precision=prec, r0=r0, oversample=0, max_rounds=1, seed=9)
             out[cols] = [eng.get_block(b, st)[0] for b in (0, eng.n_blocks // 2, eng.n_blocks - 1)]
         with pytest.raises(RuntimeError):
             eng.set_tri_cols(5)
     bar = 1e-6 if prec == "c64" else 1e-13
-    for cols in (4, 16):
+    for cols in (0, 4, 16):
         for a, b in zip(out[cols], out[8]):
             assert np.abs(a - b).max() <= bar * np.abs(b).max()
 
@@ -49,8 +49,8 @@ def test_autotune_picks_a_variant(sphere, tmp_path):
         rep = autotune.autotune_fill(eng, "c64", samples=16, repeats=1, include_entry=True,
                                      cache=cache, gpu_name="test")
         assert not rep["cached"]
-        assert set(rep["ms"]) == {"tri4", "tri8", "tri16", "tri32_4", "tri32_8", "tri32_16",
-                                  "entry0", "entry1", "entry2", "entry4"}
+        assert set(rep["ms"]) == {"tri0", "tri4", "tri8", "tri16", "tri32_0", "tri32_4", "tri32_8",
+                                  "tri32_16", "entry0", "entry1", "entry2", "entry4"}
         best = min(rep["ms"], key=rep["ms"].get)
         assert f"{rep['choice'][0]}{rep['choice'][1]}" == best
         st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)

@@ -34,3 +34,20 @@ def test_roofline_work_counts():
     # 30 factor entries of 8 bytes, 9 core entries of 16 bytes, 2 x 9 vector entries of 8 bytes
     assert roofline.matvec_bytes([4], [6], [3], 2, 8.0, 16.0) == 30 * 8 + 9 * 16 + 2 * 10 * 8
     assert roofline.recompress_flops([4], [6], [2], [1]) == 8 * (2 * 4 * 4 + 2 * 6 * 4) + 84 * 8 + 8 * 10 * 2
+
+
+def test_balanced_tile_width_rule():
+    """The per-job tile width of the triangle-moment fill: items = triangles x width fill the
+    256 threads of a CTA best (restated here in Python against the rule's examples)."""
+    def width(nt, most=16):
+        best, best_eff = most, -1.0
+        for c in range(most, 3, -1):
+            items = nt * c
+            eff = items / (-(-items // 256) * 256)
+            if eff > best_eff + 1e-9:
+                best, best_eff = c, eff
+        return best
+    assert width(100) == 15      # 1500 of 1536 slots (as good as 10, and wider)
+    assert width(128) == 16      # 2048 = 8 x 256 exactly
+    assert width(64) == 16       # 1024
+    assert 4 <= width(37) <= 16
