@@ -212,6 +212,29 @@ __device__ __forceinline__ void sincos_2pi(float g, int q, float *s, float *c) {
     rotate_quadrant(q, sn, cs, s, c);
 }
 
+// sin/cos(2 pi g) for |g| <= 1/4 turn (|theta| <= pi/2), no quadrant rotation: the Taylor series
+// in g itself, coefficients (-1)^j (2 pi)^n / n!, truncated where the first omitted term is below
+// FP32 rounding at pi/2 (sin: theta^13/13! ~ 6e-8, cos: theta^14/14! ~ 6e-9). Used with a
+// half-turn reduction t = n/2 + g, where sin and cos of 2 pi t both take the sign (-1)^n.
+__host__ __device__ constexpr double two_pi_pow(int n) { return n == 0 ? 1.0 : 6.28318530717958647692 * two_pi_pow(n - 1); }
+__host__ __device__ constexpr double taylor_2pi(int n) { return two_pi_pow(n) * inv_fact(n); }
+
+__device__ __forceinline__ void sincos_2pi_half(float g, float *s, float *c) {
+    const float t2 = g * g;
+    float ps = fmaf(t2, -(float)taylor_2pi(11), (float)taylor_2pi(9));
+    ps = fmaf(t2, ps, -(float)taylor_2pi(7));
+    ps = fmaf(t2, ps, (float)taylor_2pi(5));
+    ps = fmaf(t2, ps, -(float)taylor_2pi(3));
+    ps = fmaf(t2, ps, (float)taylor_2pi(1));
+    *s = g * ps;
+    float pc = fmaf(t2, (float)taylor_2pi(12), -(float)taylor_2pi(10));
+    pc = fmaf(t2, pc, (float)taylor_2pi(8));
+    pc = fmaf(t2, pc, -(float)taylor_2pi(6));
+    pc = fmaf(t2, pc, (float)taylor_2pi(4));
+    pc = fmaf(t2, pc, -(float)taylor_2pi(2));
+    *c = fmaf(t2, pc, 1.0f);
+}
+
 __device__ __forceinline__ void sincos_2pi(double g, int q, double *s, double *c) {
     const double th = g * 6.28318530717958647692;
     const double t2 = th * th;
@@ -598,10 +621,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
             v.z = ok ? (T)src[5 * NP + q] : T(0);
             v.w = ok ? (T)src[6 * NP + q] : T(0);
             s_v[idx] = v;
-            if (OFS)
-                s_d[idx] = make_float4(ok ? (float)(src[q] - src[0]) : 0.f,
-                                       ok ? (float)(src[NP + q] - src[NP]) : 0.f,
-                                       ok ? (float)(src[2 * NP + q] - src[2 * NP]) : 0.f, 0.f);
+            if (OFS) {
+                const float dx = ok ? (float)(src[q] - src[0]) : 0.f;
+                const float dy = ok ? (float)(src[NP + q] - src[NP]) : 0.f;
+                const float dz = ok ? (float)(src[2 * NP + q] - src[2 * NP]) : 0.f;
+                s_d[idx] = make_float4(dx, dy, dz, fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+            }
         }
         for (int idx = threadIdx.x; idx < 2 * job.m * tcols; idx += blockDim.x) zs[idx] = T(0);
         __syncthreads();
@@ -638,23 +663,29 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
                 const double x = tr[3 * p], y = tr[3 * p + 1], z = tr[3 * p + 2];
                 T s0r = 0, s0i = 0, s1r[3] = {0, 0, 0}, s1i[3] = {0, 0, 0};
                 const float ex0 = (float)(x - cx), ey0 = (float)(y - cy), ez0 = (float)(z - cz);
+                // OFS, per test point: A_p = D + x'_p and c_p = 2 D . x'_p + |x'_p|^2, so that per
+                // pair u = |R|^2 - |D|^2 = c_p + |d_q|^2 - 2 A_p . d_q (d_q = y_q - y_0)
+                const float Ax = fmaf(0.5f, D2x, ex0), Ay = fmaf(0.5f, D2y, ey0), Az = fmaf(0.5f, D2z, ez0);
+                const float cp = fmaf(ex0, fmaf(1.0f, D2x, ex0), fmaf(ey0, D2y + ey0, ez0 * (D2z + ez0)));
 #pragma unroll 2
                 for (int q = 0; q < NP; ++q) {
                     T rinv, sn, cs;
                     int quad;
                     if constexpr (OFS) {
-                        const float4 d = sd[q];
-                        const float ex = ex0 - d.x, ey = ey0 - d.y, ez = ez0 - d.z;
-                        const float u = fmaf(ex, D2x + ex, fmaf(ey, D2y + ey, ez * (D2z + ez)));
+                        const float4 d = sd[q];  // (d_q, |d_q|^2)
+                        const float dot = fmaf(Ax, d.x, fmaf(Ay, d.y, Az * d.z));
+                        const float u = fmaf(-2.0f, dot, cp + d.w);
                         const float R2f = DDf + u;
                         const float ri = rsqrtf(R2f);
                         const float corr = __fdividef(u, fmaf(R2f, ri, Dnf));  // R - |D|
                         const float turns = fmaf(corr, kturnf, ph0);
-                        const float tm = fmaf(turns, 4.0f, 12582912.0f);     // 1.5 * 2^23
-                        quad = __float_as_int(tm);
-                        const float g = fmaf(tm - 12582912.0f, -0.25f, turns);
-                        sincos_2pi(g, quad, &sn, &cs);
-                        rinv = ri;
+                        // half-turn reduction: turns = n/2 + g, |g| <= 1/4; sin and cos take (-1)^n,
+                        // folded into the sign of 1/R
+                        const float tm = fmaf(turns, 2.0f, 12582912.0f);     // 1.5 * 2^23
+                        const float g = fmaf(tm - 12582912.0f, -0.5f, turns);
+                        sincos_2pi_half(g, &sn, &cs);
+                        rinv = __int_as_float(__float_as_int(ri) ^ (__float_as_int(tm) << 31));
+                        (void)quad;
                     } else {
                     const double2 xy = sxy[q];
                     const double dx = x - xy.x, dy = y - xy.y, dz = z - sz[q];
