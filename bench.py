@@ -290,7 +290,8 @@ def run_ours(args, rank, world, dev):
         err_plain = eng.true_errors()
     blockops = run_blockops(eng, st, m, flush)
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
-    e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush)
+    e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
+                                   fill_choice=tune["choice"])
     if args.save and rank == 0:
         np.savez(args.save, m=st["m"], n=st["n"], r=st["r"], rounds=st["rounds"], est=st["est"],
                  err=err, r_plain=st_plain["r"], rounds_plain=st_plain["rounds"],
@@ -324,7 +325,10 @@ def run_ours(args, rank, world, dev):
                    fill_point_pairs=float(t_plain["point_pairs"]),
                    err_max=None if err_plain is None else float(err_plain.max()),
                    blocks_over_tol=None if err_plain is None else int((err_plain > TOL).sum())),
-        roofline=dict(bound="alu", kernel="tri_fill_kernel<float,7> (c64 triangle moments, FP64 geometry)",
+        roofline=dict(bound="alu",
+                      kernel="tri_fill_kernel<float,7> (c64 triangle moments, "
+                             + ("FP32 pair geometry" if tune["choice"][0] == "tri32_" else "FP64 geometry")
+                             + f", tile width {tune['choice'][1] or 'balanced per job'})",
                       achieved=round(achieved, 3), peak=round(fp32_peak.value, 3), unit="TFLOP/s",
                       frac=round(achieved / fp32_peak.value, 4),
                       traffic=FILL_TRAFFIC_BYTES if args.workload == "sphere30k" else None,
@@ -433,11 +437,11 @@ def _hbm_peak():
         return 6650.0
 
 
-def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush):
+def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None):
     """Host data in, compressed blocks resident on the GPU, per-block stats out."""
     import torch
 
-    from pskel import _lib
+    from pskel import _lib, autotune
     from pskel.engine import Engine
     from pskel.predictor import features
 
@@ -447,6 +451,8 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush):
     sp.gt, sp.gs, sp.sizes, sp.extents, sp.centres = sub_gt, sub_gs, part.sizes, part.extents, part.centres
     a = m.as_f64()
     eng = Engine(dev)
+    if fill_choice is not None:  # the fill variant the autotuner picked for this GPU and workload
+        autotune.apply(eng, PRODUCT["precision"], fill_choice)
     L = _lib.lib()
     feats_host = features(sp, K_WAVE, TOL)
     x_pin = torch.from_numpy(((feats_host - pred.mean) / pred.std).astype(np.float32)).pin_memory()

@@ -26,7 +26,8 @@ TRI32_VARIANTS = [("tri32_", 0), ("tri32_", 4), ("tri32_", 8), ("tri32_", 16)]
 ENTRY_VARIANTS = [("entry", 0), ("entry", 1), ("entry", 2), ("entry", 4)]
 
 
-def _apply(eng, precision, variant):
+def apply(eng, precision, variant):
+    """Set a fill variant (as returned in an autotune report's 'choice') on an engine."""
     kind, v = variant
     if precision != "c128":
         eng.set_fill_geometry(kind == "tri32_")
@@ -57,7 +58,7 @@ def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int =
             table = json.load(f)
         if key in table:
             choice = tuple(table[key]["choice"])
-            _apply(eng, precision, choice)
+            apply(eng, precision, choice)
             return {"choice": choice, "ms": table[key]["ms"], "cached": True}
     sizes = np.diff(np.asarray(eng._gp))
     variants = list(TRI_VARIANTS) if sizes.max() <= 512 else []
@@ -68,7 +69,7 @@ def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int =
     r0 = np.minimum(samples, np.minimum(sizes[eng._gt], sizes[eng._gs])).astype(np.int32)
     timings = {}
     for variant in variants:
-        _apply(eng, precision, variant)
+        apply(eng, precision, variant)
         best = float("inf")
         for rep in range(repeats + 1):  # the first run sets kernel attributes and warms up
             eng.compress(1.0, precision=precision, r0=r0, oversample=0, max_rounds=1, seed=rep)
@@ -77,7 +78,7 @@ def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int =
         timings[f"{variant[0]}{variant[1]}"] = round(best, 4)
     best_name = min(timings, key=timings.get)
     choice = next(v for v in variants if f"{v[0]}{v[1]}" == best_name)
-    _apply(eng, precision, choice)
+    apply(eng, precision, choice)
     if cache:
         table = {}
         if os.path.exists(cache):
