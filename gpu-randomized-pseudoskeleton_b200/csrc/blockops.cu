@@ -26,14 +26,25 @@ template <typename A> __device__ __forceinline__ typename CT<A>::c mk(double x, 
 template <> __device__ __forceinline__ double2 mk<double>(double x, double y) { return make_double2(x, y); }
 template <> __device__ __forceinline__ float2 mk<float>(double x, double y) { return make_float2((float)x, (float)y); }
 
-// One block per CTA iteration: T1 = R X(cols) (r x nrhs), T2 = U T1, Y(rows) += C T2.
+// One block per CTA iteration: T1 = R X(cols) (r x nrhs), T2 = U T1, Y(rows) += C T2; a mirror
+// block (the transpose of a stored one) uses R_p^T U_p^T C_p^T from its primary's factors.
 // Arithmetic type A (float or double), storage S (float2 or double2) of C and R.
 struct MatvecBlock {
     const int *rows, *cols;
-    const void *C, *R;
+    const void *C, *R;  // the stored factors: C m_c x r (ld ldc), R r x n_r (ld ldr)
     const double2 *U;
-    int m, n, r, ldr;
+    int m, n, r, ldr;   // m, n: this block's rows and columns
+    int ldc, trans;     // trans: mirror block
 };
+
+// factor element accessors: Rop(i, k) = R(i, k) (k < n), or C_p(k, i) for a mirror;
+// Uop(i, k) = U(i, k) or U(k, i); Cop(i, k) = C(i, k) (i < m), or R_p(k, i)
+template <typename S> __device__ __forceinline__ double2 r_op(const MatvecBlock &w, const S *R, const S *C, int i, int k) {
+    return w.trans ? ld_c(C, k + (size_t)i * w.ldc) : ld_c(R, i + (size_t)k * w.ldr);
+}
+template <typename S> __device__ __forceinline__ double2 c_op(const MatvecBlock &w, const S *R, const S *C, int i, int k) {
+    return w.trans ? ld_c(R, k + (size_t)i * w.ldr) : ld_c(C, i + (size_t)k * w.ldc);
+}
 
 template <typename A, typename S>
 __global__ void __launch_bounds__(256) matvec_kernel(const MatvecBlock *__restrict__ blocks, int nb,
@@ -51,7 +62,7 @@ __global__ void __launch_bounds__(256) matvec_kernel(const MatvecBlock *__restri
             const int i = e % w.r, j = e / w.r;
             A sr = 0, si = 0;
             for (int k = 0; k < w.n; ++k) {
-                const double2 rv = ld_c(R, i + (size_t)k * w.ldr);
+                const double2 rv = r_op(w, R, Cm, i, k);
                 const C2 x = X[w.cols[k] + (size_t)j * ldx];
                 sr += (A)rv.x * x.x - (A)rv.y * x.y;
                 si += (A)rv.x * x.y + (A)rv.y * x.x;
@@ -63,7 +74,7 @@ __global__ void __launch_bounds__(256) matvec_kernel(const MatvecBlock *__restri
             const int i = e % w.r, j = e / w.r;
             A sr = 0, si = 0;
             for (int k = 0; k < w.r; ++k) {
-                const double2 u = w.U[i + (size_t)k * w.r];
+                const double2 u = w.trans ? w.U[k + (size_t)i * w.r] : w.U[i + (size_t)k * w.r];
                 const C2 t = t1[k + j * w.r];
                 sr += (A)u.x * t.x - (A)u.y * t.y;
                 si += (A)u.x * t.y + (A)u.y * t.x;
@@ -75,7 +86,7 @@ __global__ void __launch_bounds__(256) matvec_kernel(const MatvecBlock *__restri
             const int i = e % w.m, j = e / w.m;
             A sr = 0, si = 0;
             for (int k = 0; k < w.r; ++k) {
-                const double2 c = ld_c(Cm, i + (size_t)k * w.m);
+                const double2 c = c_op(w, R, Cm, i, k);
                 const C2 t = t2[k + j * w.r];
                 sr += (A)c.x * t.x - (A)c.y * t.y;
                 si += (A)c.x * t.y + (A)c.y * t.x;
@@ -116,11 +127,12 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
                 set_error(PSKEL_ERR_STATE, "matvec: block %d has no retained factors", b);
                 return PSKEL_ERR_STATE;
             }
-            const char *base = c->arenas[res.arena].keep.as<char>();
+            const BlockResult &pr = res.mirror >= 0 ? c->results[res.mirror] : res;
+            const char *base = c->arenas[pr.arena].keep.as<char>();
             hb[b] = MatvecBlock{c->d_gids.as<int>() + c->gptr[c->gt[b]],
-                                c->d_gids.as<int>() + c->gptr[c->gs[b]], base + res.offC,
-                                base + res.offRx, reinterpret_cast<const double2 *>(base + res.offU),
-                                res.m, res.n, res.r, res.r + res.pe};
+                                c->d_gids.as<int>() + c->gptr[c->gs[b]], base + pr.offC,
+                                base + pr.offRx, reinterpret_cast<const double2 *>(base + pr.offU),
+                                res.m, res.n, res.r, pr.r + pr.pe, pr.m, res.mirror >= 0 ? 1 : 0};
             max_r = std::max(max_r, res.r);
         }
         PSKEL_TRY(c->mv_table.reserve(sizeof(MatvecBlock) * nb + 256));
@@ -231,18 +243,26 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         return PSKEL_ERR_ARG;
     }
     PSKEL_CUDA(cudaSetDevice(c->device));
-    const int nb = c->n_blocks;
+    const int nball = c->n_blocks;
     const bool f32 = c->precision == PSKEL_C64;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    std::vector<size_t> off(nb + 1, 0);
-    for (int b = 0; b < nb; ++b) {
-        const BlockResult &res = c->results[b];
-        if (res.arena < 0) {
+    // only blocks with their own factors are recompressed; a mirror block takes its primary's
+    // recompression transposed
+    std::vector<int> prims;
+    for (int b = 0; b < nball; ++b) {
+        if (c->results[b].arena < 0) {
             set_error(PSKEL_ERR_STATE, "recompress: block %d has no retained factors", b);
             return PSKEL_ERR_STATE;
         }
+        if (c->results[b].mirror < 0) prims.push_back(b);
+    }
+    const int nb = (int)prims.size();
+    std::vector<size_t> off(nb + 1, 0);
+    for (int pi = 0; pi < nb; ++pi) {
+        const int b = prims[pi];
+        const BlockResult &res = c->results[b];
         const size_t m = res.m, n = res.n, r = res.r;
-        off[b + 1] = off[b] + 2 * al(16 * m * r) + 3 * al(16 * n * r) + 8 * al(16 * r * r) +
+        off[pi + 1] = off[pi] + 2 * al(16 * m * r) + 3 * al(16 * n * r) + 8 * al(16 * r * r) +
                      2 * al(16 * r) + 4 * al(8 * r) + al(4 * r) + 256;
     }
     PSKEL_TRY(c->recomp.reserve(off[nb] + 256));
@@ -255,7 +275,7 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     std::vector<ZgemmJob> g1, g2;
     std::vector<ApplyQJob> aps;
     aps.reserve(2 * nb);
-    c->recomp_slots.assign(nb, {});
+    c->recomp_slots.assign(nball, {});
     // device job tables (the k table is referenced by the apply jobs)
     const size_t jb = sizeof(RecompBlock) * nb, s2 = sizeof(SvdJob) * nb;
     PSKEL_TRY(c->tmp.reserve(al(jb) + al(s2) + sizeof(int) * nb + 1024));
@@ -263,13 +283,14 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     RecompBlock *d_jobs = reinterpret_cast<RecompBlock *>(d);
     SvdJob *d_s2 = reinterpret_cast<SvdJob *>(d + al(jb));
     int *d_k = reinterpret_cast<int *>(d + al(jb) + al(s2));
-    for (int b = 0; b < nb; ++b) {
+    for (int pi = 0; pi < nb; ++pi) {
+        const int b = prims[pi];
         const BlockResult &res = c->results[b];
         const char *kb = c->arenas[res.arena].keep.as<char>();
-        char *q = base + off[b];
+        char *q = base + off[pi];
         auto take = [&](size_t bytes) { char *x = q; q += al(bytes); return x; };
         const size_t m = res.m, n = res.n, r = res.r;
-        RecompBlock &w = jobs[b];
+        RecompBlock &w = jobs[pi];
         w.C = kb + res.offC;
         w.R = kb + res.offRx;
         w.U = reinterpret_cast<const double2 *>(kb + res.offU);
@@ -293,7 +314,7 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         w.sm = reinterpret_cast<double *>(take(8 * r));
         w.S = reinterpret_cast<double *>(take(8 * r));
         w.pm = reinterpret_cast<int *>(take(4 * r));
-        w.kout = d_k + b;
+        w.kout = d_k + pi;
         w.m = res.m;
         w.n = res.n;
         w.r = res.r;
@@ -308,7 +329,7 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         aps.push_back(ApplyQJob{w.Bc, w.v0c, w.cc, res.m, res.r, w.Zc, res.r, w.Cp, res.m, res.r, w.kout});
         aps.push_back(ApplyQJob{w.Br, w.v0r, w.cr, res.n, res.r, w.Zr, res.r, w.RpH, res.n, res.r, w.kout});
         c->recomp_slots[b] = RecompSlot{(size_t)((char *)w.Cp - base), (size_t)((char *)w.Rp - base),
-                                        (size_t)((char *)w.S - base), 0};
+                                        (size_t)((char *)w.S - base), 0, -1};
     }
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, c->stream));
@@ -335,9 +356,14 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
             set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a core did not converge");
             return PSKEL_ERR_NOCONV;
         }
-    for (int b = 0; b < nb; ++b) {
-        c->recomp_slots[b].k = ks[b];
-        if (ranks) ranks[b] = ks[b];
+    for (int pi = 0; pi < nb; ++pi) c->recomp_slots[prims[pi]].k = ks[pi];
+    for (int b = 0; b < nball; ++b) {
+        const int mb = c->results[b].mirror;
+        if (mb >= 0) {
+            c->recomp_slots[b] = c->recomp_slots[mb];
+            c->recomp_slots[b].mirror = mb;
+        }
+        if (ranks) ranks[b] = c->recomp_slots[b].k;
     }
     return PSKEL_OK;
 }
@@ -350,6 +376,19 @@ extern "C" int pskel_get_recompressed(pskel_ctx *c, int b, pskel_c128 *Cp, doubl
     }
     PSKEL_CUDA(cudaSetDevice(c->device));
     const RecompSlot &sl = c->recomp_slots[b];
+    if (sl.mirror >= 0) {  // transpose of the primary's: C' = R'_p^T, R' = C'_p^T
+        const BlockResult &res = c->results[b];
+        const size_t k = sl.k, mb = res.m, nb_ = res.n;
+        std::vector<pskel_c128> Cpp(nb_ * k), Rpp(k * mb);
+        PSKEL_TRY(pskel_get_recompressed(c, sl.mirror, Cpp.data(), S, Rpp.data()));
+        if (Cp)
+            for (size_t t = 0; t < k; ++t)
+                for (size_t i = 0; i < mb; ++i) Cp[i + t * mb] = Rpp[t + i * k];
+        if (Rp)
+            for (size_t j = 0; j < nb_; ++j)
+                for (size_t t = 0; t < k; ++t) Rp[t + j * k] = Cpp[j + t * nb_];
+        return PSKEL_OK;
+    }
     const BlockResult &res = c->results[b];
     const char *base = c->recomp.as<char>();
     const size_t k = sl.k;

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <numeric>
 
 #include "pskel_internal.cuh"
@@ -734,6 +735,15 @@ extern "C" int pskel_set_blocks(pskel_ctx *c, const int *group_ptr, const int *g
     c->gs.assign(gs, gs + n_blocks);
     c->n_groups = n_groups;
     c->n_blocks = n_blocks;
+    {  // the block with swapped groups, for the symmetric mode
+        std::map<std::pair<int, int>, int> where;
+        for (int b = 0; b < n_blocks; ++b) where[{gt[b], gs[b]}] = b;
+        c->partner.assign(n_blocks, -1);
+        for (int b = 0; b < n_blocks; ++b) {
+            auto it = where.find({gs[b], gt[b]});
+            if (it != where.end() && it->second != b) c->partner[b] = it->second;
+        }
+    }
     PSKEL_TRY(c->d_gids.reserve(sizeof(int) * nids));
     PSKEL_CUDA(cudaMemcpyAsync(c->d_gids.ptr, group_ids, sizeof(int) * nids, cudaMemcpyHostToDevice,
                                c->stream));
@@ -960,14 +970,31 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     }
     return PSKEL_OK;
     };
+    for (int b = 0; b < nb; ++b) c->results[b].mirror = -1;
     if (o.per_block) {
         for (int b = 0; b < nb; ++b) PSKEL_TRY(run_rounds(std::vector<int>{b}, false));
         // each block reused the round arenas: only the last block's factors are still there
         for (int b = 0; b + 1 < nb; ++b) c->results[b].arena = -1;
     } else {
-        std::vector<int> all(nb);
-        std::iota(all.begin(), all.end(), 0);
+        // symmetric mode: the block of a (t, s) / (s, t) pair with the smaller index is compressed,
+        // the other takes its transpose (Z(s, t) = Z(t, s)^T for a Galerkin EFIE matrix)
+        const bool sym = c->symmetric != 0;
+        std::vector<int> all;
+        all.reserve(nb);
+        for (int b = 0; b < nb; ++b)
+            if (!sym || c->partner[b] < 0 || b < c->partner[b]) all.push_back(b);
         PSKEL_TRY(run_rounds(all, true));
+        if (sym)
+            for (int b = 0; b < nb; ++b) {
+                const int pb = c->partner[b];
+                if (pb < 0 || b < pb) continue;
+                BlockResult res = c->results[pb];
+                res.mirror = pb;
+                res.m = c->results[pb].n;
+                res.n = c->results[pb].m;
+                c->results[b] = res;
+                rounds_used[b] = rounds_used[pb];
+            }
     }
     PSKEL_CUDA(cudaEventRecord(t1, c->stream));
     PSKEL_CUDA(cudaEventSynchronize(t1));
@@ -1025,6 +1052,16 @@ extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
     return PSKEL_OK;
 }
 
+extern "C" int pskel_set_symmetric(pskel_ctx *c, int on) {
+    PSKEL_TRY(ctx_ok(c));
+    if (on != 0 && on != 1) {
+        set_error(PSKEL_ERR_ARG, "symmetric: 0 or 1");
+        return PSKEL_ERR_ARG;
+    }
+    c->symmetric = on;
+    return PSKEL_OK;
+}
+
 extern "C" int pskel_set_fill_geometry(pskel_ctx *c, int fp32_offsets) {
     PSKEL_TRY(ctx_ok(c));
     if (fp32_offsets != 0 && fp32_offsets != 1) {
@@ -1053,6 +1090,25 @@ extern "C" int pskel_get_block(pskel_ctx *c, int b, pskel_c128 *C, pskel_c128 *U
         return PSKEL_ERR_ARG;
     }
     const BlockResult &res = c->results[b];
+    if (res.mirror >= 0) {
+        // the transpose of the primary's factors: C = R_p^T, U = U_p^T, R = C_p^T, I = J_p, J = I_p
+        const size_t mb = res.m, nb_ = res.n, r = res.r;
+        std::vector<pskel_c128> Cp(nb_ * r), Up(r * r), Rp(r * mb);
+        std::vector<int> Ip(r), Jp(r);
+        PSKEL_TRY(pskel_get_block(c, res.mirror, Cp.data(), Up.data(), Rp.data(), Ip.data(), Jp.data()));
+        if (C)
+            for (size_t k = 0; k < r; ++k)
+                for (size_t i = 0; i < mb; ++i) C[i + k * mb] = Rp[k + i * r];
+        if (U)
+            for (size_t k = 0; k < r; ++k)
+                for (size_t i = 0; i < r; ++i) U[i + k * r] = Up[k + i * r];
+        if (R)
+            for (size_t j = 0; j < nb_; ++j)
+                for (size_t k = 0; k < r; ++k) R[k + j * r] = Cp[j + k * nb_];
+        if (I) std::copy(Jp.begin(), Jp.end(), I);
+        if (J) std::copy(Ip.begin(), Ip.end(), J);
+        return PSKEL_OK;
+    }
     const char *base = c->arenas[res.arena].keep.as<char>();
     const size_t m = res.m, n = res.n, r = res.r, ldr = res.r + res.pe;
     const bool f32 = c->precision == PSKEL_C64;
@@ -1109,8 +1165,9 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         int b1 = b0;
         while (b1 < nb) {
             const BlockResult &res = c->results[b1];
+            const BlockResult &pr = res.mirror >= 0 ? c->results[res.mirror] : res;  // factor storage
             const size_t d = (size_t)res.m * res.n;
-            const size_t wsz = (size_t)res.r * res.n + (f32 ? (size_t)res.m * res.r + (size_t)(res.r + res.pe) * res.n : 0);
+            const size_t wsz = (size_t)res.r * res.n + (f32 ? (size_t)pr.m * pr.r + (size_t)(pr.r + pr.pe) * pr.n : 0);
             if (b1 > b0 && dense + d > budget) break;
             dense += d;
             work += wsz;
@@ -1148,31 +1205,38 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
                                                      : ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn));
             mats[i] = Z;
             sizes[i] = (long long)res.m * res.n;
+            const BlockResult &pr = res.mirror >= 0 ? c->results[res.mirror] : res;  // factor storage
+            const bool mir = res.mirror >= 0;
             const double2 *Cd;
             const double2 *Rd;
-            int ldr = res.r + res.pe;
+            int ldr = pr.r + pr.pe;
             double2 *T = Wb + wo;
             wo += (size_t)res.r * res.n;
             if (f32) {
                 double2 *Cc = Wb + wo;
-                wo += (size_t)res.m * res.r;
+                wo += (size_t)pr.m * pr.r;
                 double2 *Rc = Wb + wo;
-                wo += (size_t)ldr * res.n;
-                const long long nC = (long long)res.m * res.r, nR = (long long)ldr * res.n;
+                wo += (size_t)ldr * pr.n;
+                const long long nC = (long long)pr.m * pr.r, nR = (long long)ldr * pr.n;
                 promote_kernel<float2><<<(unsigned)((nC + 255) / 256), 256, 0, c->stream>>>(
-                    reinterpret_cast<const float2 *>(base + res.offC), Cc, nC);
+                    reinterpret_cast<const float2 *>(base + pr.offC), Cc, nC);
                 promote_kernel<float2><<<(unsigned)((nR + 255) / 256), 256, 0, c->stream>>>(
-                    reinterpret_cast<const float2 *>(base + res.offRx), Rc, nR);
+                    reinterpret_cast<const float2 *>(base + pr.offRx), Rc, nR);
                 count_launch(2);
                 Cd = Cc;
                 Rd = Rc;
             } else {
-                Cd = reinterpret_cast<const double2 *>(base + res.offC);
-                Rd = reinterpret_cast<const double2 *>(base + res.offRx);
+                Cd = reinterpret_cast<const double2 *>(base + pr.offC);
+                Rd = reinterpret_cast<const double2 *>(base + pr.offRx);
             }
-            const double2 *Ud = reinterpret_cast<const double2 *>(base + res.offU);
-            g1.push_back(zjob(Ud, res.r, ZOP_N, Rd, ldr, ZOP_N, T, res.r, res.r, res.n, res.r));
-            ZgemmJob j2 = zjob(Cd, res.m, ZOP_N, T, res.r, ZOP_N, Z, res.m, res.m, res.n, res.r);
+            const double2 *Ud = reinterpret_cast<const double2 *>(base + pr.offU);
+            // Z - C U R, or for a mirror block Z - R_p^T U_p^T C_p^T
+            if (!mir)
+                g1.push_back(zjob(Ud, res.r, ZOP_N, Rd, ldr, ZOP_N, T, res.r, res.r, res.n, res.r));
+            else
+                g1.push_back(zjob(Ud, res.r, ZOP_T, Cd, pr.m, ZOP_T, T, res.r, res.r, res.n, res.r));
+            ZgemmJob j2 = !mir ? zjob(Cd, res.m, ZOP_N, T, res.r, ZOP_N, Z, res.m, res.m, res.n, res.r)
+                               : zjob(Rd, ldr, ZOP_T, T, res.r, ZOP_N, Z, res.m, res.m, res.n, res.r);
             j2.alpha = make_double2(-1.0, 0.0);
             j2.beta = make_double2(1.0, 0.0);
             g2.push_back(j2);

@@ -38,6 +38,10 @@ struct BlockResult {
     double est = 0;
     int arena = -1;
     size_t offC = 0, offRx = 0, offU = 0, offI = 0, offJ = 0;
+    // >= 0: this block is the transpose of block `mirror` (Galerkin symmetry Z = Z^T), whose
+    // factors it shares: C = R_p^T, U = U_p^T, R = C_p^T, I = J_p, J = I_p. m and n are this
+    // block's own sizes; the other fields describe the primary's storage.
+    int mirror = -1;
 };
 
 struct RoundArena {
@@ -52,6 +56,7 @@ struct RoundArena {
 struct RecompSlot {
     size_t offCp, offRp, offS;
     int k;
+    int mirror;  // >= 0: the transpose of that block's recompression (offsets are its)
 };
 
 // Compressed store of the recompressed blocks (csrc/store.cu): host copy of its layout.
@@ -101,6 +106,8 @@ struct pskel_ctx {
     int split[2] = {8, 8};  // fill variant: 8 triangle moments, 0 two rows per thread, 1/2/4 lanes per entry
     int tri_cols = pskel::kTriFillColsDefault;  // columns per CTA of the triangle-moment fill
     int geom32 = 0;  // complex-FP32 fill: 1 = FP32 pair geometry from per-item offsets
+    int symmetric = 0;        // compress one block of each (t, s) / (s, t) pair, mirror the other
+    std::vector<int> partner; // per block: index of the block with swapped groups, or -1
     double timing[13] = {};  // [0..11] as reported by pskel_last_timing, [12] core SVD count
     // CUDA graph of the first round
     cudaGraphExec_t graph = nullptr;

@@ -68,10 +68,11 @@ __device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 *hi, __nv_bflo
 
 // ---------------------------------------------------------------- pack (once per recompression)
 struct PackBlock {
-    const double2 *Cp;  // m x r (ld m), first k columns
+    const double2 *Cp;  // m x r (ld ldcp), first k columns
     const double2 *Rp;  // r x n (ld r), first k rows
     const double *S;    // k
     int m, n, r, k;
+    int trans, ldcp;    // trans: mirror block, Cp and Rp are its primary's (C' = R'_p^T, R' = C'_p^T)
     long long a1_base;  // phase-1 group base (elements) and the block's first row in it
     int a1_kc, a1_row0;
     long long a2_base;  // phase-2 group base and the block's first K column (real part)
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__
     // phase 1: rows S_i R'(i, :) of the source group's stack, [re | im] along K
     for (int e = threadIdx.x; e < w.k * w.n; e += blockDim.x) {
         const int i = e % w.k, j = e / w.k;
-        const double2 v = w.Rp[i + (size_t)j * w.r];
+        const double2 v = w.trans ? w.Cp[j + (size_t)i * w.ldcp] : w.Rp[i + (size_t)j * w.r];
         const double s = w.S[i];
         const int row = w.a1_row0 + i;
         const long long o_re = st_a_off(w.a1_base, w.a1_kc, row, j);
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__
     // phase 2: columns C'(:, i) in the test group's stack
     for (int e = threadIdx.x; e < w.m * w.k; e += blockDim.x) {
         const int i = e % w.m, j = e / w.m;
-        const double2 v = w.Cp[i + (size_t)j * w.m];
+        const double2 v = w.trans ? w.Rp[j + (size_t)i * w.r] : w.Cp[i + (size_t)j * w.ldcp];
         const long long o_re = st_a_off(w.a2_base, w.a2_kc, i, w.a2_col0 + j);
         const long long o_im = st_a_off(w.a2_base, w.a2_kc, i, w.a2_K + w.a2_col0 + j);
         split_bf16((float)v.x, A2h + o_re, A2l + o_re);
@@ -529,6 +530,8 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
         w.n = res.n;
         w.r = res.r;
         w.k = sl.k;
+        w.trans = sl.mirror >= 0 ? 1 : 0;
+        w.ldcp = sl.mirror >= 0 ? c->results[sl.mirror].m : res.m;
     }
     L.a1 = a1;
     L.a2 = a2;

@@ -82,6 +82,7 @@ SIGNATURES = {
     "pskel_set_fill_split": (ci, [VP, ci, ci]),
     "pskel_set_tri_cols": (ci, [VP, ci]),
     "pskel_set_fill_geometry": (ci, [VP, ci]),
+    "pskel_set_symmetric": (ci, [VP, ci]),
     "pskel_matvec": (ci, [VP, VP, ci, VP, ci, ci, ci, VP]),
     "pskel_recompress": (ci, [VP, cd, I32]),
     "pskel_get_recompressed": (ci, [VP, ci, VP, D, VP]),

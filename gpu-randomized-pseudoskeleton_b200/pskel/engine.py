@@ -232,6 +232,16 @@ class Engine:
         """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
+    def set_symmetric(self, on: bool = True):
+        """Compress one block of each (t, s) / (s, t) pair and take the other as its transpose
+        (Galerkin symmetry Z = Z^T)."""
+        _lib.check(self._lib.pskel_set_symmetric(self._h, int(bool(on))))
+
+    def mirror_of(self) -> np.ndarray:
+        """Per block: the index of the block with swapped groups (-1 if none)."""
+        where = {(int(t), int(s)): b for b, (t, s) in enumerate(zip(self._gt, self._gs))}
+        return np.array([where.get((int(s), int(t)), -1) for t, s in zip(self._gt, self._gs)])
+
     def set_fill_geometry(self, fp32_offsets: bool):
         """Complex-FP32 triangle-moment fill: FP32 pair geometry from per-item offsets (True)
         or FP64 differences and phase (False, default)."""

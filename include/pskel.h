@@ -264,6 +264,15 @@ int pskel_set_tri_cols(pskel_ctx *ctx, int cols);
    offsets (phase error ~1e-7 turn). Selected by the autotuner. */
 int pskel_set_fill_geometry(pskel_ctx *ctx, int fp32_offsets);
 
+/* Symmetric mode (on = 1): of every pair of blocks (t, s) and (s, t) in the block list, only the
+   one with the smaller index is compressed; the other is its transpose (the Galerkin EFIE matrix
+   is symmetric, Z = Z^T, for equal test and source rules): C = R_p^T, U = U_p^T, R = C_p^T with
+   the sample sets swapped, which is exactly the CUR that the other block's own round would form
+   from those samples, with the same error. pskel_get_block, pskel_true_errors, pskel_matvec,
+   pskel_recompress and the store treat such blocks as transposes. The per-block driving mode
+   ignores it. No counterpart in the reference, which compresses single blocks. */
+int pskel_set_symmetric(pskel_ctx *ctx, int on);
+
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
