@@ -221,8 +221,15 @@ def run_ours(args, rank, world, dev):
         return np.clip(np.ceil(pred.margin * np.exp2(y)), 1, Dmin).astype(np.int32)
 
     def step():
+        eng.set_symmetric(True)
         r0 = predict_r0()
         return eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
+
+    def without_symmetry(fn):
+        def run():
+            eng.set_symmetric(False)
+            return fn()
+        return run
 
     def timed(fn, steps, warmup):
         for _ in range(warmup):
@@ -262,18 +269,22 @@ def run_ours(args, rank, world, dev):
     # plain FP64 GPU pseudoskeleton (the drop-in baseline): start at min(m,n)/10 and double,
     # driven one block at a time as the reference's drivers call its GPU CUR; same kernels,
     # samples and estimator as the batched modes
-    plain_pb = lambda: eng.compress(TOL, per_block=True, **PLAIN)
+    plain_pb = without_symmetry(lambda: eng.compress(TOL, per_block=True, **PLAIN))
     plain_ms, _, _, _ = timed(plain_pb, 1, 1)
-    # ablations, all blocks batched per round: plain FP64, mixed precision only, learned only
-    plain = lambda: eng.compress(TOL, **PLAIN)
+    # ablations, all blocks batched per round, every block compressed (no symmetry): plain FP64,
+    # mixed precision only, learned only, learned + mixed
+    plain = without_symmetry(lambda: eng.compress(TOL, **PLAIN))
     plain_b_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
     t_plain = eng.timing()
-    mixed_only = lambda: eng.compress(TOL, **dict(PLAIN, precision="c64"))
+    mixed_only = without_symmetry(lambda: eng.compress(TOL, **dict(PLAIN, precision="c64")))
     mixed_ms, _, _, _ = timed(mixed_only, 1, 1)
-    learned_only = lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
-                                        **dict(PRODUCT, precision="c128"))
+    learned_only = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
+                                                         **dict(PRODUCT, precision="c128")))
     learned_ms, _, _, _ = timed(learned_only, 1, 2)
+    lm_nosym = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True, **PRODUCT))
+    lm_nosym_ms, _, _, _ = timed(lm_nosym, 1, 2)
     # per-phase timing of the product without the graph (roofline of the fill)
+    eng.set_symmetric(True)
     r0 = predict_r0()
     st_np = eng.compress(TOL, r0=r0, use_graph=False, **PRODUCT)
     tph = eng.timing()
@@ -286,8 +297,11 @@ def run_ours(args, rank, world, dev):
     err = eng.true_errors()
     err_plain = None
     if args.plain_errors:
+        eng.set_symmetric(False)
         st_plain = eng.compress(TOL, **PLAIN)
         err_plain = eng.true_errors()
+        eng.set_symmetric(True)
+        st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     blockops = run_blockops(eng, st, m, flush)
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
@@ -307,16 +321,23 @@ def run_ours(args, rank, world, dev):
                     quadrature="7-point per triangle", precision=PRODUCT["precision"],
                     pinv_tau_relative=PRODUCT["tau"], estimator="16 extra rows + 16 extra columns, safety 2",
                     l2="512 MB write before every timed step (inputs also exceed L2)",
-                    fill_variant=f"{tune['choice'][0]}{tune['choice'][1]} (autotuned: {tune['ms']} ms)"),
+                    fill_variant=f"{tune['choice'][0]}{tune['choice'][1]} (autotuned: {tune['ms']} ms)",
+                    symmetry="one block of each (t,s)/(s,t) pair compressed, the other taken as its "
+                             "transpose (Galerkin Z = Z^T); every block's error measured against its "
+                             "own dense FP64 fill"),
         plain_ms=round(plain_ms, 3), speedup_vs_plain=round(plain_ms / ms, 3),
         plain_desc="plain FP64 GPU pseudoskeleton: start min(m,n)/10, doubling, same estimator, "
                    "driven one block at a time (the reference's per-block driving)",
         ablation_ms=dict(plain_batched=round(plain_b_ms, 3), mixed_batched=round(mixed_ms, 3),
-                         learned_batched=round(learned_ms, 3), learned_mixed_batched=round(ms, 3)),
+                         learned_batched=round(learned_ms, 3),
+                         learned_mixed_batched=round(lm_nosym_ms, 3),
+                         learned_mixed_batched_symmetric=round(ms, 3)),
         speedup_vs_plain_batched=round(plain_b_ms / ms, 3),
         step_times_ms=[round(t, 3) for t in times],
         phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},
         product=dict(r_mean=float(st["r"].mean()), rounds_mean=float(st["rounds"].mean()),
+                     blocks_compressed=int(sum(1 for b, p in enumerate(eng.mirror_of()) if p < 0 or b < p)),
+                     blocks_mirrored=int(sum(1 for b, p in enumerate(eng.mirror_of()) if 0 <= p < b)),
                      first_round_accepted=float(np.mean(st["rounds"] == 1)),
                      err_max=float(err.max()), err_median=float(np.median(err)),
                      blocks_over_tol=int((err > TOL).sum()),
@@ -453,6 +474,7 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
     eng = Engine(dev)
     if fill_choice is not None:  # the fill variant the autotuner picked for this GPU and workload
         autotune.apply(eng, PRODUCT["precision"], fill_choice)
+    eng.set_symmetric(True)
     L = _lib.lib()
     feats_host = features(sp, K_WAVE, TOL)
     x_pin = torch.from_numpy(((feats_host - pred.mean) / pred.std).astype(np.float32)).pin_memory()
