@@ -178,6 +178,36 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- GPU arm
+def shard_blocks(gt, gs, rank: int, world: int) -> np.ndarray:
+    """Block indices of one rank: the unordered group pairs {t, s} dealt round-robin, each rank
+    taking both (t, s) and (s, t) of its pairs, so the symmetric mode still halves every rank's
+    work. No data crosses ranks: every block is independent."""
+    gt = np.asarray(gt)
+    gs = np.asarray(gs)
+    where = {(int(t), int(s)): b for b, (t, s) in enumerate(zip(gt, gs))}
+    primaries = [b for b, (t, s) in enumerate(zip(gt, gs))
+                 if where.get((int(s), int(t)), -1) < 0 or b < where[(int(s), int(t))]]
+    mine = []
+    for i, b in enumerate(primaries):
+        if i % world != rank:
+            continue
+        mine.append(b)
+        p = where.get((int(gs[b]), int(gt[b])), -1)
+        if p >= 0 and p != b:
+            mine.append(p)
+    return np.array(sorted(mine), dtype=np.int64)
+
+
+def max_over_ranks(value: float, world: int, device=None) -> float:
+    """The largest of the ranks' values (the job's time is its slowest rank's)."""
+    if world <= 1:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_ours(args, rank, world, dev):
     import torch
 
@@ -190,7 +220,7 @@ def run_ours(args, rank, world, dev):
     L = _lib.lib()
     m, part = build_workload(args.workload)
     # shard blocks over ranks (interleaved: balanced sizes)
-    mine = np.arange(part.n_blocks)[rank::world]
+    mine = shard_blocks(part.gt, part.gs, rank, world)
     sub_gt, sub_gs = part.gt[mine], part.gs[mine]
     pred = Predictor.load()
     eng = Engine(dev)
@@ -198,8 +228,13 @@ def run_ours(args, rank, world, dev):
     eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt, gs=sub_gs)
     nb = len(mine)
     # fill variant picked by the autotuner on this GPU and block list (outside the timed region)
-    tune = autotune.autotune_fill(eng, PRODUCT["precision"], samples=24, repeats=1,
-                                  gpu_name=torch.cuda.get_device_name(dev))
+    if args.fill_variant:  # given (e.g. for a profile without the autotuner's launches)
+        kind = args.fill_variant.rstrip("0123456789")
+        tune = {"choice": (kind, int(args.fill_variant[len(kind):])), "ms": "given", "cached": False}
+        autotune.apply(eng, PRODUCT["precision"], tune["choice"])
+    else:
+        tune = autotune.autotune_fill(eng, PRODUCT["precision"], samples=24, repeats=1,
+                                      gpu_name=torch.cuda.get_device_name(dev))
 
     class Sub:  # the rank's block list, for the feature builder
         pass
@@ -250,10 +285,7 @@ def run_ours(args, rank, world, dev):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1))
         launches = L.pskel_kernel_launches() - launches0
-        t = torch.tensor([float(np.mean(times))], device="cuda")
-        if world > 1:
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item()), out, launches // max(steps, 1), times
+        return max_over_ranks(float(np.mean(times)), world, "cuda"), out, launches // max(steps, 1), times
 
     with ClockSampler(dev) as clk:
         ms, st, launches, times = timed(step, args.steps, args.warmup)
@@ -526,6 +558,9 @@ def main():
     ap.add_argument("--save", default=None, help="write per-block stats (npz)")
     ap.add_argument("--plain-errors", action="store_true", help="also check the plain run's errors")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fill-variant", default=None,
+                    help="fill variant instead of the autotuner's choice: tri<w> or tri32_<w> "
+                         "(w = 0 balanced, 4, 8, 16) or entry<s>")
     ap.add_argument("--product-only", action="store_true",
                     help="time the product steps only (no baselines, ablations, checks): the "
                          "command the kernel launch list is captured from")
