@@ -53,7 +53,7 @@ WORKLOADS = {
 
 # DRAM bytes (read + write) of the round-1 fill launch of the product step on sphere30k, from
 # one ncu capture (profiles/tri_fill_traffic_sphere30k.md)
-FILL_TRAFFIC_BYTES = 5.534e9
+FILL_TRAFFIC_BYTES = 2.186e9
 
 PRODUCT = dict(precision="c64", tau=1e-7, extra_rows=16, extra_cols=16, est_safety=2.0,
                oversample=0, max_rounds=12, seed=0)
