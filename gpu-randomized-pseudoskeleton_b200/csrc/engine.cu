@@ -562,7 +562,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     else
         gather_core_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.svd, 60, s));
+    PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.svd, 60, s, &c->svd_par));
     PSKEL_TRY(batched_pinv(p.d_pinv, p.nb, p.pinv_tiles, s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));
     if (o.precision == PSKEL_C64)
@@ -611,6 +611,8 @@ extern "C" int pskel_create(pskel_ctx **out, int device) {
         }
     int st = c->flags.reserve(256);
     if (st != PSKEL_OK) return fail(st);
+    st = svd_streams_create(c->svd_par);
+    if (st != PSKEL_OK) return fail(st);
     cudaMemsetAsync(c->flags.ptr, 0, 256, c->stream);
     *out = c;
     return PSKEL_OK;
@@ -631,6 +633,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->mv_table.release();
     for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
+    svd_streams_destroy(c->svd_par);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSKEL_OK;

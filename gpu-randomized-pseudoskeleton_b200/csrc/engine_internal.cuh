@@ -87,6 +87,7 @@ struct pskel_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
+    pskel::SvdStreams svd_par;  // side streams of the concurrent SVD size classes
     DevMesh mesh;
     pskel_em_t em{};
     bool have_mesh = false;

@@ -20,6 +20,7 @@
 //  * blocked: one CTA per matrix keeps 2b columns of A and V in shared memory at a time and
 //    sweeps over all block pairs, the matrix itself staying in global memory (L2-resident);
 //    used for the large sample counts of the reference's doubling rule.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -37,7 +38,10 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 
 // circle-method player at position pos in round rho for nn (even) players
 __device__ __forceinline__ int circle_player(int pos, int rho, int nn) {
-    return pos == 0 ? 0 : ((pos - 1 + rho) % (nn - 1)) + 1;
+    // (pos - 1 + rho) mod (nn - 1) without a division: both terms are below nn - 1
+    int v = pos - 1 + rho;
+    if (v >= nn - 1) v -= nn - 1;
+    return pos == 0 ? 0 : v + 1;
 }
 
 // One round-robin sweep over the w columns held in shared memory (column-major, lds rows for
@@ -593,17 +597,59 @@ int svd_resident_attr() {
     return PSKEL_OK;
 }
 
+int svd_streams_create(SvdStreams &p) {
+    if (p.ready) return PSKEL_OK;
+    for (int i = 0; i < kSvdAux; ++i) {
+        PSKEL_CUDA(cudaStreamCreateWithFlags(&p.aux[i], cudaStreamNonBlocking));
+        PSKEL_CUDA(cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming));
+    }
+    PSKEL_CUDA(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming));
+    p.ready = true;
+    return PSKEL_OK;
+}
+
+void svd_streams_destroy(SvdStreams &p) {
+    if (!p.ready) return;
+    for (int i = 0; i < kSvdAux; ++i) {
+        cudaStreamDestroy(p.aux[i]);
+        cudaEventDestroy(p.join[i]);
+    }
+    cudaEventDestroy(p.fork);
+    p.ready = false;
+}
+
 int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
-               cudaStream_t stream) {
+               cudaStream_t stream, const SvdStreams *par) {
     PSKEL_TRY(svd_resident_attr());
-    for (const SvdPlan::Cls &c : plan.res) {
-        svd_resident_kernel<<<c.count, c.threads, c.smem, stream>>>(d_jobs, d_idx + c.off, max_sweeps);
+    const int nl = (int)plan.res.size() + (plan.blk_count > 0 ? 1 : 0);
+    // launch l on the main stream (l = 0) or on side stream l - 1 (the classes are independent)
+    const bool fan = par && par->ready && nl > 1;
+    const int used = fan ? std::min(nl - 1, kSvdAux) : 0;
+    if (fan) {
+        PSKEL_CUDA(cudaEventRecord(par->fork, stream));
+        for (int a = 0; a < used; ++a) PSKEL_CUDA(cudaStreamWaitEvent(par->aux[a], par->fork, 0));
+    }
+    auto lane = [&](int l) -> cudaStream_t { return (!fan || l == 0) ? stream : par->aux[(l - 1) % kSvdAux]; };
+    int l = 0;
+    // the class with the most jobs on the main stream
+    std::vector<int> order(plan.res.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return plan.res[a].count > plan.res[b].count; });
+    for (int ci : order) {
+        const SvdPlan::Cls &c = plan.res[ci];
+        cudaStream_t s = lane(l++);
+        svd_resident_kernel<<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
     if (plan.blk_count > 0) {
-        svd_blocked_kernel<<<plan.blk_count, kSvdThreads, kSmemBudget, stream>>>(
+        cudaStream_t s = lane(l++);
+        svd_blocked_kernel<<<plan.blk_count, kSvdThreads, kSmemBudget, s>>>(
             d_jobs, d_idx + plan.blk_off, max_sweeps, (int)kSmemBudget);
         PSKEL_LAUNCHED(1);
+    }
+    for (int a = 0; a < used; ++a) {
+        PSKEL_CUDA(cudaEventRecord(par->join[a], par->aux[a]));
+        PSKEL_CUDA(cudaStreamWaitEvent(stream, par->join[a], 0));
     }
     return PSKEL_OK;
 }

@@ -202,8 +202,18 @@ struct SvdPlan {
     int blk_off = 0, blk_count = 0;
 };
 int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan);
+// Side streams for the size-class launches of one SVD plan: the classes are independent, so
+// they run concurrently (fork on `fork`, join through `join`); graph capture follows the events.
+constexpr int kSvdAux = 4;
+struct SvdStreams {
+    cudaStream_t aux[kSvdAux] = {};
+    cudaEvent_t fork = nullptr, join[kSvdAux] = {};
+    bool ready = false;
+};
+int svd_streams_create(SvdStreams &p);
+void svd_streams_destroy(SvdStreams &p);
 int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
-               cudaStream_t stream);
+               cudaStream_t stream, const SvdStreams *par = nullptr);
 // One resident job (m x n fits in shared memory) whose index map entry is d_idx0[0].
 int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
                                cudaStream_t stream);
