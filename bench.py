@@ -335,6 +335,7 @@ def run_ours(args, rank, world, dev):
         eng.set_symmetric(True)
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     blockops = run_blockops(eng, st, m, flush)
+    octree_t = run_octree(args, m, part, dev) if rank == 0 else None
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
                                    fill_choice=tune["choice"])
@@ -397,6 +398,7 @@ def run_ours(args, rank, world, dev):
                  d2h_bytes_per_step=int(d2h)),
         clocks=clocks, gpu_launches=int(launches),
         blockops=blockops,
+        octree=octree_t,
     )
     eng.close()
     return out
@@ -488,6 +490,47 @@ def _hbm_peak():
             return float(json.load(f)["hbm_gbs"])
     except (OSError, KeyError, ValueError):
         return 6650.0
+
+
+def run_octree(args, m, part, dev, reps=5):
+    """The workload's octree partition and far list built on the device (mesh resident) against
+    the host restatement: wall times of the whole call (device build + copy-out to host arrays)
+    and of the device build alone, and whether the two partitions are identical."""
+    import time
+
+    from pskel import octree
+    from pskel.engine import Engine
+    w = WORKLOADS[args.workload]
+    kw = dict(origin=(0, 0, 0), min_group=w["min_group"])
+    with Engine(dev) as eng:
+        eng.upload_mesh(m, K_WAVE, ETA, q=7)
+        d = eng.octree(w["leaf"], **kw)
+        same = (np.array_equal(d.group_ptr, part.group_ptr) and np.array_equal(d.group_ids, part.group_ids)
+                and np.array_equal(d.centres, part.centres) and np.array_equal(d.gt, part.gt)
+                and np.array_equal(d.gs, part.gs))
+        tg, tb = [], []
+        o = np.zeros(3)
+        ng, nbk = ctypes.c_int(), ctypes.c_longlong()
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            eng.octree(w["leaf"], **kw)
+            tg.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            rc = eng._lib.pskel_octree_build(eng._h, w["leaf"], o.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                             2.0, w["min_group"], 0, ctypes.byref(ng), ctypes.byref(nbk))
+            tb.append(time.perf_counter() - t0)
+            assert rc == 0
+    th = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        octree.partition(m, w["leaf"], **kw)
+        th.append(time.perf_counter() - t0)
+    return dict(groups=int(d.n_groups), blocks=int(d.n_blocks), identical_to_host=bool(same),
+                device_ms=round(1e3 * float(np.median(tg)), 3),
+                device_build_only_ms=round(1e3 * float(np.median(tb)), 3),
+                host_ms=round(1e3 * float(np.median(th)), 3),
+                desc="Morton keys, CUB radix sort, key runs, far test on the device; small-group "
+                     "merge on the host; host = numpy restatement (pskel/octree.py)")
 
 
 def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None):

@@ -22,6 +22,7 @@ LIB = os.path.join(HERE, "libpskel_b200.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+              "-Xcompiler", "-ffp-contract=off",
               "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC]
 
 

@@ -634,6 +634,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     svd_streams_destroy(c->svd_par);
+    octree_release(c->octree);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSKEL_OK;

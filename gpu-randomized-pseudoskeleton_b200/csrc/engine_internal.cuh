@@ -27,6 +27,20 @@ struct BlockWork {
     double *est;
 };
 
+// Single-level octree partition of the uploaded mesh's RWG basis centres and its far-pair list,
+// built on the device (csrc/octree.cu). Group ids, extents and the far list stay in device
+// memory; offsets and centres are kept on the host as well.
+struct OctreeState {
+    DevBuf hdr, c, idx, ka, kb, va, vb, cnt, start, bc, map, fkey, fkey2, gids, gptr, fc, ext;
+    DevBuf rowcnt, rowoff, gt, gs, tmp;
+    int n = 0, n_groups = 0;
+    long long n_blocks = 0;
+    std::vector<int> h_gptr;
+    std::vector<double> h_centres;  // (G, 3) row-major
+    bool valid = false;
+};
+void octree_release(OctreeState &o);
+
 }  // namespace pskel
 
 using pskel::BlockWork;
@@ -124,5 +138,6 @@ struct pskel_ctx {
     int mv_max_r = 0;
     StoreLayout store;                      // compressed store (bf16 hi/lo planes, tiled)
     DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
+    pskel::OctreeState octree;              // device octree partition (pskel_octree_build)
 };
 

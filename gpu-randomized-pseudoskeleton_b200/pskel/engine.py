@@ -87,6 +87,35 @@ class Engine:
         self.partition = part
         self._gp, self._gi, self._gt, self._gs = gp, gi, t, s
 
+    def octree(self, leaf: float, origin=None, admissibility: float = 2.0, min_group: int = 1,
+               symmetric: bool = False):
+        """Octree partition of the uploaded mesh built on the device: the same
+        ``octree.Partition`` as ``octree.partition(mesh, ...)`` on the host, bit for bit
+        (extents to rounding)."""
+        from . import octree as _oct
+        ng, nb = ctypes.c_int(), ctypes.c_longlong()
+        o = None
+        if origin is not None:
+            o = np.ascontiguousarray(origin, dtype=np.float64)
+            if o.shape != (3,):
+                raise ValueError("origin: 3 coordinates")
+            o = o.ctypes.data_as(_lib.D)
+        _lib.check(self._lib.pskel_octree_build(self._h, float(leaf), o, float(admissibility),
+                                                int(min_group), int(bool(symmetric)),
+                                                ctypes.byref(ng), ctypes.byref(nb)))
+        g, b = ng.value, nb.value
+        gp = np.empty(g + 1, dtype=np.int32)
+        gi = np.empty(self.mesh.N, dtype=np.int32)
+        cen = np.empty((g, 3), dtype=np.float64)
+        ext = np.empty(g, dtype=np.float64)
+        gt = np.empty(b, dtype=np.int32)
+        gs = np.empty(b, dtype=np.int32)
+        P = lambda x: x.ctypes.data_as(_lib.I32)
+        _lib.check(self._lib.pskel_octree_get(self._h, P(gp), P(gi), cen.ctypes.data_as(_lib.D),
+                                              ext.ctypes.data_as(_lib.D), P(gt), P(gs)))
+        return _oct.Partition(group_ptr=gp, group_ids=gi, centres=cen, extents=ext, gt=gt, gs=gs,
+                              leaf=float(leaf))
+
     @property
     def n_blocks(self) -> int:
         return len(self._gt)

@@ -12,6 +12,10 @@ not shipped). This module supplies the partition the far-field workloads are def
   size-weighted centre) so that every block has at least that many rows and columns;
 * far pairs = ordered group pairs (i, j), i != j, whose box centres are at least
   ``admissibility`` x the box diameter (sqrt(3) * leaf) apart.
+
+Every floating-point step is an elementwise IEEE operation in a fixed order (distances are
+sqrt((dx*dx + dy*dy) + dz*dz), no BLAS reductions), so that the device partition
+(``Engine.octree``) reproduces the groups, the group centres and the far list bit for bit.
 """
 from __future__ import annotations
 
@@ -57,6 +61,15 @@ def _morton3(ix, iy, iz):
     return spread(ix) | (spread(iy) << np.uint64(1)) | (spread(iz) << np.uint64(2))
 
 
+def _dist(a, b):
+    """Euclidean distance of (..., 3) points, as sqrt((dx*dx + dy*dy) + dz*dz) with every
+    product and sum rounded separately."""
+    dx = a[..., 0] - b[..., 0]
+    dy = a[..., 1] - b[..., 1]
+    dz = a[..., 2] - b[..., 2]
+    return np.sqrt((dx * dx + dy * dy) + dz * dz)
+
+
 def partition(mesh, leaf: float, origin=None, admissibility: float = 2.0,
               min_group: int = 1, symmetric: bool = False) -> Partition:
     c = mesh.basis_centres().T  # (N, 3)
@@ -85,7 +98,7 @@ def partition(mesh, leaf: float, origin=None, admissibility: float = 2.0,
                 break
             i = alive[k]
             others = [j for j in alive if j != i]
-            d = [np.linalg.norm(cen[j] - cen[i]) for j in others]
+            d = _dist(np.array([cen[j] for j in others]), cen[i])
             j = others[int(np.argmin(d))]
             ni, nj = len(members[i]), len(members[j])
             cen[j] = (cen[j] * nj + cen[i] * ni) / (ni + nj)
@@ -99,8 +112,7 @@ def partition(mesh, leaf: float, origin=None, admissibility: float = 2.0,
     centres = np.array(box_centre)
     ext = np.array([2 * np.linalg.norm(c[g] - c[g].mean(axis=0), axis=1).max() for g in groups])
     diam = np.sqrt(3.0) * leaf
-    d = np.linalg.norm(centres[:, None, :] - centres[None, :, :], axis=2)
-    far = d >= admissibility * diam
+    far = _dist(centres[:, None, :], centres[None, :, :]) >= admissibility * diam
     np.fill_diagonal(far, False)
     if symmetric:
         far = np.triu(far, 1)

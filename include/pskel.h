@@ -273,6 +273,27 @@ int pskel_set_fill_geometry(pskel_ctx *ctx, int fp32_offsets);
    ignores it. No counterpart in the reference, which compresses single blocks. */
 int pskel_set_symmetric(pskel_ctx *ctx, int on);
 
+/* Single-level octree partition of the uploaded mesh's RWG basis functions and its far-field
+   block list, built on the device. The reference has no partitioner: its multi-block driver
+   (compres_single_block_spheres.jl:1109-1347) reads MATLAB-made block lists; this builds the
+   partition its far-field workloads are defined on. Each RWG goes to the cube of side `leaf`
+   (aligned at `origin`, 3 doubles; NULL = centre of the bounding box of the basis centres)
+   holding its basis centre (user_get_OG_basis_center.m:36-39); groups are the non-empty cubes
+   in Morton order; groups below `min_group` are folded, smallest first, into the nearest group
+   (size-weighted centre); far pairs are (i, j), i != j (i < j if `symmetric`), with centres at
+   least admissibility * sqrt(3) * leaf apart, in row-major order. Outputs the group and block
+   counts; pskel_octree_get copies the result out. Exactly the host restatement's partition
+   (every step IEEE-rounded in the same order). */
+int pskel_octree_build(pskel_ctx *ctx, double leaf, const double *origin, double admissibility,
+                       int min_group, int symmetric, int *n_groups, long long *n_blocks);
+
+/* Copy the last octree partition to host arrays (any may be NULL): group_ptr (G + 1 CSR
+   offsets), group_ids (N 0-based RWG ids, ascending within each group), centres (G x 3
+   row-major), extents (G diameters of the groups' bounding spheres about their mean centre),
+   gt / gs (n_blocks test and source groups). The arrays feed pskel_set_blocks directly. */
+int pskel_octree_get(pskel_ctx *ctx, int *group_ptr, int *group_ids, double *centres,
+                     double *extents, int *gt, int *gs);
+
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
