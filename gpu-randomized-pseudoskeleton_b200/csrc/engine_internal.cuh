@@ -139,5 +139,6 @@ struct pskel_ctx {
     StoreLayout store;                      // compressed store (bf16 hi/lo planes, tiled)
     DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
     pskel::OctreeState octree;              // device octree partition (pskel_octree_build)
+    DevBuf near_jobs, near_mom;             // near-field fill: job table, same-triangle moments
 };
 

@@ -18,6 +18,7 @@ struct LegacyCtx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     DevMesh mesh;
     DevBuf flags, ids_raw, ids, jobs, out, work, scratch, scratch2;
+    DevBuf near_jobs, near_mom;  // near-field fill: job table and same-triangle moments
     std::mutex mu;
 };
 
@@ -83,8 +84,13 @@ int upload_ids(LegacyCtx &c, const double *const *lists, const int *lens, int nl
     return PSKEL_OK;
 }
 
+// Fill the jobs with the reference's element routine semantics: the centroid-rule kernel first,
+// flagging any triangle pair closer than the largest radius (and every same-triangle pair, whose
+// centroid distance is 0); if one is flagged, the whole request is refilled by the near-field
+// kernel (4-point rules, exact static 1/R, same-triangle term), so far-only requests keep the
+// fast path. Synchronises the stream when flagging is possible.
 int fill_jobs(LegacyCtx &c, const std::vector<FillJob> &jobs, double k, double eta,
-              double r_near) {
+              const NearRadii &radii) {
     int tm, tn;
     fill_tile_shape(PSKEL_C128, 1, 0, &tm, &tn);
     std::vector<int> prefix(jobs.size() + 1, 0);
@@ -97,15 +103,25 @@ int fill_jobs(LegacyCtx &c, const std::vector<FillJob> &jobs, double k, double e
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c.stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int) * prefix.size(),
                                cudaMemcpyHostToDevice, c.stream));
+    double r = radii.rinteg_s;
+    if (radii.ranal_s > r) r = radii.ranal_s;
+    if (radii.rinteg_f > r) r = radii.rinteg_f;
     FillParams p;
     p.k = k;
     p.eta = eta;
-    p.r_near = r_near;
+    p.r_near = r > 1e-150 ? r : 1e-150;  // > 0: same-triangle pairs (distance 0) are flagged too
     p.q_test = p.q_src = 1;
     p.precision = PSKEL_C128;
     p.split = 0;
-    return launch_fill(c.mesh, p, d_jobs, d_prefix, (int)jobs.size(), prefix.back(),
-                       c.flags.as<int>(), c.stream);
+    PSKEL_TRY(launch_fill(c.mesh, p, d_jobs, d_prefix, (int)jobs.size(), prefix.back(),
+                          c.flags.as<int>(), c.stream));
+    int h = 0;
+    PSKEL_CUDA(cudaMemcpyAsync(&h, c.flags.ptr, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+    PSKEL_CUDA(cudaStreamSynchronize(c.stream));
+    if (!(h & 1) || (h & 6)) return PSKEL_OK;  // far only, or a range error (check_flags)
+    PSKEL_CUDA(cudaMemsetAsync(c.flags.ptr, 0, sizeof(int), c.stream));
+    return near_fill_jobs(c.mesh, radii, k, eta, jobs, c.near_jobs, c.near_mom, c.flags.as<int>(),
+                          c.stream, false);
 }
 
 // Read the flag word after the stream drains; maps bits to statuses.
@@ -117,20 +133,16 @@ int check_flags(LegacyCtx &c) {
         set_error(PSKEL_ERR_RANGE, "an RWG, triangle or vertex id is out of range");
         return PSKEL_ERR_RANGE;
     }
-    if (h & 1) {
-        set_error(PSKEL_ERR_NEAR,
-                  "a triangle pair lies inside the integration radius; only the far-field "
-                  "(centroid) rule is implemented");
-        return PSKEL_ERR_NEAR;
-    }
     return PSKEL_OK;
 }
 
-double r_near_of(double Rinteg_s, double Ranal_s, double Rinteg_f) {
-    double r = Rinteg_s;
-    if (Ranal_s > r) r = Ranal_s;
-    if (Rinteg_f > r) r = Rinteg_f;
-    return r > 0 ? r : 0.0;
+NearRadii radii_of(double Rinteg_s, double Ranal_s, double Rinteg_f) {
+    NearRadii r;
+    r.rinteg_s = Rinteg_s;
+    r.ranal_s = Ranal_s;
+    r.rinteg_f = Rinteg_f;
+    r.q_far = 1;
+    return r;
 }
 
 int check_field(int field) {
@@ -163,7 +175,7 @@ int dense_fill(LegacyCtx &c, int field, double k, double eta, double Rinteg_s, d
     std::vector<FillJob> jobs(1);
     jobs[0] = FillJob{d_ids[0], d_ids[1], c.out.ptr, n_r1, n_r2, n_r1, 0};
     PSKEL_CUDA(cudaEventRecord(c.ev0, c.stream));
-    if ((size_t)n_r1 * n_r2 > 0) PSKEL_TRY(fill_jobs(c, jobs, k, eta, r_near_of(Rinteg_s, Ranal_s, Rinteg_f)));
+    if ((size_t)n_r1 * n_r2 > 0) PSKEL_TRY(fill_jobs(c, jobs, k, eta, radii_of(Rinteg_s, Ranal_s, Rinteg_f)));
     PSKEL_CUDA(cudaEventRecord(c.ev1, c.stream));
     PSKEL_TRY(check_flags(c));
     PSKEL_CUDA(cudaEventElapsedTime(ms, c.ev0, c.ev1));
@@ -192,8 +204,7 @@ extern "C" double impedance_matrix_cuda_elbyel4(
     int st = dense_fill(c, field, k, eta, Rinteg_s, Ranal_s, Rinteg_f, r1, r2, vertex, topol,
                         edges, ln, cent, N, n_r1, n_r2, rows_vertex, cols_vertex, rows_topol,
                         cols_topol, rows_edges, cols_edges, n_ln, rows_cent, cols_cent, &ms);
-    if (st == PSKEL_ERR_NEAR || st == PSKEL_OK) {
-        // the entries are written either way; a near-field pair makes the result NaN-flagged
+    if (st == PSKEL_OK) {
         if (Ztotal && (size_t)n_r1 * n_r2 > 0 &&
             cudaMemcpy(Ztotal, c.out.ptr, sizeof(double2) * (size_t)n_r1 * n_r2,
                        cudaMemcpyDeviceToHost) != cudaSuccess) {
@@ -532,7 +543,7 @@ extern "C" double cuda_complete_compression(
             FillJob{d_ids[0], d_ids[3], dC, (int)m, r, (int)m, 0},
             FillJob{d_ids[2], d_ids[3], dCore, r, r, r, 0},
             FillJob{d_ids[2], d_ids[1], dR, r, (int)n, r, 0}};
-        PSKEL_TRY(fill_jobs(c, jobs, k, eta, r_near_of(Rinteg_s, Ranal_s, Rinteg_f)));
+        PSKEL_TRY(fill_jobs(c, jobs, k, eta, radii_of(Rinteg_s, Ranal_s, Rinteg_f)));
         PinvOut po;
         po.P = dU;
         po.tau = pinv_tol;

@@ -130,6 +130,19 @@ int launch_fill(const DevMesh &mesh, const FillParams &p, const FillJob *d_jobs,
                 cudaStream_t stream);
 int fill_tile_shape(int precision, int q, int split, int *tm, int *tn);
 
+// Near-field rule (csrc/near.cu): radii of the reference's element routine and the rule of a
+// side outside its radius (1 = centroid, 7 = 7-point).
+struct NearRadii {
+    double rinteg_s = 0.0, ranal_s = 0.0, rinteg_f = 0.0;
+    int q_far = 1;
+};
+// Complex-FP64 fill of the jobs (host list) with the near-field rule, one thread per entry;
+// the same-triangle moments go to mom (8 double2 per triangle), for every triangle or only for
+// the triangles of the jobs' rows. flags bit 2 / 4: RWG / triangle id out of range.
+int near_fill_jobs(const DevMesh &mesh, const NearRadii &r, double k, double eta,
+                   const std::vector<FillJob> &jobs, DevBuf &scratch, DevBuf &mom, int *d_flags,
+                   cudaStream_t stream, bool all_triangles);
+
 // Triangle-moment fill of Z(group, cols) for a group of RWG functions whose triangle list and
 // triangle -> (RWG, side) adjacency are known (see tri_fill_kernel in fill.cu).
 struct GroupFillJob {

@@ -87,6 +87,16 @@ class Engine:
         self.partition = part
         self._gp, self._gi, self._gt, self._gs = gp, gi, t, s
 
+    def fill_near_device(self, rows_dev: int, nr: int, cols_dev: int, nc: int, out_dev: int,
+                         ld: int, rinteg_s: float, ranal_s: float, rinteg_f: float,
+                         q_far: int = 1):
+        """Near-field fill (complex128) into device buffers given as raw device pointers, with
+        the reference element routine's radii (see pskel_fill_near_device)."""
+        _lib.check(self._lib.pskel_fill_near_device(
+            self._h, ctypes.c_void_p(rows_dev), nr, ctypes.c_void_p(cols_dev), nc,
+            ctypes.c_void_p(out_dev), ld, float(rinteg_s), float(ranal_s), float(rinteg_f),
+            int(q_far)))
+
     def octree(self, leaf: float, origin=None, admissibility: float = 2.0, min_group: int = 1,
                symmetric: bool = False):
         """Octree partition of the uploaded mesh built on the device: the same

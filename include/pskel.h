@@ -44,7 +44,7 @@ typedef struct { float re, im; } pskel_c64;
 #define PSKEL_ERR_ARG (-1)        /* bad size, pointer or option */
 #define PSKEL_ERR_CUDA (-2)       /* a CUDA runtime call failed */
 #define PSKEL_ERR_NOCONV (-3)     /* Jacobi SVD hit its sweep limit */
-#define PSKEL_ERR_NEAR (-4)       /* a triangle pair lies inside an integration radius */
+#define PSKEL_ERR_NEAR (-4)       /* unused: near pairs are filled by the near-field rule */
 #define PSKEL_ERR_OOM (-5)        /* device allocation failed */
 #define PSKEL_ERR_RANGE (-6)      /* an RWG id is out of range */
 #define PSKEL_ERR_UNSUPPORTED (-7) /* field != 1 (only EFIE is implemented) */
@@ -222,6 +222,18 @@ int pskel_upload_mesh(pskel_ctx *ctx, const double *vertex, int nv, const double
    (pskel_c64*). Asynchronous on the context's stream. */
 int pskel_fill_device(pskel_ctx *ctx, const int *rows_dev, int nr, const int *cols_dev,
                       int nc, void *Z_dev, int ld, int precision);
+
+/* Fill Z(rows, cols) (complex FP64, DEVICE buffers as in pskel_fill_device) with the near-field
+   rule of the reference's element routine (functionsExternal.so::impedance_matrix, the radii
+   of compres_single_block_spheres.jl:800-840): per triangle pair with centroid distance dc, the
+   4-point rule on the test side if dc < rinteg_f and on the source side if dc < rinteg_s (else
+   the rule q_far: 1 = centroid as the reference, 7 = the 7-point rule), the static 1/R of the
+   source triangle integrated exactly if dc < ranal_s, and the same-triangle term as a converged
+   double integral (the reference's own is an approximation a few per cent off). One thread
+   per entry. Asynchronous on the context's stream. */
+int pskel_fill_near_device(pskel_ctx *ctx, const int *rows_dev, int nr, const int *cols_dev,
+                           int nc, pskel_c128 *Z_dev, int ld, double rinteg_s, double ranal_s,
+                           double rinteg_f, int q_far);
 
 /* Groups (CSR over 0-based RWG ids) and the block list: block b = (test group gt[b],
    source group gs[b]). Host arrays; copied to the device. */

@@ -9,7 +9,7 @@ passed for trian, as at ``:783-784``). The library is executed as a black box on
 Each fixture stores the mesh arrays it was computed on (so the mesh generator is pinned
 too), the EM parameters, the 1-based row/column id lists and the complex128 result.
 
-Usage:  python tests/golden/make_golden.py [reference_root]
+Usage:  python tests/golden/make_golden.py [reference_root] [near]
 """
 from __future__ import annotations
 
@@ -98,5 +98,41 @@ def main():
     save("so_two_spheres_close_centroid.npz", m, r1, r2, k, eta, 0.0, call(f, m, r1, r2, k, eta, 0.0, 0.0, 0.0))
 
 
+def save_near(name, m, r1, r2, k, eta, radii, Z):
+    np.savez_compressed(
+        os.path.join(HERE, name), vertex=m.vertex, topol=m.topol, trian=m.trian, edges=m.edges,
+        un=m.un, ds=m.ds, ln=m.ln, cent=m.cent, rows=np.asarray(r1, dtype=np.int64),
+        cols=np.asarray(r2, dtype=np.int64), k=k, eta=eta, radii=np.asarray(radii, dtype=np.float64),
+        Z=Z)
+    print(name, Z.shape, float(np.abs(Z).max()))
+
+
+def main_near():
+    """Near-field fixtures: blocks whose RWG pairs include same-triangle, adjacent and nearby
+    triangle pairs, with the integration radii (Rinteg_s, Ranal_s, Rinteg_f) switching the
+    library onto its near-field rules."""
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    f = load(ref)
+    eta = 376.73
+    # (n1, n2) one plate of the two-plate workload (lambda = 1): RWG 1-48 against 1-64
+    m = pmesh.two_plates(1.0, 20, 3.0)
+    k = 2 * np.pi
+    r1, r2 = np.arange(1, 49), np.arange(1, 65)
+    for tag, radii in (("r03", (0.3, 0.3, 0.3)), ("mixed", (0.2, 0.4, 0.1))):
+        save_near(f"near_plate_{tag}.npz", m, r1, r2, k, eta, radii, call(f, m, r1, r2, k, eta, *radii))
+    # (n3, n4) a coarse sphere (R = 1, 480 RWG, lambda = 2): 40 RWG against their 60 nearest
+    m = pmesh.icosphere(1.0, 2)
+    k = np.pi
+    c = m.basis_centres().T
+    r1 = np.arange(1, 41)
+    d = np.linalg.norm(c[:, None, :] - c[None, :40, :], axis=2).min(axis=1)
+    r2 = np.sort(np.argsort(d, kind="stable")[:60] + 1)
+    for tag, radii in (("r05", (0.5, 0.5, 0.5)), ("noanal", (1.0, 0.0, 1.0))):
+        save_near(f"near_sphere_{tag}.npz", m, r1, r2, k, eta, radii, call(f, m, r1, r2, k, eta, *radii))
+
+
 if __name__ == "__main__":
+    if len(sys.argv) > 2 and sys.argv[2] == "near":
+        main_near()
+        sys.exit(0)
     main()

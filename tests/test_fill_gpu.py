@@ -51,14 +51,6 @@ def test_fill_variants_agree():
     assert np.array_equal(Z4, Z3) and np.array_equal(Z4, Z2)
 
 
-def test_near_pair_is_reported():
-    m = pmesh.two_spheres(1.0, 3.0, 48)
-    em = api.EMData.for_wavelength(2.0, rint=1.5)
-    with pytest.raises(_lib.PskelError) as e:
-        api.user_impedance_cuda5(np.arange(1, 49), np.arange(49, 97), m, em)
-    assert e.value.code == -4
-
-
 def test_bad_ids_are_reported():
     m = pmesh.two_spheres(1.0, 12.0, 48)
     em = api.EMData.for_wavelength(2.0)
