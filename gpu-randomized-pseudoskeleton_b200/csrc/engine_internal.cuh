@@ -140,5 +140,7 @@ struct pskel_ctx {
     DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
     pskel::OctreeState octree;              // device octree partition (pskel_octree_build)
     DevBuf near_jobs, near_mom;             // near-field fill: job table, same-triangle moments
+    DevBuf near_data, near_tab;             // near blocks (dense complex FP64) and their table
+    int n_near = -1, near_max_n = 0;        // -1: no near blocks built
 };
 

@@ -299,6 +299,28 @@ int pskel_set_symmetric(pskel_ctx *ctx, int on);
 int pskel_octree_build(pskel_ctx *ctx, double leaf, const double *origin, double admissibility,
                        int min_group, int symmetric, int *n_groups, long long *n_blocks);
 
+/* Near-field blocks for the H-matrix product: the n_near group pairs (nt[b], ns[b]) of the
+   groups set by pskel_set_blocks (normally every pair that is not far, diagonal included) are
+   filled densely (complex FP64) with the near-field rule of pskel_fill_near_device and kept on
+   the device; bytes receives their size. The reference assembles whole matrices from block lists
+   (compres_single_block_spheres.jl:1404-1505) and solves them densely or by CBF
+   (compres_single_block_spheres.jl:983-1017). */
+int pskel_near_build(pskel_ctx *ctx, const int *nt, const int *ns, int n_near, double rinteg_s,
+                     double ranal_s, double rinteg_f, int q_far, long long *bytes);
+
+/* Y (+)= sum over near blocks of Z_b X(cols_b) scattered to rows_b (DEVICE complex-FP64 arrays,
+   N x nrhs, nrhs <= 16; accumulate = 0 overwrites Y). With pskel_matvec (which overwrites Y with
+   the far product) this is the whole H-matrix product. stream NULL = legacy default stream. */
+int pskel_near_matvec(pskel_ctx *ctx, const pskel_c128 *X, int ldx, pskel_c128 *Y, int ldy,
+                      int nrhs, int accumulate, void *stream);
+
+/* Plane-wave excitation E (DEVICE, N complex FP64) of the uploaded mesh, as the reference's
+   test_fields (compres_single_block_spheres_for_sweep2.jl:60-85): incidence theta_deg, phi_deg,
+   polarisation rot_deg, the edge-weighted tangential field at the two triangle centroids. Like
+   the reference, phi is divided by 180 without the factor pi. */
+int pskel_plane_wave(pskel_ctx *ctx, double theta_deg, double phi_deg, double rot_deg,
+                     pskel_c128 *E, void *stream);
+
 /* Copy the last octree partition to host arrays (any may be NULL): group_ptr (G + 1 CSR
    offsets), group_ids (N 0-based RWG ids, ascending within each group), centres (G x 3
    row-major), extents (G diameters of the groups' bounding spheres about their mean centre),
