@@ -256,6 +256,22 @@ class Engine:
                                                 ctypes.c_void_p(s)))
         return Y.t()
 
+    def save_store(self, path: str, thresh: float = 0.0):
+        """Write the recompressed far field (after recompress()) to a store file."""
+        _lib.check(self._lib.pskel_store_save(self._h, str(path).encode(), float(thresh)))
+
+    def load_store(self, path: str) -> int:
+        """Load a store file (mesh uploaded first); returns the block count. The groups and
+        blocks are taken from the file."""
+        nb = ctypes.c_int()
+        _lib.check(self._lib.pskel_store_load(self._h, str(path).encode(), ctypes.byref(nb)))
+        from . import storefile
+        hdr = storefile.read(path, factors=False, check=False)  # the library checked the hash
+        self._gp, self._gi, self._gt, self._gs = hdr["group_ptr"], hdr["group_ids"], hdr["gt"], hdr["gs"]
+        self._recomp_k = hdr["k"]
+        self.partition = None
+        return int(nb.value)
+
     def store_status(self) -> int:
         """Error word of the last store_matvec (0 = every pipeline wait completed)."""
         w = np.zeros(1, dtype=np.int32)

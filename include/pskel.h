@@ -299,6 +299,21 @@ int pskel_set_symmetric(pskel_ctx *ctx, int on);
 int pskel_octree_build(pskel_ctx *ctx, double leaf, const double *origin, double admissibility,
                        int min_group, int symmetric, int *n_groups, long long *n_blocks);
 
+/* Write the recompressed far field (after pskel_recompress) to a file: the partition, per block
+   its sizes, kept rank k and mirror link, the factors C' (m x k), S (k), R' (k x n) of every
+   block that is not a transpose, and an FNV-1a hash (layout in csrc/storefile.cu). thresh is
+   recorded as the recompression threshold used. No counterpart in the reference, which keeps
+   its compressed blocks in Julia session files. */
+int pskel_store_save(pskel_ctx *ctx, const char *path, double thresh);
+
+/* Load such a file into a context whose mesh (same RWG count) is uploaded: installs its groups
+   and blocks (as pskel_set_blocks) and its recompressed factors, after which
+   pskel_get_recompressed, pskel_store_build and pskel_store_matvec run as after a
+   pskel_recompress (pskel_matvec, the CUR form, needs the CUR factors and is refused). Rejects a
+   wrong magic, version, RWG count, inconsistent records or a hash mismatch. n_blocks receives
+   the block count. */
+int pskel_store_load(pskel_ctx *ctx, const char *path, int *n_blocks);
+
 /* Near-field blocks for the H-matrix product: the n_near group pairs (nt[b], ns[b]) of the
    groups set by pskel_set_blocks (normally every pair that is not far, diagonal included) are
    filled densely (complex FP64) with the near-field rule of pskel_fill_near_device and kept on
