@@ -636,6 +636,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     svd_streams_destroy(c->svd_par);
     octree_release(c->octree);
     c->near_jobs.release(); c->near_mom.release(); c->near_data.release(); c->near_tab.release();
+    c->aca_buf.release(); c->aca_tab.release();
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSKEL_OK;

@@ -142,5 +142,11 @@ struct pskel_ctx {
     DevBuf near_jobs, near_mom;             // near-field fill: job table, same-triangle moments
     DevBuf near_data, near_tab;             // near blocks (dense complex FP64) and their table
     int n_near = -1, near_max_n = 0;        // -1: no near blocks built
+    // adaptive cross approximation of the far blocks (csrc/aca.cu)
+    DevBuf aca_buf, aca_tab;
+    std::vector<int> aca_k, aca_status, aca_mirror;
+    std::vector<size_t> aca_offU, aca_offV, aca_offI, aca_offJ;
+    int aca_kmax = 0;
+    float aca_ms = 0.0f;
 };
 

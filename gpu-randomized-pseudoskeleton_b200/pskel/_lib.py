@@ -86,6 +86,9 @@ SIGNATURES = {
     "pskel_fill_near_device": (ci, [VP, VP, ci, VP, ci, VP, ci, cd, cd, cd, ci]),
     "pskel_store_save": (ci, [VP, ctypes.c_char_p, cd]),
     "pskel_store_load": (ci, [VP, ctypes.c_char_p, I32]),
+    "pskel_aca_compress": (ci, [VP, cd, ci, I32, I32]),
+    "pskel_aca_get_block": (ci, [VP, ci, VP, VP, I32, I32]),
+    "pskel_aca_true_errors": (ci, [VP, D]),
     "pskel_near_build": (ci, [VP, I32, I32, ci, cd, cd, cd, ci, ctypes.POINTER(ctypes.c_longlong)]),
     "pskel_near_matvec": (ci, [VP, VP, ci, VP, ci, ci, ci, VP]),
     "pskel_plane_wave": (ci, [VP, cd, cd, cd, VP, VP]),

@@ -256,6 +256,35 @@ class Engine:
                                                 ctypes.c_void_p(s)))
         return Y.t()
 
+    def aca_compress(self, tol: float, kmax: int = 128) -> dict:
+        """Adaptive cross approximation of every far block (see pskel_aca_compress); returns
+        ranks, statuses and the kernel time in ms."""
+        nb = self.n_blocks
+        k = np.zeros(nb, dtype=np.int32)
+        st = np.zeros(nb, dtype=np.int32)
+        _lib.check(self._lib.pskel_aca_compress(self._h, float(tol), int(kmax),
+                                                k.ctypes.data_as(_lib.I32), st.ctypes.data_as(_lib.I32)))
+        self._aca_k = k
+        return dict(k=k, status=st)
+
+    def aca_get_block(self, b: int):
+        """(U, V, I, J) of ACA block b: Z(rows, cols) ~ U V, pivots local to the block."""
+        rows, cols = self.block_ids(b)
+        k = int(self._aca_k[b])
+        U = np.zeros((len(rows), k), dtype=np.complex128, order="F")
+        V = np.zeros((k, len(cols)), dtype=np.complex128, order="F")
+        I = np.zeros(max(k, 1), dtype=np.int32)
+        J = np.zeros(max(k, 1), dtype=np.int32)
+        vp = lambda x: ctypes.c_void_p(x.ctypes.data)
+        _lib.check(self._lib.pskel_aca_get_block(self._h, int(b), vp(U), vp(V), I.ctypes.data_as(_lib.I32),
+                                                 J.ctypes.data_as(_lib.I32)))
+        return U, V, I[:k], J[:k]
+
+    def aca_true_errors(self) -> np.ndarray:
+        err = np.zeros(self.n_blocks)
+        _lib.check(self._lib.pskel_aca_true_errors(self._h, err.ctypes.data_as(_lib.D)))
+        return err
+
     def save_store(self, path: str, thresh: float = 0.0):
         """Write the recompressed far field (after recompress()) to a store file."""
         _lib.check(self._lib.pskel_store_save(self._h, str(path).encode(), float(thresh)))

@@ -314,6 +314,27 @@ int pskel_store_save(pskel_ctx *ctx, const char *path, double thresh);
    the block count. */
 int pskel_store_load(pskel_ctx *ctx, const char *path, int *n_blocks);
 
+/* Adaptive cross approximation of every far block of the block list (the comparison method of
+   the reference's ACA-vs-CUR study: ACA_julia.jl:2-112, c_ACA.c:327-558), one CTA per block on
+   the device, entries computed on demand in complex FP64 with the 7-point rule (the mesh must be
+   uploaded with q = 7). Same steps as the reference: first row first, column pivot = largest
+   unused entry of the row residual, row pivot = largest unused entry of the column residual,
+   stop when ||U_k|| ||V_k|| <= tol ||U V||_F (from the second step), on a zero pivot or at full
+   rank; kmax caps the rank (status 1 when it stops a block). In the symmetric mode one block of
+   each (t, s) / (s, t) pair is approximated and the other is its transpose. ranks / status
+   (host, n_blocks, may be NULL): rank k and 0 (converged or full rank), 1 (kmax reached) or 2
+   (zero pivot). */
+int pskel_aca_compress(pskel_ctx *ctx, double tol, int kmax, int *ranks, int *status);
+
+/* Factors of block b after pskel_aca_compress: U (m x k, column-major), V (k x n, column-major),
+   Z(rows, cols) ~ U V, and the pivot rows I / columns J (k each, 0-based within the block);
+   any may be NULL. */
+int pskel_aca_get_block(pskel_ctx *ctx, int b, pskel_c128 *U, pskel_c128 *V, int *I, int *J);
+
+/* Relative Frobenius error of every ACA block against its dense complex-FP64 fill; err (host,
+   n_blocks). */
+int pskel_aca_true_errors(pskel_ctx *ctx, double *err);
+
 /* Near-field blocks for the H-matrix product: the n_near group pairs (nt[b], ns[b]) of the
    groups set by pskel_set_blocks (normally every pair that is not far, diagonal included) are
    filled densely (complex FP64) with the near-field rule of pskel_fill_near_device and kept on
