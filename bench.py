@@ -336,6 +336,7 @@ def run_ours(args, rank, world, dev):
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     blockops = run_blockops(eng, st, m, flush)
     octree_t = run_octree(args, m, part, dev) if rank == 0 else None
+    aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only) else None
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
                                    fill_choice=tune["choice"])
@@ -399,6 +400,7 @@ def run_ours(args, rank, world, dev):
         clocks=clocks, gpu_launches=int(launches),
         blockops=blockops,
         octree=octree_t,
+        aca=aca_t,
     )
     eng.close()
     return out
@@ -531,6 +533,32 @@ def run_octree(args, m, part, dev, reps=5):
                 host_ms=round(1e3 * float(np.median(th)), 3),
                 desc="Morton keys, CUB radix sort, key runs, far test on the device; small-group "
                      "merge on the host; host = numpy restatement (pskel/octree.py)")
+
+
+def run_aca(m, part, dev, reps=3):
+    """The comparison compressor: batched device ACA (the reference's ACA_julia steps and
+    stopping rule, complex FP64, 7-point entries on demand) on the same blocks and tolerance,
+    symmetric mode, with every block's error against its dense FP64 fill."""
+    import torch
+
+    from pskel.engine import Engine
+    with Engine(dev) as eng:
+        eng.upload_mesh(m, K_WAVE, ETA, q=7)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        eng.aca_compress(TOL)
+        ts = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            out = eng.aca_compress(TOL)
+            ts.append(time.perf_counter() - t0)
+        err = eng.aca_true_errors()
+    return dict(ms=round(1e3 * float(np.median(ts)), 3), rank_mean=float(out["k"].mean()),
+                rank_max=int(out["k"].max()), err_max=float(err.max()),
+                err_median=float(np.median(err)), blocks_over_tol=int((err > TOL).sum()),
+                desc="partially pivoted ACA (ACA_julia.jl steps and stopping rule), complex FP64, "
+                     "one CTA per block, symmetric mode; wall time of the call")
 
 
 def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None):
