@@ -99,6 +99,166 @@ __global__ void __launch_bounds__(256) matvec_kernel(const MatvecBlock *__restri
     }
 }
 
+// The same product organised by test group: one CTA per chunk of up to kMvChunk blocks that share
+// their test group. Per block, T1 = R X(cols) has the block's X rows staged in shared memory and
+// the k range split over the 8 warps (lane = row of R, JB right-hand sides in registers, broadcast
+// reads of X), partial sums reduced through shared memory; T2 = U T1; the test-group accumulator
+// (m x nrhs, each entry owned by one thread) gains C T2 with JB right-hand sides per thread in
+// registers; it is added to Y once per chunk. Register blocking over the right-hand sides reads
+// every factor entry once per JB products instead of once per product, and the chunk divides
+// the global atomics by its length.
+constexpr int kMvChunk = 8;
+constexpr int kMvWarps = 8;
+
+struct MatvecChunk {
+    int first, count;  // blocks [first, first + count) of the group-ordered table
+    const int *rows;   // the chunk's test group
+    int m;
+};
+
+template <typename A, typename S, int JB>
+__global__ void __launch_bounds__(256) matvec_group_kernel(const MatvecBlock *__restrict__ blocks,
+                                                           const MatvecChunk *__restrict__ chunks,
+                                                           const typename CT<A>::c *__restrict__ X, int ldx,
+                                                           A *__restrict__ Y, int ldy, int nrhs, int max_r,
+                                                           int max_n) {
+    using C2 = typename CT<A>::c;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const MatvecChunk ch = chunks[blockIdx.x];
+    C2 *acc = reinterpret_cast<C2 *>(smem_raw);  // m x nrhs
+    C2 *t1 = acc + (size_t)ch.m * nrhs;          // r x nrhs
+    C2 *t2 = t1 + (size_t)max_r * nrhs;          // r x nrhs
+    C2 *xs = t2 + (size_t)max_r * nrhs;          // n x JB
+    C2 *part = xs + (size_t)max_n * JB;          // warps x 32 (JB = 1 only)
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int e = threadIdx.x; e < ch.m * nrhs; e += blockDim.x) acc[e] = mk<A>(0.0, 0.0);
+    for (int bi = 0; bi < ch.count; ++bi) {
+        const MatvecBlock w = blocks[ch.first + bi];
+        const S *R = reinterpret_cast<const S *>(w.R);
+        const S *Cm = reinterpret_cast<const S *>(w.C);
+        const int k0 = (w.n * wid) / kMvWarps, k1 = (w.n * (wid + 1)) / kMvWarps;
+        // T1 = R X(cols)
+        if (JB == 1) {
+            // one right-hand side at a time: the k range split over the warps, partial sums
+            // reduced through shared memory
+            for (int j0 = 0; j0 < nrhs; ++j0) {
+                __syncthreads();  // xs and part are free
+                for (int k = threadIdx.x; k < w.n; k += blockDim.x) xs[k] = X[w.cols[k] + (size_t)j0 * ldx];
+                __syncthreads();
+                for (int ib = 0; ib < w.r; ib += 32) {
+                    const int i = ib + lane;
+                    A ar = 0, ai = 0;
+                    if (i < w.r)
+                        for (int k = k0; k < k1; ++k) {
+                            const double2 rv = r_op(w, R, Cm, i, k);
+                            const C2 x = xs[k];
+                            ar += (A)rv.x * x.x - (A)rv.y * x.y;
+                            ai += (A)rv.x * x.y + (A)rv.y * x.x;
+                        }
+                    part[wid * 32 + lane] = mk<A>(ar, ai);
+                    __syncthreads();
+                    if (threadIdx.x < 32 && ib + threadIdx.x < w.r) {
+                        A sr = 0, si = 0;
+                        for (int q = 0; q < kMvWarps; ++q) {
+                            const C2 v = part[q * 32 + threadIdx.x];
+                            sr += v.x;
+                            si += v.y;
+                        }
+                        t1[(ib + threadIdx.x) + j0 * w.r] = mk<A>(sr, si);
+                    }
+                    __syncthreads();
+                }
+            }
+        } else {
+            // several right-hand sides: X(cols, :) staged once, each warp takes JB / kMvWarps of
+            // them over the whole k range (lane = row of R); no cross-warp reduction
+            constexpr int RPW = JB / kMvWarps > 0 ? JB / kMvWarps : 1;
+            for (int j0 = 0; j0 < nrhs; j0 += JB) {
+                __syncthreads();  // xs is free
+                for (int e = threadIdx.x; e < w.n * JB; e += blockDim.x) {
+                    const int jj = e / w.n, k = e - jj * w.n;  // xs[jj][k]: one row of X per jj
+                    xs[e] = j0 + jj < nrhs ? X[w.cols[k] + (size_t)(j0 + jj) * ldx] : mk<A>(0.0, 0.0);
+                }
+                __syncthreads();
+                for (int g = wid; g * RPW < JB; g += kMvWarps) {
+                    for (int ib = 0; ib < w.r; ib += 32) {
+                        const int i = ib + lane;
+                        if (i >= w.r) continue;
+                        A ar[RPW], ai[RPW];
+#pragma unroll
+                        for (int q = 0; q < RPW; ++q) ar[q] = ai[q] = 0;
+                        for (int k = 0; k < w.n; ++k) {
+                            const double2 rv = r_op(w, R, Cm, i, k);
+                            const A rx = (A)rv.x, ry = (A)rv.y;
+#pragma unroll
+                            for (int q = 0; q < RPW; ++q) {
+                                const C2 x = xs[(g * RPW + q) * w.n + k];
+                                ar[q] += rx * x.x - ry * x.y;
+                                ai[q] += rx * x.y + ry * x.x;
+                            }
+                        }
+#pragma unroll
+                        for (int q = 0; q < RPW; ++q) {
+                            const int j = j0 + g * RPW + q;
+                            if (j < nrhs) t1[i + j * w.r] = mk<A>(ar[q], ai[q]);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // T2 = U T1
+        for (int e = threadIdx.x; e < w.r * nrhs; e += blockDim.x) {
+            const int i = e % w.r, j = e / w.r;
+            A sr = 0, si = 0;
+            for (int k = 0; k < w.r; ++k) {
+                const double2 u = w.trans ? w.U[k + (size_t)i * w.r] : w.U[i + (size_t)k * w.r];
+                const C2 t = t1[k + j * w.r];
+                sr += (A)u.x * t.x - (A)u.y * t.y;
+                si += (A)u.x * t.y + (A)u.y * t.x;
+            }
+            t2[e] = mk<A>(sr, si);
+        }
+        __syncthreads();
+        // acc += C T2
+        for (int i = threadIdx.x; i < ch.m; i += blockDim.x) {
+            for (int j0 = 0; j0 < nrhs; j0 += JB) {
+                A ar[JB], ai[JB];
+#pragma unroll
+                for (int jj = 0; jj < JB; ++jj) ar[jj] = ai[jj] = 0;
+                for (int k = 0; k < w.r; ++k) {
+                    const double2 cv = c_op(w, R, Cm, i, k);
+                    const A cx = (A)cv.x, cy = (A)cv.y;
+#pragma unroll
+                    for (int jj = 0; jj < JB; ++jj) {
+                        if (j0 + jj < nrhs) {
+                            const C2 t = t2[k + (j0 + jj) * w.r];
+                            ar[jj] += cx * t.x - cy * t.y;
+                            ai[jj] += cx * t.y + cy * t.x;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int jj = 0; jj < JB; ++jj) {
+                    if (j0 + jj < nrhs) {
+                        C2 a = acc[i + (size_t)(j0 + jj) * ch.m];
+                        a.x += ar[jj];
+                        a.y += ai[jj];
+                        acc[i + (size_t)(j0 + jj) * ch.m] = a;
+                    }
+                }
+            }
+        }
+        __syncthreads();  // t1 / t2 are reused by the next block
+    }
+    for (int e = threadIdx.x; e < ch.m * nrhs; e += blockDim.x) {
+        const int i = e % ch.m, j = e / ch.m;
+        A *y = Y + 2 * (ch.rows[i] + (size_t)j * ldy);
+        atomicAdd(y, acc[e].x);
+        atomicAdd(y + 1, acc[e].y);
+    }
+}
+
 }  // namespace pskel
 
 using namespace pskel;
@@ -118,10 +278,15 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
     cudaStream_t st = static_cast<cudaStream_t>(stream);  // NULL: legacy default stream
     const int nb = c->n_blocks;
     if (c->mv_generation != c->generation) {
-        // block table: built once per compression, uploaded synchronously
+        // block table in test-group order and its chunks: built once per compression
+        std::vector<int> order(nb);
+        for (int b = 0; b < nb; ++b) order[b] = b;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return c->gt[a] < c->gt[b]; });
         std::vector<MatvecBlock> hb(nb);
-        int max_r = 0;
-        for (int b = 0; b < nb; ++b) {
+        std::vector<MatvecChunk> hc;
+        int max_r = 0, max_m = 0, max_n = 0;
+        for (int pos = 0; pos < nb; ++pos) {
+            const int b = order[pos];
             const BlockResult &res = c->results[b];
             if (res.arena < 0) {
                 set_error(PSKEL_ERR_STATE, "matvec: block %d has no retained factors", b);
@@ -129,17 +294,28 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
             }
             const BlockResult &pr = res.mirror >= 0 ? c->results[res.mirror] : res;
             const char *base = c->arenas[pr.arena].keep.as<char>();
-            hb[b] = MatvecBlock{c->d_gids.as<int>() + c->gptr[c->gt[b]],
-                                c->d_gids.as<int>() + c->gptr[c->gs[b]], base + pr.offC,
-                                base + pr.offRx, reinterpret_cast<const double2 *>(base + pr.offU),
-                                res.m, res.n, res.r, pr.r + pr.pe, pr.m, res.mirror >= 0 ? 1 : 0};
+            const int *rows = c->d_gids.as<int>() + c->gptr[c->gt[b]];
+            hb[pos] = MatvecBlock{rows, c->d_gids.as<int>() + c->gptr[c->gs[b]], base + pr.offC,
+                                  base + pr.offRx, reinterpret_cast<const double2 *>(base + pr.offU),
+                                  res.m, res.n, res.r, pr.r + pr.pe, pr.m, res.mirror >= 0 ? 1 : 0};
             max_r = std::max(max_r, res.r);
+            max_m = std::max(max_m, res.m);
+            max_n = std::max(max_n, res.n);
+            if (hc.empty() || c->gt[order[hc.back().first]] != c->gt[b] || hc.back().count == kMvChunk)
+                hc.push_back(MatvecChunk{pos, 0, rows, res.m});
+            ++hc.back().count;
         }
-        PSKEL_TRY(c->mv_table.reserve(sizeof(MatvecBlock) * nb + 256));
+        const size_t tb = (sizeof(MatvecBlock) * nb + 255) & ~size_t(255);
+        PSKEL_TRY(c->mv_table.reserve(tb + sizeof(MatvecChunk) * hc.size() + 256));
         PSKEL_CUDA(cudaStreamSynchronize(c->stream));
-        PSKEL_CUDA(cudaMemcpy(c->mv_table.ptr, hb.data(), sizeof(MatvecBlock) * nb,
+        PSKEL_CUDA(cudaMemcpy(c->mv_table.ptr, hb.data(), sizeof(MatvecBlock) * nb, cudaMemcpyHostToDevice));
+        PSKEL_CUDA(cudaMemcpy(c->mv_table.as<char>() + tb, hc.data(), sizeof(MatvecChunk) * hc.size(),
                               cudaMemcpyHostToDevice));
         c->mv_max_r = max_r;
+        c->mv_max_m = max_m;
+        c->mv_max_n = max_n;
+        c->mv_chunks = (int)hc.size();
+        c->mv_chunk_off = tb;
         c->mv_generation = c->generation;
     }
     const size_t es = precision == PSKEL_C64 ? sizeof(float2) : sizeof(double2);
@@ -152,13 +328,33 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
     const bool f32 = c->precision == PSKEL_C64;  // storage of the factors
     const int grid = std::min(nb, sm_count() * 8);
     const MatvecBlock *d_b = c->mv_table.as<MatvecBlock>();
+    const MatvecChunk *d_c = reinterpret_cast<const MatvecChunk *>(c->mv_table.as<char>() + c->mv_chunk_off);
+    // grouped version when the test group's accumulator and staging fit in shared memory; JB
+    // right-hand sides per thread
+    int jb = nrhs >= 16 ? 16 : (nrhs >= 8 ? 8 : 1);
+    auto gsz = [&](int j) {
+        return smem + es * ((size_t)c->mv_max_m * nrhs + (size_t)c->mv_max_n * j + (size_t)kMvWarps * 32);
+    };
+    while (jb > 1 && gsz(jb) > 200 * 1024) jb = jb == 16 ? 8 : 1;
+    const size_t gsmem = gsz(jb);
+    const bool grouped = gsmem <= 200 * 1024;
 #define PSKEL_MV(A, S)                                                                         \
     do {                                                                                       \
-        auto k = matvec_kernel<A, S>;                                                          \
-        PSKEL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,       \
-                                        200 * 1024));                                          \
-        k<<<grid, 256, smem, st>>>(d_b, nb, reinterpret_cast<const CT<A>::c *>(X), ldx, \
-                                          reinterpret_cast<A *>(Y), ldy, nrhs);               \
+        if (grouped) {                                                                         \
+            auto k = jb == 16 ? matvec_group_kernel<A, S, 16>                                  \
+                              : (jb == 8 ? matvec_group_kernel<A, S, 8> : matvec_group_kernel<A, S, 1>); \
+            PSKEL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                            200 * 1024));                                      \
+            k<<<c->mv_chunks, 256, gsmem, st>>>(d_b, d_c, reinterpret_cast<const CT<A>::c *>(X), \
+                                                ldx, reinterpret_cast<A *>(Y), ldy, nrhs,     \
+                                                c->mv_max_r, c->mv_max_n);                     \
+        } else {                                                                               \
+            auto k = matvec_kernel<A, S>;                                                      \
+            PSKEL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                            200 * 1024));                                      \
+            k<<<grid, 256, smem, st>>>(d_b, nb, reinterpret_cast<const CT<A>::c *>(X), ldx,   \
+                                       reinterpret_cast<A *>(Y), ldy, nrhs);                   \
+        }                                                                                      \
         PSKEL_LAUNCHED(1);                                                                     \
     } while (0)
     if (precision == PSKEL_C64) {

@@ -135,7 +135,8 @@ struct pskel_ctx {
     long long generation = 0;               // incremented by every compression
     DevBuf mv_table;                        // matvec block table (built once per compression)
     long long mv_generation = -1;
-    int mv_max_r = 0;
+    int mv_max_r = 0, mv_max_m = 0, mv_max_n = 0, mv_chunks = 0;  // largest rank / groups, chunks
+    size_t mv_chunk_off = 0;                        // byte offset of the chunk table in mv_table
     StoreLayout store;                      // compressed store (bf16 hi/lo planes, tiled)
     DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
     pskel::OctreeState octree;              // device octree partition (pskel_octree_build)
