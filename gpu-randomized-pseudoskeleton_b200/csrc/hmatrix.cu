@@ -150,8 +150,35 @@ extern "C" int pskel_near_build(pskel_ctx *c, const int *nt, const int *ns, int 
     r.rinteg_f = rinteg_f;
     r.q_far = q_far;
     PSKEL_CUDA(cudaMemsetAsync(c->flags.ptr, 0, sizeof(int), c->stream));
+    // most near-block entries have every triangle pair outside the radii: fill all with the batched
+    // far kernel of the same outside rule, then recompute only the entries with a pair inside a
+    // radius or a same-triangle pair with the near kernel
+    if (n_near > 0) {
+        if (!c->mesh.records(q_far).f64.ptr) PSKEL_TRY(build_records(c->mesh, q_far, c->stream, c->flags.as<int>()));
+        int tm, tn;
+        fill_tile_shape(PSKEL_C128, q_far, 0, &tm, &tn);
+        std::vector<int> prefix(n_near + 1, 0);
+        for (int b = 0; b < n_near; ++b)
+            prefix[b + 1] = prefix[b] + ((tab[b].m + tm - 1) / tm) * ((tab[b].n + tn - 1) / tn);
+        const size_t jb = (sizeof(FillJob) * n_near + 255) & ~size_t(255);
+        PSKEL_TRY(c->tmp2.reserve(jb + sizeof(int) * prefix.size() + 256));
+        FillJob *d_jobs = c->tmp2.as<FillJob>();
+        int *d_prefix = reinterpret_cast<int *>(c->tmp2.as<char>() + jb);
+        PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(FillJob) * n_near, cudaMemcpyHostToDevice, c->stream));
+        PSKEL_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice,
+                                   c->stream));
+        FillParams fp;
+        fp.k = c->em.k;
+        fp.eta = c->em.eta;
+        fp.r_near = 0;
+        fp.q_test = fp.q_src = q_far;
+        fp.precision = PSKEL_C128;
+        fp.split = 0;
+        PSKEL_TRY(launch_fill(c->mesh, fp, d_jobs, d_prefix, n_near, prefix.back(), c->flags.as<int>(), c->stream));
+        PSKEL_CUDA(cudaStreamSynchronize(c->stream));  // the host job table goes out of scope below
+    }
     PSKEL_TRY(near_fill_jobs(c->mesh, r, c->em.k, c->em.eta, jobs, c->near_jobs, c->near_mom,
-                             c->flags.as<int>(), c->stream, true));
+                             c->flags.as<int>(), c->stream, true, true));
     int h = 0;
     PSKEL_CUDA(cudaMemcpyAsync(&h, c->flags.ptr, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));

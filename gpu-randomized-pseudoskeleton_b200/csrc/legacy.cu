@@ -121,7 +121,7 @@ int fill_jobs(LegacyCtx &c, const std::vector<FillJob> &jobs, double k, double e
     if (!(h & 1) || (h & 6)) return PSKEL_OK;  // far only, or a range error (check_flags)
     PSKEL_CUDA(cudaMemsetAsync(c.flags.ptr, 0, sizeof(int), c.stream));
     return near_fill_jobs(c.mesh, radii, k, eta, jobs, c.near_jobs, c.near_mom, c.flags.as<int>(),
-                          c.stream, false);
+                          c.stream, false, false);
 }
 
 // Read the flag word after the stream drains; maps bits to statuses.

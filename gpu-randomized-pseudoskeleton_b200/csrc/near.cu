@@ -309,30 +309,42 @@ self_moments_kernel(const double *__restrict__ vertex, const double *__restrict_
 struct NearArgs {
     double k, eta, rs, ra, rf;
     int q_far;
+    int patch;  // 1: only entries with a triangle pair inside a radius or a same-triangle pair
 };
 
-// Points of one side: the 4-point rule (four = true), else the centroid or the 7-point rule.
-__device__ __forceinline__ int side_points(bool four, int q_far, const double (*V)[3],
-                                           const double *cen, double (*P)[3], double *w) {
-    if (four) {
-        for (int p = 0; p < 4; ++p) {
-            for (int d = 0; d < 3; ++d)
-                P[p][d] = c_rule4[4 * p] * V[0][d] + c_rule4[4 * p + 1] * V[1][d] + c_rule4[4 * p + 2] * V[2][d];
-            w[p] = c_rule4[4 * p + 3];
+// Does entry (m, n) have a same-triangle pair or a pair with centroid distance below a radius?
+__device__ __forceinline__ bool entry_is_near(int m, int n, const double *__restrict__ edges,
+                                              const double *__restrict__ cent, int nt, double rmax) {
+    for (int a = 0; a < 2; ++a) {
+        const double tad = edges[4 * (size_t)m + a];
+        if (!(tad >= 1.0 && tad <= (double)nt)) return true;  // let the full path report it
+        const double *ca = cent + 3 * ((size_t)tad - 1);
+        for (int b = 0; b < 2; ++b) {
+            const double tbd = edges[4 * (size_t)n + b];
+            if (!(tbd >= 1.0 && tbd <= (double)nt) || tad == tbd) return true;
+            const double *cb = cent + 3 * ((size_t)tbd - 1);
+            const double dcv[3] = {ca[0] - cb[0], ca[1] - cb[1], ca[2] - cb[2]};
+            if (sqrt(dot3(dcv, dcv)) < rmax) return true;  // as near_entry computes dc
         }
-        return 4;
     }
-    if (q_far == 7) {
-        for (int p = 0; p < 7; ++p) {
-            for (int d = 0; d < 3; ++d)
-                P[p][d] = c_rule7[4 * p] * V[0][d] + c_rule7[4 * p + 1] * V[1][d] + c_rule7[4 * p + 2] * V[2][d];
-            w[p] = c_rule7[4 * p + 3];
-        }
-        return 7;
+    return false;
+}
+
+// Rule of one side: 0 = centroid, 1 = the 4-point rule, 2 = the 7-point rule. Points are formed
+// when used (no per-side point arrays: fewer registers, more resident warps).
+__device__ __forceinline__ int side_rule(bool four, int q_far) { return four ? 1 : (q_far == 7 ? 2 : 0); }
+__device__ __forceinline__ int rule_points(int rule) { return rule == 1 ? 4 : (rule == 2 ? 7 : 1); }
+__device__ __forceinline__ double rule_point(int rule, int p, const double (*V)[3], const double *cen,
+                                             double *x) {
+    if (rule == 0) {
+        x[0] = cen[0];
+        x[1] = cen[1];
+        x[2] = cen[2];
+        return 1.0;
     }
-    for (int d = 0; d < 3; ++d) P[0][d] = cen[d];
-    w[0] = 1.0;
-    return 1;
+    const double *b = rule == 1 ? c_rule4 + 4 * p : c_rule7 + 4 * p;
+    for (int d = 0; d < 3; ++d) x[d] = b[0] * V[0][d] + b[1] * V[1][d] + b[2] * V[2][d];
+    return b[3];
 }
 
 // One entry Z(m, n). Returns false on an out-of-range id inside the mesh arrays.
@@ -382,23 +394,24 @@ __device__ bool near_entry(int m, int n, const double *__restrict__ vertex,
             const double dc = sqrt(dot3(dcv, dcv));
             double VS[3][3];
             if (!load_tri(tb, vertex, topol, nv, VS)) return false;
-            double Pt[7][3], wt[7], Ps[7][3], ws[7];
-            const int ntp = side_points(dc < a.rf, a.q_far, VT, ca, Pt, wt);
-            const int nsp = side_points(dc < a.rs, a.q_far, VS, cb, Ps, ws);
+            const int rt = side_rule(dc < a.rf, a.q_far), rsr = side_rule(dc < a.rs, a.q_far);
+            const int ntp = rule_points(rt), nsp = rule_points(rsr);
             const bool anal = dc < a.ra;
 #pragma unroll 1
             for (int p = 0; p < ntp; ++p) {
-                const double *x = Pt[p];
+                double x[3];
+                const double wtp = rule_point(rt, p, VT, ca, x);
                 const double rho_a[3] = {sa * (x[0] - va[0]), sa * (x[1] - va[1]), sa * (x[2] - va[2])};
                 double sgr = 0.0, sgi = 0.0, srr[3] = {0, 0, 0}, sri[3] = {0, 0, 0};
 #pragma unroll 1
                 for (int q = 0; q < nsp; ++q) {
-                    const double *y = Ps[q];
+                    double y[3];
+                    const double wsq = rule_point(rsr, q, VS, cb, y);
                     const double dd[3] = {x[0] - y[0], x[1] - y[1], x[2] - y[2]};
                     const double R = sqrt(dot3(dd, dd));
                     double s, c;
                     sincos(a.k * R, &s, &c);
-                    const double f = ws[q] * C / R;
+                    const double f = wsq * C / R;
                     const double gr = (c - (anal ? 1.0 : 0.0)) * f, gi = -s * f;
                     sgr += gr;
                     sgi += gi;
@@ -416,8 +429,8 @@ __device__ bool near_entry(int m, int n, const double *__restrict__ vertex,
                 }
                 const double dr = dot3(rho_a, srr), di = dot3(rho_a, sri);
                 // z += w_p (j cvec (rho_a . S_r) - j cdiv ss S_g)
-                zr += wt[p] * (-cvec * di + cdiv * ss * sgi);
-                zi += wt[p] * (cvec * dr - cdiv * ss * sgr);
+                zr += wtp * (-cvec * di + cdiv * ss * sgi);
+                zi += wtp * (cvec * dr - cdiv * ss * sgr);
             }
         }
     }
@@ -425,7 +438,7 @@ __device__ bool near_entry(int m, int n, const double *__restrict__ vertex,
     return true;
 }
 
-__global__ void __launch_bounds__(kNearThreads)
+__global__ void __launch_bounds__(kNearThreads, 2)
 near_fill_kernel(const double *__restrict__ vertex, const double *__restrict__ topol,
                  const double *__restrict__ edges, const double *__restrict__ ln,
                  const double *__restrict__ cent, int ne, int nt, int nv,
@@ -446,6 +459,7 @@ near_fill_kernel(const double *__restrict__ vertex, const double *__restrict__ t
         atomicOr(flags, 2);
         return;
     }
+    if (a.patch && !entry_is_near(m, n, edges, cent, nt, fmax(a.rs, fmax(a.ra, a.rf)))) return;
     double2 z;
     if (!near_entry(m, n, vertex, topol, edges, ln, cent, nt, nv, a, mom, &z)) {
         atomicOr(flags, 4);
@@ -459,7 +473,7 @@ near_fill_kernel(const double *__restrict__ vertex, const double *__restrict__ t
 
 int near_fill_jobs(const DevMesh &mesh, const NearRadii &r, double k, double eta,
                    const std::vector<FillJob> &jobs, DevBuf &scratch, DevBuf &mom, int *d_flags,
-                   cudaStream_t stream, bool all_triangles) {
+                   cudaStream_t stream, bool all_triangles, bool patch) {
     PSKEL_TRY(upload_rules());
     if (jobs.empty()) return PSKEL_OK;
     std::vector<long long> prefix(jobs.size() + 1, 0);
@@ -495,7 +509,7 @@ int near_fill_jobs(const DevMesh &mesh, const NearRadii &r, double k, double eta
             PSKEL_LAUNCHED(1);
         }
     }
-    NearArgs a{k, eta, r.rinteg_s, r.ranal_s, r.rinteg_f, r.q_far};
+    NearArgs a{k, eta, r.rinteg_s, r.ranal_s, r.rinteg_f, r.q_far, patch ? 1 : 0};
     near_fill_kernel<<<(unsigned)prefix.back(), kNearThreads, 0, stream>>>(
         mesh.vertex.as<double>(), mesh.topol.as<double>(), mesh.edges.as<double>(),
         mesh.ln.as<double>(), mesh.cent.as<double>(), mesh.ne, mesh.nt, mesh.nv, d_jobs, d_prefix,
@@ -533,5 +547,5 @@ extern "C" int pskel_fill_near_device(pskel_ctx *c, const int *rows_dev, int nr,
     r.q_far = q_far;
     std::vector<FillJob> jobs{FillJob{rows_dev, cols_dev, Z_dev, nr, nc, ld, 0}};
     return near_fill_jobs(c->mesh, r, c->em.k, c->em.eta, jobs, c->near_jobs, c->near_mom,
-                          c->flags.as<int>(), c->stream, false);
+                          c->flags.as<int>(), c->stream, false, false);
 }

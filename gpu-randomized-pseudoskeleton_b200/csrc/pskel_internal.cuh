@@ -138,10 +138,12 @@ struct NearRadii {
 };
 // Complex-FP64 fill of the jobs (host list) with the near-field rule, one thread per entry;
 // the same-triangle moments go to mom (8 double2 per triangle), for every triangle or only for
-// the triangles of the jobs' rows. flags bit 2 / 4: RWG / triangle id out of range.
+// the triangles of the jobs' rows. patch: only the entries with a same-triangle pair or a pair
+// inside a radius are written (the caller filled the rest with the far rule). flags bit 2 / 4:
+// RWG / triangle id out of range.
 int near_fill_jobs(const DevMesh &mesh, const NearRadii &r, double k, double eta,
                    const std::vector<FillJob> &jobs, DevBuf &scratch, DevBuf &mom, int *d_flags,
-                   cudaStream_t stream, bool all_triangles);
+                   cudaStream_t stream, bool all_triangles, bool patch);
 
 // Triangle-moment fill of Z(group, cols) for a group of RWG functions whose triangle list and
 // triangle -> (RWG, side) adjacency are known (see tri_fill_kernel in fill.cu).

@@ -2,6 +2,7 @@
 
     python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py PRECISION [CALLS] [SPLIT] [GEOM32]
     python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py store [CALLS]
+    python gpu-randomized-pseudoskeleton_b200/pskel/profile_case.py extras
 
 builds the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions, 0.5-lambda leaves), then
 makes CALLS (default 3) single-round compressions of every far block at a fixed sample count of
@@ -11,6 +12,9 @@ geometry), printing the fill time and point-pair
 rate of each call. Under a profiler the fill launch of call i is the i-th launch of the chosen fill kernel.
 The store form compresses the same sphere, recompresses it, builds the compressed store and runs
 CALLS tensor-core matvecs of 16 right-hand sides.
+The extras form runs, once each on the same sphere: the device octree partition, the batched ACA
+of every far block (tol 1e-4, symmetric mode), a 2,048 x 2,048 near-field fill (radii 0.15
+lambda) and one H-matrix product (CUR far blocks at tol 1e-4 + near blocks, one right-hand side).
 """
 from __future__ import annotations
 
@@ -51,7 +55,52 @@ def store_case(calls):
                   f"status {eng.store_status()}", flush=True)
 
 
+def extras_case():
+    """Octree, ACA, near-field fill and one H-matrix product on the 7,680-RWG sphere."""
+    import time
+
+    import torch
+
+    from pskel.solve import HMatrix
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        t0 = time.perf_counter()
+        p2 = eng.octree(0.5, origin=(0, 0, 0), min_group=30)
+        print(f"octree: {1e3 * (time.perf_counter() - t0):.3f} ms, {p2.n_groups} groups, "
+              f"{p2.n_blocks} far blocks", flush=True)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        t0 = time.perf_counter()
+        out = eng.aca_compress(1e-4)
+        print(f"aca: {1e3 * (time.perf_counter() - t0):.3f} ms, rank mean {out['k'].mean():.1f}",
+              flush=True)
+        c = m.basis_centres().T
+        patch = np.argsort(np.linalg.norm(c - c[0], axis=1), kind="stable")[:2048].astype(np.int32)
+        ids = torch.as_tensor(patch, device="cuda")
+        Z = torch.empty((2048, 2048), dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.fill_near_device(ids.data_ptr(), 2048, ids.data_ptr(), 2048, Z.data_ptr(), 2048,
+                             0.15, 0.15, 0.15, q_far=1)
+        torch.cuda.synchronize()
+        print(f"near fill 2048 x 2048: {1e3 * (time.perf_counter() - t0):.3f} ms", flush=True)
+        eng.compress(1e-4, precision="c128", tau=1e-10, seed=0)
+        H = HMatrix(eng, part, (0.15, 0.15, 0.15), q_far=7)
+        X = torch.randn(m.N, dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H.matvec(X)
+        torch.cuda.synchronize()
+        print(f"H-matrix product: {1e3 * (time.perf_counter() - t0):.3f} ms, near blocks "
+              f"{H.near_bytes / 1e6:.0f} MB", flush=True)
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "extras":
+        extras_case()
+        return
     if len(sys.argv) > 1 and sys.argv[1] == "store":
         store_case(int(sys.argv[2]) if len(sys.argv) > 2 else 3)
         return
