@@ -315,6 +315,12 @@ def run_ours(args, rank, world, dev):
     learned_ms, _, _, _ = timed(learned_only, 1, 2)
     lm_nosym = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True, **PRODUCT))
     lm_nosym_ms, _, _, _ = timed(lm_nosym, 1, 2)
+    # learned + batched + symmetric in complex FP64: the same-precision counterpart of the ACA
+    # comparison (which computes in complex FP64)
+    def learned_sym_c128():
+        eng.set_symmetric(True)
+        return eng.compress(TOL, r0=predict_r0(), use_graph=True, **dict(PRODUCT, precision="c128"))
+    lsym128_ms, _, _, _ = timed(learned_sym_c128, 1, 2)
     # per-phase timing of the product without the graph (roofline of the fill)
     eng.set_symmetric(True)
     r0 = predict_r0()
@@ -365,7 +371,8 @@ def run_ours(args, rank, world, dev):
         ablation_ms=dict(plain_batched=round(plain_b_ms, 3), mixed_batched=round(mixed_ms, 3),
                          learned_batched=round(learned_ms, 3),
                          learned_mixed_batched=round(lm_nosym_ms, 3),
-                         learned_mixed_batched_symmetric=round(ms, 3)),
+                         learned_mixed_batched_symmetric=round(ms, 3),
+                         learned_batched_symmetric_c128=round(lsym128_ms, 3)),
         speedup_vs_plain_batched=round(plain_b_ms / ms, 3),
         step_times_ms=[round(t, 3) for t in times],
         phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},

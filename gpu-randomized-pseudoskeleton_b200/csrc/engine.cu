@@ -741,13 +741,30 @@ extern "C" int pskel_set_blocks(pskel_ctx *c, const int *group_ptr, const int *g
     c->gs.assign(gs, gs + n_blocks);
     c->n_groups = n_groups;
     c->n_blocks = n_blocks;
-    {  // the block with swapped groups, for the symmetric mode
-        std::map<std::pair<int, int>, int> where;
-        for (int b = 0; b < n_blocks; ++b) where[{gt[b], gs[b]}] = b;
+    {  // the block with swapped groups, for the symmetric mode (the last block listed for a pair)
         c->partner.assign(n_blocks, -1);
-        for (int b = 0; b < n_blocks; ++b) {
-            auto it = where.find({gs[b], gt[b]});
-            if (it != where.end() && it->second != b) c->partner[b] = it->second;
+        const long long G = n_groups;
+        if (G * G <= (1LL << 24)) {  // dense group-pair table
+            std::vector<int> where((size_t)(G * G), -1);
+            for (int b = 0; b < n_blocks; ++b) where[(size_t)(gt[b] * G + gs[b])] = b;
+            for (int b = 0; b < n_blocks; ++b) {
+                const int p = where[(size_t)(gs[b] * G + gt[b])];
+                if (p >= 0 && p != b) c->partner[b] = p;
+            }
+        } else {  // sorted keys
+            std::vector<std::pair<long long, int>> keys(n_blocks);
+            for (int b = 0; b < n_blocks; ++b) keys[b] = {gt[b] * G + gs[b], b};
+            std::stable_sort(keys.begin(), keys.end(),
+                             [](const std::pair<long long, int> &a, const std::pair<long long, int> &b) {
+                                 return a.first < b.first;
+                             });
+            for (int b = 0; b < n_blocks; ++b) {
+                const long long want = gs[b] * G + gt[b];
+                auto it = std::upper_bound(keys.begin(), keys.end(), want,
+                                           [](long long v, const std::pair<long long, int> &e) { return v < e.first; });
+                if (it != keys.begin() && (it - 1)->first == want && (it - 1)->second != b)
+                    c->partner[b] = (it - 1)->second;
+            }
         }
     }
     PSKEL_TRY(c->d_gids.reserve(sizeof(int) * nids));
