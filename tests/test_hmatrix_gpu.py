@@ -86,3 +86,4 @@ def test_gmres_solution_matches_dense_solve(setup):
     xd = torch.linalg.solve(-Z, E)
     rel = float(torch.linalg.norm(x - xd) / torch.linalg.norm(xd))
     assert rel < 1e-4, (rel, nmv)
+
