@@ -19,7 +19,6 @@
 // pair is approximated; the other is its transpose (U_b = V_p^T, V_b = U_p^T).
 #include <algorithm>
 #include <cmath>
-#include <map>
 #include <vector>
 
 #include "engine_internal.cuh"

@@ -18,7 +18,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <map>
 #include <numeric>
 
 #include "pskel_internal.cuh"
