@@ -246,6 +246,10 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
         set_error(PSKEL_ERR_ARG, "store_load: %s is truncated or corrupt (hash mismatch)", path);
         return PSKEL_ERR_ARG;
     }
+    if (std::fgetc(r.f) != EOF) {
+        set_error(PSKEL_ERR_ARG, "store_load: %s has bytes after its hash", path);
+        return PSKEL_ERR_ARG;
+    }
     PSKEL_TRY(pskel_set_blocks(c, gptr.data(), gids.data(), G, gt.data(), gs.data(), B));
     PSKEL_TRY(c->recomp.reserve(total + 256));
     if (total > 0) PSKEL_CUDA(cudaMemcpy(c->recomp.ptr, data.data(), total, cudaMemcpyHostToDevice));

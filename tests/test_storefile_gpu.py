@@ -85,7 +85,7 @@ def test_bad_files_refused(saved, tmp_path):
     flipped[len(raw) // 2] ^= 0x10
     with Engine() as eng:
         eng.upload_mesh(m, K, ETA, q=7)
-        for data in (bytes(flipped), raw[:-100]):
+        for data in (bytes(flipped), raw[:-100], raw + b"\0"):
             bad.write_bytes(data)
             with pytest.raises(_lib.PskelError):
                 eng.load_store(bad)
