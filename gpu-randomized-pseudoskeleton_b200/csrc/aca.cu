@@ -10,7 +10,7 @@
 //   + ||U_k||^2 ||V_k||^2, stop when ||U_k|| ||V_k|| <= tol ||U V||_F (from the second step),
 //   next row = argmax over unused rows of |R_j|.
 //
-// Device design: one CTA (128 threads) per block runs the whole loop; the block's row and column
+// Device design: one CTA (128 threads, 64 registers: 8 CTAs per SM) per block runs the whole loop; the block's row and column
 // residuals, used-index marks and the pivot RWG's quadrature record live in shared memory; U
 // (m x kmax, column-major) and V (kmax x n, row-major) in a per-call global buffer. Every entry
 // is computed in FP64 from the 7-point quadrature records: the pivot RWG's record is staged in
@@ -110,7 +110,7 @@ __device__ double block_sum(double v, double *sv) {
     return s;
 }
 
-__global__ void __launch_bounds__(kAcaThreads)
+__global__ void __launch_bounds__(kAcaThreads, 8)
 aca_kernel(const AcaJob *__restrict__ jobs, const double *__restrict__ rec, int stride, double k,
            double scale, double tol) {
     extern __shared__ __align__(16) unsigned char smem[];
