@@ -24,6 +24,7 @@ import multiprocessing as mp
 import os
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -131,8 +132,8 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                                 f".clocks_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="pskel_clocks_", suffix=".csv")
+        os.close(fd)
 
     def __enter__(self):
         try:
@@ -626,6 +627,113 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
     return float(t.item()), h2d, d2h
 
 
+# ----------------------------------------------------------------------------- profiling cases
+# Small, repeatable workloads on the 7,680-RWG sphere (icosphere R = 2 lambda, 4 subdivisions,
+# 0.5-lambda leaves) that the kernel profiles in profiles/ are captured from:
+#   python bench.py --profile-case fill --precision c64 --calls 2 --split 8 --geom32 1
+#   python bench.py --profile-case store --calls 5
+#   python bench.py --profile-case extras
+def fill_case(prec, calls, split, geom32):
+    """CALLS single-round compressions of every far block of the 7,680-RWG sphere at a fixed
+    sample count of 24 with the given precision (c128 or c64) and fill variant (8: triangle
+    moments, the default; 0: two rows per thread; 1, 2, 4: lanes per entry; geom32 = 1:
+    complex-FP32 fill with FP32 pair geometry), printing the fill time and point-pair rate of
+    each call. Under a profiler the fill launch of call i is the i-th launch of the fill kernel."""
+    from pskel import mesh as pmesh
+    from pskel import octree
+    from pskel.engine import Engine
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        if prec == "c128":
+            eng.set_fill_split(split_c128=split)
+        else:
+            eng.set_fill_split(split_c64=split)
+            eng.set_fill_geometry(bool(geom32))
+        for i in range(calls):
+            eng.compress(1.0, precision=prec, r0=np.full(part.n_blocks, 24), oversample=0,
+                         max_rounds=1, seed=i)
+            t = eng.timing()
+            print(f"{prec} split {split} call {i}: fill {t['fill']:.3f} ms, "
+                  f"{t['point_pairs'] / t['fill'] / 1e6:.1f} G point pairs/s, pinv "
+                  f"{t['pinv']:.3f} ms, Jacobi sweeps mean {t['sweeps_mean']:.2f} "
+                  f"max {t['sweeps_max']:.0f}", flush=True)
+
+
+def store_case(calls):
+    """Compress the same sphere at tol 1e-4 (c64), recompress to 1e-4, build the compressed
+    store and run CALLS tensor-core matvecs with 16 right-hand sides."""
+    import torch
+    from pskel import mesh as pmesh
+    from pskel import octree
+    from pskel.engine import Engine
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        eng.recompress(1e-4)
+        nbytes = eng.build_store()
+        X = torch.randn((m.N, 16), dtype=torch.complex64, device="cuda")
+        for i in range(calls):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.store_matvec(X)
+            e1.record()
+            torch.cuda.synchronize()
+            print(f"store matvec call {i}: {e0.elapsed_time(e1):.4f} ms, store {nbytes / 1e6:.1f} MB, "
+                  f"status {eng.store_status()}", flush=True)
+
+
+def extras_case():
+    """Octree, ACA, near-field fill and one H-matrix product on the 7,680-RWG sphere."""
+    import time
+
+    import torch
+
+    from pskel.solve import HMatrix
+    from pskel import mesh as pmesh
+    from pskel import octree
+    from pskel.engine import Engine
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        t0 = time.perf_counter()
+        p2 = eng.octree(0.5, origin=(0, 0, 0), min_group=30)
+        print(f"octree: {1e3 * (time.perf_counter() - t0):.3f} ms, {p2.n_groups} groups, "
+              f"{p2.n_blocks} far blocks", flush=True)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        t0 = time.perf_counter()
+        out = eng.aca_compress(1e-4)
+        print(f"aca: {1e3 * (time.perf_counter() - t0):.3f} ms, rank mean {out['k'].mean():.1f}",
+              flush=True)
+        c = m.basis_centres().T
+        patch = np.argsort(np.linalg.norm(c - c[0], axis=1), kind="stable")[:2048].astype(np.int32)
+        ids = torch.as_tensor(patch, device="cuda")
+        Z = torch.empty((2048, 2048), dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        eng.fill_near_device(ids.data_ptr(), 2048, ids.data_ptr(), 2048, Z.data_ptr(), 2048,
+                             0.15, 0.15, 0.15, q_far=1)
+        torch.cuda.synchronize()
+        print(f"near fill 2048 x 2048: {1e3 * (time.perf_counter() - t0):.3f} ms", flush=True)
+        eng.compress(1e-4, precision="c128", tau=1e-10, seed=0)
+        H = HMatrix(eng, part, (0.15, 0.15, 0.15), q_far=7)
+        X = torch.randn(m.N, dtype=torch.complex128, device="cuda")
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H.matvec(X)
+        torch.cuda.synchronize()
+        print(f"H-matrix product: {1e3 * (time.perf_counter() - t0):.3f} ms, near blocks "
+              f"{H.near_bytes / 1e6:.0f} MB", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -642,7 +750,22 @@ def main():
     ap.add_argument("--product-only", action="store_true",
                     help="time the product steps only (no baselines, ablations, checks): the "
                          "command the kernel launch list is captured from")
+    ap.add_argument("--profile-case", choices=("fill", "store", "extras"), default=None,
+                    help="run one small profiling workload on the 7,680-RWG sphere instead of the "
+                         "benchmark (the cases the kernel profiles are captured from)")
+    ap.add_argument("--precision", default="c64", help="profiling case fill: c64 or c128")
+    ap.add_argument("--calls", type=int, default=3, help="profiling cases: calls of the kernel")
+    ap.add_argument("--split", type=int, default=8, help="profiling case fill: fill variant")
+    ap.add_argument("--geom32", type=int, default=0, help="profiling case fill: FP32 pair geometry")
     args = ap.parse_args()
+    if args.profile_case:
+        if args.profile_case == "fill":
+            fill_case(args.precision, args.calls, args.split, args.geom32)
+        elif args.profile_case == "store":
+            store_case(args.calls)
+        else:
+            extras_case()
+        return
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -34,7 +34,8 @@ def nvcc() -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) +
+            glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
 def _compile(src: str, verbose: bool, extra: list[str]) -> str:

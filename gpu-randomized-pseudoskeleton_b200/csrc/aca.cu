@@ -345,11 +345,7 @@ extern "C" int pskel_aca_compress(pskel_ctx *c, double tol, int kmax, int *ranks
     if (!c->mesh.records(kAcaQ).f64.ptr) PSKEL_TRY(build_records(c->mesh, kAcaQ, c->stream, c->flags.as<int>()));
     const size_t smem = sizeof(double2) * ((size_t)maxm + maxn + maxk) + sizeof(double) * 7 * kAcaNP +
                         (size_t)maxm + maxn + 64;
-    static int attr_dev = -1;
-    if (attr_dev != c->device) {
-        PSKEL_CUDA(cudaFuncSetAttribute(aca_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-        attr_dev = c->device;
-    }
+    PSKEL_TRY(ensure_smem_attr(aca_kernel, 200 * 1024));
     if (smem > 200 * 1024) {
         set_error(PSKEL_ERR_ARG, "aca_compress: shared memory %zu bytes", smem);
         return PSKEL_ERR_ARG;

@@ -343,15 +343,13 @@ extern "C" int pskel_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int l
         if (grouped) {                                                                         \
             auto k = jb == 16 ? matvec_group_kernel<A, S, 16>                                  \
                               : (jb == 8 ? matvec_group_kernel<A, S, 8> : matvec_group_kernel<A, S, 1>); \
-            PSKEL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                            200 * 1024));                                      \
+            PSKEL_TRY(ensure_smem_attr(k, 200 * 1024));                                        \
             k<<<c->mv_chunks, 256, gsmem, st>>>(d_b, d_c, reinterpret_cast<const CT<A>::c *>(X), \
                                                 ldx, reinterpret_cast<A *>(Y), ldy, nrhs,     \
                                                 c->mv_max_r, c->mv_max_n);                     \
         } else {                                                                               \
             auto k = matvec_kernel<A, S>;                                                      \
-            PSKEL_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                            200 * 1024));                                      \
+            PSKEL_TRY(ensure_smem_attr(k, 200 * 1024));                                        \
             k<<<grid, 256, smem, st>>>(d_b, nb, reinterpret_cast<const CT<A>::c *>(X), ldx,   \
                                        reinterpret_cast<A *>(Y), ldy, nrhs);                   \
         }                                                                                      \

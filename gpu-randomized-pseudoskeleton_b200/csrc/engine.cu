@@ -576,14 +576,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     return PSKEL_OK;
 }
 
-int set_kernel_attrs() {
-    static bool done = false;
-    if (done) return PSKEL_OK;
-    PSKEL_CUDA(cudaFuncSetAttribute(sample_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sample_smem()));
-    done = true;
-    return PSKEL_OK;
-}
+int set_kernel_attrs() { return ensure_smem_attr(sample_kernel, sample_smem()); }
 
 }  // namespace
 

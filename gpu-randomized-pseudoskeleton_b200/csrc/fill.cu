@@ -435,11 +435,7 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
                         (sizeof(double) * PS + sizeof(T) * VS) * (size_t)TM + 16;
     auto kern = fill2_kernel<T, Q, TM, TN>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     if (per_sm < 1) per_sm = 1;
@@ -464,12 +460,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     constexpr int NT = TM * TN * SPLIT;
     const size_t smem = (sizeof(double) * PS + sizeof(T) * VS) * (size_t)(TM + TN) + 16;
     auto kern = fill_kernel<T, Q, TM, TN, SPLIT>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)smem));
-        attr_set = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     if (per_sm < 1) per_sm = 1;
@@ -776,12 +767,7 @@ static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillP
     const int rows = p.max_rows > 0 && p.max_rows < kTriFillMaxRows ? p.max_rows : kTriFillMaxRows;
     const size_t smem = rec_bytes + 2 * sizeof(T) * (size_t)rows * TN + 16;
     auto kern = tri_fill_kernel<T, Q, TN, OFS>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        const size_t most = rec_bytes + 2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16;
-        PSKEL_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)most));
-        attr_set = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(kern, rec_bytes + 2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;

@@ -216,12 +216,7 @@ extern "C" int pskel_near_matvec(pskel_ctx *c, const pskel_c128 *X, int ldx, psk
     }
     // the near fill ran on the context's stream
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
-    static bool attr = false;
-    if (!attr) {
-        PSKEL_CUDA(cudaFuncSetAttribute(near_matvec_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        200 * 1024));
-        attr = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(near_matvec_kernel, 200 * 1024));
     near_matvec_kernel<<<c->n_near, kNearMvThreads, smem, st>>>(
         c->near_tab.as<NearBlock>(), c->near_data.as<double2>(),
         reinterpret_cast<const double2 *>(X), ldx, reinterpret_cast<double2 *>(Y), ldy, nrhs);

@@ -584,17 +584,8 @@ int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
 }
 
 int svd_resident_attr() {
-    static bool attr = false;
-    if (!attr) {
-        PSKEL_CUDA(cudaFuncSetAttribute(svd_resident_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kSmemBudget));
-        PSKEL_CUDA(cudaFuncSetAttribute(svd_blocked_kernel,
-                                        cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kSmemBudget));
-        attr = true;
-    }
-    return PSKEL_OK;
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel, kSmemBudget));
+    return ensure_smem_attr(svd_blocked_kernel, kSmemBudget);
 }
 
 int svd_streams_create(SvdStreams &p) {

@@ -22,8 +22,17 @@ struct LegacyCtx {
     std::mutex mu;
 };
 
-LegacyCtx &ctx() {
-    static LegacyCtx c;
+// One context per device ordinal: the reference entry points run on whichever device is
+// current when they are called, and streams, events and buffers belong to one device.
+LegacyCtx *ctx() {
+    static PerDevice<LegacyCtx> contexts;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        set_error(PSKEL_ERR_CUDA, "cudaGetDevice failed");
+        return nullptr;
+    }
+    LegacyCtx *c = contexts.get(dev);
+    if (!c) set_error(PSKEL_ERR_ARG, "device ordinal %d beyond %d", dev, kMaxDevices);
     return c;
 }
 
@@ -198,7 +207,9 @@ extern "C" double impedance_matrix_cuda_elbyel4(
     (void)cor_solid; (void)flag; (void)trian; (void)un; (void)ds; (void)rows_trian;
     (void)cols_trian; (void)rows_un; (void)cols_un; (void)rows_ds; (void)cols_ds;
     (void)blocks_x; (void)blocks_y; (void)threads_x; (void)threads_y; (void)limx; (void)limy;
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return kNaN;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     float ms = 0;
     int st = dense_fill(c, field, k, eta, Rinteg_s, Ranal_s, Rinteg_f, r1, r2, vertex, topol,
@@ -237,7 +248,9 @@ static int split_fill(double *Zr, double *Zi, int field, double k, double eta, d
                       double *topol, double *edges, double *ln, double *cent, int N, int n_r1,
                       int n_r2, int rows_vertex, int cols_vertex, int rows_topol, int cols_topol,
                       int rows_edges, int cols_edges, int n_ln, int rows_cent, int cols_cent) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return 0;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     float ms = 0;
     int st = dense_fill(c, field, k, eta, Rinteg_s, Ranal_s, Rinteg_f, r1, r2, vertex, topol,
@@ -501,7 +514,9 @@ extern "C" double cuda_complete_compression(
     (void)un; (void)ds; (void)rows_trian; (void)cols_trian; (void)rows_un; (void)cols_un;
     (void)rows_ds; (void)cols_ds; (void)blocks_x; (void)blocks_y; (void)threads_x;
     (void)threads_y; (void)limx; (void)limy;
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return kNaN;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     auto run_round = [&](double &err) -> int {
         PSKEL_TRY(check_field(field));
@@ -569,7 +584,9 @@ extern "C" double cuda_complete_compression(
 extern "C" double compute_error_compression(pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
                                             pskel_c128 *Avtest_old, pskel_c128 *Avtest_new,
                                             pskel_c128 *vtest, int M1, int N1, int M2) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return kNaN;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     double err = kNaN;
     auto run = [&]() -> int {
@@ -633,7 +650,9 @@ static int host_pinv(LegacyCtx &c, const pskel_c128 *A, int M, int N, double tau
 extern "C" int aux_pinv_compression(pskel_c128 *C, pskel_c128 *U, pskel_c128 *R, pskel_c128 *A,
                                     int64_t *row_samples, int64_t *col_samples, int ns, int M,
                                     int N, double tolerance) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return 0;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     if (!C || !U || !R || !A || !row_samples || !col_samples || ns <= 0 || M <= 0 || N <= 0) {
         set_error(PSKEL_ERR_ARG, "aux_pinv_compression: ns=%d M=%d N=%d", ns, M, N);
@@ -658,13 +677,17 @@ extern "C" int aux_pinv_compression(pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
 
 extern "C" int cuda_pinv(pskel_c128 *pinvA, pskel_c128 *U, double *S, pskel_c128 *Vt,
                          pskel_c128 *A, int M, int N, double treshold) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return 0;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     return host_pinv(c, A, M, N, treshold, pinvA, U, S, Vt, 1) == PSKEL_OK ? 1 : 0;
 }
 
 extern "C" int cuda_svd(pskel_c128 *U, double *S, pskel_c128 *Vt, pskel_c128 *A, int M, int N) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return 0;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     return host_pinv(c, A, M, N, 0.0, nullptr, U, S, Vt, 0) == PSKEL_OK ? 1 : 0;
 }
@@ -683,7 +706,9 @@ __global__ void filter_kernel(double *v, int n, double thr) {
 }  // namespace pskel
 
 extern "C" int cuda_filter(double *V, double treshold, int N) {
-    LegacyCtx &c = ctx();
+    LegacyCtx *cp = ctx();
+    if (!cp) return 0;
+    LegacyCtx &c = *cp;
     std::lock_guard<std::mutex> lk(c.mu);
     auto run = [&]() -> int {
         if (!V || N < 0) {

@@ -25,14 +25,35 @@ void count_launch(long long n) { g_launches.fetch_add(n, std::memory_order_relax
 long long launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 int sm_count() {
-    static int n = 0;
-    if (n == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
+    static std::atomic<int> counts[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= kMaxDevices) dev = 0;
+    int n = counts[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
         cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
         if (n <= 0) n = 148;
+        counts[dev].store(n, std::memory_order_relaxed);
     }
     return n;
+}
+
+static SmemAttrTable g_smem_attrs;
+
+int ensure_smem_attr(const void *func, size_t bytes) {
+    int dev = 0;
+    PSKEL_CUDA(cudaGetDevice(&dev));
+    cudaError_t err = cudaSuccess;
+    const bool ok = g_smem_attrs.raise(func, dev, bytes, [&](size_t b) {
+        err = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+        return err == cudaSuccess;
+    });
+    if (!ok) {
+        set_error(PSKEL_ERR_CUDA, "cudaFuncSetAttribute(%zu bytes of shared memory) on device %d: %s",
+                  bytes, dev, cudaGetErrorString(err));
+        return PSKEL_ERR_CUDA;
+    }
+    return PSKEL_OK;
 }
 
 // ------------------------------------------------------------------ 7-point rule

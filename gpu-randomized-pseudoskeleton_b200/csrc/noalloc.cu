@@ -17,6 +17,9 @@
 //  * The first call on a device looks up the device address of the scratch array
 //    (cudaGetSymbolAddress, with that device current) and sets the kernel attributes; make
 //    that first call before any stream capture.
+//  * The call reads the convergence status back and waits for its stream (see below), which
+//    a stream capture does not allow: on a stream that is being captured it returns
+//    PSKEL_ERR_STATE before doing anything, so the caller's capture stays intact.
 //  * All calls share the array, and it keeps the contents of the last call; everything the
 //    kernels read is written by the same call before it is read. Calls whose work overlaps
 //    on the GPU (other streams or host threads) race on the array: serialise them.
@@ -115,7 +118,6 @@ __global__ void noalloc_finish_kernel(const unsigned char *base, int M, int N, d
 }
 
 namespace {
-constexpr int kMaxDevices = 64;
 unsigned char *g_scratch_addr[kMaxDevices] = {};
 std::mutex g_setup_mu;
 
@@ -154,9 +156,16 @@ extern "C" int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau,
         set_error(PSKEL_ERR_ARG, "pinv_noalloc: device %d out of range", dev);
         return PSKEL_ERR_ARG;
     }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    PSKEL_CUDA(cudaStreamIsCapturing(s, &cap));
+    if (cap != cudaStreamCaptureStatusNone) {
+        set_error(PSKEL_ERR_STATE, "pinv_noalloc: the stream is being captured; the call waits "
+                                   "for its stream to read the convergence status");
+        return PSKEL_ERR_STATE;
+    }
     unsigned char *base = nullptr;
     PSKEL_TRY(noalloc_setup_device(dev, &base));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const double2 *Ad = reinterpret_cast<const double2 *>(A);
     noalloc_setup_kernel<<<16, 256, 0, s>>>(base, Ad, M, N, tau, relative);
     PSKEL_LAUNCHED(1);

@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "device_state.hpp"
 #include "pskel.h"
 
 namespace pskel {
@@ -232,7 +233,7 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
 // One resident job (m x n fits in shared memory) whose index map entry is d_idx0[0].
 int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
                                cudaStream_t stream);
-// Shared-memory attributes of the SVD kernels (set once per process).
+// Shared-memory limits of the SVD kernels on the current device (set once per device).
 int svd_resident_attr();
 
 // pinv of each job after batched_svd: P_b (n_b x m_b) = V diag(1/sigma^2) (A V)^H over the
@@ -284,7 +285,16 @@ int cur_matvec_error(const double2 *C, const double2 *U, const double2 *R, const
                      cudaStream_t stream, DevBuf &scratch);
 
 // ------------------------------------------------------------------ device properties
+// SM count of the current device.
 int sm_count();
+
+// Raises the dynamic-shared-memory limit of a kernel on the CURRENT device to at least `bytes`
+// (the attribute is per device; set once per kernel, device and size; thread-safe).
+int ensure_smem_attr(const void *func, size_t bytes);
+template <typename K>
+int ensure_smem_attr(K *kern, size_t bytes) {
+    return ensure_smem_attr(reinterpret_cast<const void *>(kern), bytes);
+}
 
 // Count of kernels launched by the library (reported by pskel_kernel_launches).
 void count_launch(long long n = 1);

@@ -204,12 +204,7 @@ static bool qr_fits(int m, int n) { return (size_t)m * n * sizeof(double2) <= kQ
 
 int batched_qr(const std::vector<QrJob> &h_jobs, cudaStream_t stream, DevBuf &scratch) {
     if (h_jobs.empty()) return PSKEL_OK;
-    static bool attr = false;
-    if (!attr) {
-        PSKEL_CUDA(cudaFuncSetAttribute(qr_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kQrSmem));
-        attr = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(qr_kernel<true>, kQrSmem));
     // two launches: the jobs that fit in shared memory (grouped by size for the allocation) and
     // the rest in global memory
     std::vector<QrJob> fit, big;

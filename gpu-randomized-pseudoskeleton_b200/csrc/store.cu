@@ -608,12 +608,7 @@ extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y,
     }
     PSKEL_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    static bool attr = false;
-    if (!attr) {
-        PSKEL_CUDA(cudaFuncSetAttribute(store_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        (int)kStSmem));
-        attr = true;
-    }
+    PSKEL_TRY(ensure_smem_attr(store_gemm_kernel, kStSmem));
     PSKEL_TRY(c->st_err.reserve(256));
     PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
     PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));

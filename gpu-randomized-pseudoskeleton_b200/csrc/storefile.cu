@@ -19,6 +19,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 #include <vector>
 
 #include "engine_internal.cuh"
@@ -154,7 +156,7 @@ extern "C" int pskel_store_save(pskel_ctx *c, const char *path, double thresh) {
     return PSKEL_OK;
 }
 
-extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
+static int store_load_impl(pskel_ctx *c, const char *path, int *n_blocks) {
     if (!c || !path) {
         set_error(PSKEL_ERR_ARG, "store_load: null argument");
         return PSKEL_ERR_ARG;
@@ -174,6 +176,14 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
         FILE *f;
         ~Closer() { std::fclose(f); }
     } closer{r.f};
+    // every count read from the header is bounded by the file's size before anything is sized
+    // from it, so a corrupt or hostile header cannot ask for more memory than the file holds
+    long long fsize = -1;
+    if (std::fseek(r.f, 0, SEEK_END) == 0) fsize = std::ftell(r.f);
+    if (fsize < 0 || std::fseek(r.f, 0, SEEK_SET) != 0) {
+        set_error(PSKEL_ERR_ARG, "store_load: cannot size %s", path);
+        return PSKEL_ERR_ARG;
+    }
     char magic[8];
     r.get(magic, 8);
     const unsigned version = r.get<unsigned>();
@@ -185,7 +195,8 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
         set_error(PSKEL_ERR_ARG, "store_load: %s is not a version-%u store file", path, kStoreVersion);
         return PSKEL_ERR_ARG;
     }
-    if (N != c->mesh.ne || G <= 0 || B <= 0 || G > (1 << 26) || B > (1 << 28)) {
+    if (N != c->mesh.ne || G <= 0 || B <= 0 || G > (1 << 26) || B > (1 << 28) ||
+        4 * ((long long)G + 1) + 24 * (long long)B > fsize) {
         set_error(PSKEL_ERR_ARG, "store_load: N=%lld G=%d B=%d (the mesh has %d RWG)", N, G, B,
                   c->mesh.ne);
         return PSKEL_ERR_ARG;
@@ -201,6 +212,10 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
             set_error(PSKEL_ERR_ARG, "store_load: bad group offsets");
             return PSKEL_ERR_ARG;
         }
+    if (4 * (long long)gptr[G] > fsize) {
+        set_error(PSKEL_ERR_ARG, "store_load: %s is truncated", path);
+        return PSKEL_ERR_ARG;
+    }
     std::vector<int> gids(gptr[G]);
     r.get(gids.data(), sizeof(int) * gids.size());
     r.get(gt.data(), sizeof(int) * B);
@@ -223,6 +238,10 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
             return PSKEL_ERR_ARG;
         }
         if (mir < 0) total += al256(16 * (size_t)m * k) + al256(8 * (size_t)k) + al256(16 * (size_t)k * n);
+    }
+    if (total > (size_t)fsize + 256 * (size_t)B * 3) {  // factor bytes plus their padding
+        set_error(PSKEL_ERR_ARG, "store_load: %s is truncated", path);
+        return PSKEL_ERR_ARG;
     }
     std::vector<char> data(total + 1);
     std::vector<size_t> off(B, 0);
@@ -278,4 +297,16 @@ extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
     ++c->generation;  // the CUR-form tables no longer describe these blocks
     if (n_blocks) *n_blocks = B;
     return PSKEL_OK;
+}
+
+extern "C" int pskel_store_load(pskel_ctx *c, const char *path, int *n_blocks) {
+    try {
+        return store_load_impl(c, path, n_blocks);
+    } catch (const std::bad_alloc &) {
+        set_error(PSKEL_ERR_OOM, "store_load: out of host memory reading %s", path ? path : "");
+        return PSKEL_ERR_OOM;
+    } catch (const std::length_error &) {
+        set_error(PSKEL_ERR_ARG, "store_load: %s: sizes out of range", path ? path : "");
+        return PSKEL_ERR_ARG;
+    }
 }

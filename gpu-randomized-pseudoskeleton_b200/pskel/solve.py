@@ -94,9 +94,18 @@ def gmres(A, b, tol: float = 1e-6, restart: int = 60, maxiter: int = 2000, x0=No
     ||b - A x|| <= tol ||b|| (checked at every restart) or after maxiter products."""
     import torch
     if M is not None:
-        y, hist, nmv = gmres(lambda v: A(M(v)), b, tol, restart, maxiter,
-                             None if x0 is None else x0, None)
-        return M(y), hist, nmv
+        if x0 is None:
+            y, hist, nmv = gmres(lambda v: A(M(v)), b, tol, restart, maxiter, None, None)
+            return M(y), hist, nmv
+        # x0 is a guess of x, not of y: solve A M y = b - A x0 for the correction from y = 0,
+        # to the same absolute residual tol ||b||, and return x0 + M y
+        bn = float(torch.linalg.vector_norm(b))
+        r0 = b - A(x0)
+        rn = float(torch.linalg.vector_norm(r0))
+        if rn <= tol * bn:
+            return x0.clone(), [rn / bn if bn > 0 else 0.0], 1
+        y, hist, nmv = gmres(lambda v: A(M(v)), r0, tol * bn / rn, restart, maxiter - 1, None, None)
+        return x0 + M(y), [h * rn / bn for h in hist], nmv + 1
     n = b.shape[0]
     bn = float(torch.linalg.vector_norm(b))
     if bn == 0.0:

@@ -436,8 +436,9 @@ int pskel_mlp_adam(float *params, const float *grad, float *m, float *v, int t, 
    tau * s_max (relative = 1) are dropped. The scratch is one fixed 256 KiB device array per
    GPU, shared by all calls: calls that overlap on the GPU race. The first call on a device
    looks up that array's address; make it before any stream capture. Returns after its stream
-   has finished, with PSKEL_ERR_ARG for sizes above 64 and PSKEL_ERR_NOCONV if the Jacobi
-   sweeps did not converge. */
+   has finished, with PSKEL_ERR_ARG for sizes above 64, PSKEL_ERR_NOCONV if the Jacobi
+   sweeps did not converge and PSKEL_ERR_STATE, without doing anything, when the stream is
+   being captured (the call waits for its stream). */
 int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau, int relative,
                        pskel_c128 *P, double *sigma, int *rank, void *stream);
 

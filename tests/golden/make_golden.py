@@ -9,7 +9,9 @@ passed for trian, as at ``:783-784``). The library is executed as a black box on
 Each fixture stores the mesh arrays it was computed on (so the mesh generator is pinned
 too), the EM parameters, the 1-based row/column id lists and the complex128 result.
 
-Usage:  python tests/golden/make_golden.py [reference_root] [near]
+Usage:  python tests/golden/make_golden.py REFERENCE_ROOT [near]
+
+REFERENCE_ROOT is the root of a checkout of the reference repository (required).
 """
 from __future__ import annotations
 
@@ -25,6 +27,12 @@ sys.path.insert(0, os.path.join(ROOT, "gpu-randomized-pseudoskeleton_b200"))
 from pskel import mesh as pmesh  # noqa: E402
 
 _D = ctypes.POINTER(ctypes.c_double)
+
+
+def reference_root() -> str:
+    if len(sys.argv) < 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [near]  (root of a reference checkout)")
+    return sys.argv[1]
 
 
 def load(ref_root: str):
@@ -59,8 +67,7 @@ def save(name, m, r1, r2, k, eta, rint, Z):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    f = load(ref)
+    f = load(reference_root())
     eta = 120 * np.pi
     rng = np.random.default_rng(20261203)
 
@@ -111,8 +118,7 @@ def main_near():
     """Near-field fixtures: blocks whose RWG pairs include same-triangle, adjacent and nearby
     triangle pairs, with the integration radii (Rinteg_s, Ranal_s, Rinteg_f) switching the
     library onto its near-field rules."""
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    f = load(ref)
+    f = load(reference_root())
     eta = 376.73
     # (n1, n2) one plate of the two-plate workload (lambda = 1): RWG 1-48 against 1-64
     m = pmesh.two_plates(1.0, 20, 3.0)
