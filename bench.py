@@ -74,7 +74,6 @@ def build_workload(name):
 # ----------------------------------------------------------------------------- CPU baseline
 def _cpu_worker(args):
     name, blocks = args
-    os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
     from oracle import cur_oracle as co
     from oracle import element as el
     m, part = build_workload(name)
@@ -99,18 +98,34 @@ def cpu_baseline(name, n_sample=96, seed=0):
     cores = os.cpu_count() or 1
     chunks = [(name, sample[i::cores].tolist()) for i in range(cores) if len(sample[i::cores])]
     ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(len(chunks)) as pool:
-        res = [x for part_res in pool.map(_cpu_worker, chunks) for x in part_res]
-    wall = time.perf_counter() - t0
+    # one BLAS thread per worker: the spawned workers inherit this environment before they
+    # import numpy, so each worker is one single-threaded reference process
+    saved = {k: os.environ.get(k) for k in _BLAS_THREADS}
+    os.environ.update({k: "1" for k in _BLAS_THREADS})
+    try:
+        t0 = time.perf_counter()
+        with ctx.Pool(len(chunks)) as pool:
+            res = [x for part_res in pool.map(_cpu_worker, chunks) for x in part_res]
+        wall = time.perf_counter() - t0
+    finally:
+        for k, v in saved.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
     per_block = np.array([t for _, t, _ in res])
     core_s = per_block.sum()
     est_ms = per_block.mean() * part.n_blocks / cores * 1e3
     return dict(value=float(est_ms), unit="ms", cores=cores, kind="port",
-                sample=f"{len(sample)} random far blocks of {part.n_blocks} (seed {seed}); "
-                       f"{core_s:.1f} core-s, {wall:.1f} s wall; whole-job time extrapolated "
-                       f"as mean block time x blocks / cores",
+                single_core_ms=float(per_block.mean() * part.n_blocks * 1e3),
+                sample=f"{len(sample)} random far blocks of {part.n_blocks} (seed {seed}), each "
+                       f"compressed by a single-threaded worker (one BLAS thread); {core_s:.1f} "
+                       f"core-s, {wall:.1f} s wall; whole-job time EXTRAPOLATED as mean block "
+                       f"time x blocks / cores (single_core_ms: x blocks)",
                 cpu=_cpu_model())
+
+
+_BLAS_THREADS = ("OPENBLAS_NUM_THREADS", "OMP_NUM_THREADS", "MKL_NUM_THREADS")
 
 
 def _cpu_model():
@@ -309,6 +324,13 @@ def run_ours(args, rank, world, dev):
     plain = without_symmetry(lambda: eng.compress(TOL, **PLAIN))
     plain_b_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
     t_plain = eng.timing()
+
+    # the same plain method with the symmetric mode: the product against it isolates what the
+    # three patterns (learned, mixed precision, batched + graph) gain on their own
+    def plain_symmetric():
+        eng.set_symmetric(True)
+        return eng.compress(TOL, **PLAIN)
+    plain_sym_ms, _, _, _ = timed(plain_symmetric, max(1, min(2, args.steps)), 1)
     mixed_only = without_symmetry(lambda: eng.compress(TOL, **dict(PLAIN, precision="c64")))
     mixed_ms, _, _, _ = timed(mixed_only, 1, 1)
     learned_only = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
@@ -335,13 +357,22 @@ def run_ours(args, rank, world, dev):
     st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     err = eng.true_errors()
     err_plain = None
-    if args.plain_errors:
+    if not args.no_plain_errors:
         eng.set_symmetric(False)
         st_plain = eng.compress(TOL, **PLAIN)
         err_plain = eng.true_errors()
         eng.set_symmetric(True)
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     blockops = run_blockops(eng, st, m, flush)
+    config3 = None
+    if not args.no_config3:
+        def r0_for(tol):
+            fe = features(sp, K_WAVE, tol)
+            y = pred.predict_log2(fe)
+            return np.clip(np.ceil(pred.margin * np.exp2(y)), 1, Dmin).astype(np.int32)
+        config3 = run_config3(eng, m, r0_for)
+        eng.set_symmetric(True)
+        st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     octree_t = run_octree(args, m, part, dev) if rank == 0 else None
     aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only) else None
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
@@ -355,7 +386,8 @@ def run_ours(args, rank, world, dev):
         metric=METRIC, value=round(ms, 3), unit="ms", n_gpus=world, steps=args.steps,
         warmup=args.warmup, ms_per_step=round(ms, 3), higher_is_better=False,
         scaling="strong" if world > 1 else "weak", vs_baseline=None,
-        dtype="c64 fill (FP64 geometry) + FP64 Jacobi pinv",
+        dtype="c64 fill (" + ("FP32 pair geometry" if tune["choice"][0] == "tri32_" else "FP64 geometry")
+              + ") + FP64 Jacobi pinv",
         data="synthetic: " + WORKLOADS[args.workload]["desc"] + "; no dataset",
         config=dict(workload=args.workload, rwg=m.N, groups=part.n_groups,
                     blocks=int(part.n_blocks), blocks_this_rank=int(nb), tol=TOL,
@@ -369,12 +401,18 @@ def run_ours(args, rank, world, dev):
         plain_ms=round(plain_ms, 3), speedup_vs_plain=round(plain_ms / ms, 3),
         plain_desc="plain FP64 GPU pseudoskeleton: start min(m,n)/10, doubling, same estimator, "
                    "driven one block at a time (the reference's per-block driving)",
-        ablation_ms=dict(plain_batched=round(plain_b_ms, 3), mixed_batched=round(mixed_ms, 3),
+        ablation_ms=dict(plain_batched=round(plain_b_ms, 3),
+                         plain_batched_symmetric=round(plain_sym_ms, 3),
+                         mixed_batched=round(mixed_ms, 3),
                          learned_batched=round(learned_ms, 3),
                          learned_mixed_batched=round(lm_nosym_ms, 3),
                          learned_mixed_batched_symmetric=round(ms, 3),
                          learned_batched_symmetric_c128=round(lsym128_ms, 3)),
         speedup_vs_plain_batched=round(plain_b_ms / ms, 3),
+        speedup_three_patterns=round(plain_sym_ms / ms, 3),
+        speedup_three_patterns_desc="plain FP64 batched with the symmetric mode / the product: the "
+                                    "learned first sample count, complex-FP32 fill and graph "
+                                    "replay alone (both arms use the symmetric mode)",
         step_times_ms=[round(t, 3) for t in times],
         phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},
         product=dict(r_mean=float(st["r"].mean()), rounds_mean=float(st["rounds"].mean()),
@@ -407,6 +445,7 @@ def run_ours(args, rank, world, dev):
                  d2h_bytes_per_step=int(d2h)),
         clocks=clocks, gpu_launches=int(launches),
         blockops=blockops,
+        mixed_precision=config3,
         octree=octree_t,
         aca=aca_t,
     )
@@ -445,11 +484,16 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     flops = roofline.matvec_flops(mm, nn, rr, nrhs)
     peak = _hbm_peak()
     gbs = (factor_bytes + vec_bytes) / (mv_ms * 1e-3) / 1e9
-    # recompression to the compression tolerance
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    ks = eng.recompress(TOL)
-    rc_ms = (time.perf_counter() - t0) * 1e3
+    # recompression to the compression tolerance (device time of its launches, from the
+    # library's own events on its stream)
+    eng.recompress(TOL)
+    rc_times = []
+    for _ in range(3):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ks = eng.recompress(TOL)
+        rc_times.append(eng.recompress_ms())
+    rc_ms = float(np.mean(rc_times))
     # compressed store and the tensor-core matvec over it
     t0 = time.perf_counter()
     store_bytes = eng.build_store()
@@ -472,8 +516,8 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     st_ms = float(np.mean(st_times))
     st_status = eng.store_status()
     kk = ks.astype(np.float64)
-    st_alg_bytes = roofline.matvec_bytes(mm, nn, kk, 0, 8.0)  # bf16 hi + lo of re and im
-    st_gbs = (st_alg_bytes + vec_bytes) / (st_ms * 1e-3) / 1e9
+    st_alg_bytes = roofline.store_matvec_bytes(mm, nn, kk, m.N, nrhs)
+    st_gbs = st_alg_bytes / (st_ms * 1e-3) / 1e9
     return dict(
         matvec=dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),
                     factor_bytes=factor_bytes, vector_bytes=vec_bytes,
@@ -487,11 +531,66 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
                           achieved_gbs=round(st_gbs, 1), peak_gbs=peak, frac=round(st_gbs / peak, 4),
                           arithmetic="tcgen05 kind::f16, bf16 hi/lo split (3 products), FP32 accumulation",
                           bytes="C' and diag(S) R' as bf16 hi + lo of [re | im] (8 bytes per complex "
-                                "entry), gathered X and scattered Y (algorithmic; tile padding excluded)"),
+                                "entry), X and Y once each, T written and read once (algorithmic; "
+                                "store_bytes is the tiled store including its padding)"),
         recompress=dict(ms=round(rc_ms, 3), thresh=TOL, r_mean=float(rr.mean()),
-                        k_mean=float(ks.mean()), arithmetic="FP64 (Jacobi on C, R^H and the core)",
-                        timing="host wall clock around the synchronous call"),
+                        k_mean=float(ks.mean()),
+                        gflops=round(roofline.recompress_flops(mm, nn, rr, kk) / (rc_ms * 1e-3) / 1e9, 1),
+                        arithmetic="FP64 (Householder QR of C and R^H, Jacobi SVD of the core)",
+                        timing="device time between the library's events around its launches "
+                               "(mean of 3 calls)"),
     )
+
+
+STORE_ENTRY_BYTES = {"bf16x3": 8.0, "tf32": 8.0, "tf32x3": 16.0}  # per complex factor entry
+
+
+def run_config3(eng, m, r0_for, nrhs=16, reps=5):
+    """Mixed precision at tolerances 1e-3 and 1e-4: the product compression (complex-FP32 fill,
+    FP64 pinv) with every block's error against its dense FP64 fill, then the recompressed
+    store in each operand format (one TF32 plane, TF32 hi + lo, bf16 hi + lo) and its 16-RHS
+    matvec against the dense FP64 far-field product on complex Gaussian vectors (seed 0)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(0)
+    X = torch.randn((m.N, nrhs), dtype=torch.complex64, device="cuda", generator=g)
+    Yd = eng.dense_far_matvec(X.to(torch.complex128))
+    nd = float(torch.linalg.vector_norm(Yd))
+    out = {}
+    for tol in (1e-3, 1e-4):
+        eng.set_symmetric(True)
+        st = eng.compress(tol, r0=r0_for(tol), **PRODUCT)
+        err = eng.true_errors()
+        thresh = tol / 10
+        ks = eng.recompress(thresh)
+        mm, nn, kk = (x.astype(np.float64) for x in (st["m"], st["n"], ks))
+        row = dict(blocks=int(len(err)), err_max=float(err.max()), err_median=float(np.median(err)),
+                   blocks_over_tol=int((err > tol).sum()), recompress_thresh=thresh,
+                   k_mean=float(kk.mean()), formats={})
+        for mode in ("tf32", "tf32x3", "bf16x3"):
+            nbytes = eng.build_store(mode)
+            for _ in range(2):
+                Y = eng.store_matvec(X)
+            torch.cuda.synchronize()
+            ts = []
+            for _ in range(reps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                Y = eng.store_matvec(X)
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = float(np.mean(ts))
+            rel = float(torch.linalg.vector_norm(Y.to(torch.complex128) - Yd)) / nd
+            alg = roofline.store_matvec_bytes(mm, nn, kk, m.N, nrhs, STORE_ENTRY_BYTES[mode])
+            row["formats"][mode] = dict(matvec_ms=round(ms, 4), store_bytes=int(nbytes),
+                                        status=int(eng.store_status()),
+                                        rel_err_vs_dense=rel, achieved_gbs=round(alg / (ms * 1e-3) / 1e9, 1))
+        out[f"tol_{tol:g}"] = row
+    out["desc"] = ("complex-FP32 fill + FP64 pinv (product options), recompression at tol/10, "
+                   "store matvec with 16 complex Gaussian right-hand sides against the dense FP64 "
+                   "far-field product")
+    return out
 
 
 def _hbm_peak():
@@ -742,8 +841,11 @@ def main():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", choices=tuple(WORKLOADS), default="sphere30k")
     ap.add_argument("--save", default=None, help="write per-block stats (npz)")
-    ap.add_argument("--plain-errors", action="store_true", help="also check the plain run's errors")
+    ap.add_argument("--no-plain-errors", action="store_true",
+                    help="skip the dense-fill error check of the plain baseline's blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-config3", action="store_true",
+                    help="skip the mixed-precision report (store formats against the dense product)")
     ap.add_argument("--fill-variant", default=None,
                     help="fill variant instead of the autotuner's choice: tri<w> or tri32_<w> "
                          "(w = 0 balanced, 4, 8, 16) or entry<s>")
@@ -787,6 +889,9 @@ def main():
                     data="synthetic: " + WORKLOADS[args.workload]["desc"],
                     config=dict(workload=args.workload, tol=TOL, quadrature="7-point per triangle"),
                     cpu_baseline=dict(last, value=round(v, 1)),
+                    extrapolated=True, sample_blocks_per_step=48,
+                    note="each step times 48 random blocks over all host cores and extrapolates to "
+                         "the whole block list; value = median over the steps",
                     e2e=dict(value=round(v, 1), unit="ms", h2d_bytes_per_step=0, d2h_bytes_per_step=0))
         print(json.dumps(line), flush=True)
         return

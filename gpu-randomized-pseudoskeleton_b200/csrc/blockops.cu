@@ -527,6 +527,7 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     }
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, c->stream));
+    PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
     if (f32) recomp_load_kernel<float2><<<nb, 256, 0, c->stream>>>(d_jobs);
     else recomp_load_kernel<double2><<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
@@ -539,12 +540,18 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     PSKEL_TRY(batched_apply_q(aps, c->stream, c->tmp3));
     recomp_rp_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
+    PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
     // ranks and SVD statuses back to the host
     std::vector<SvdJob> h2(nb);
     std::vector<int> ks(nb);
     PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(ks.data(), d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
+        c->timing[4] = ms;
+    }
     for (const SvdJob &j : h2)
         if (j.status != PSKEL_OK) {
             set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a core did not converge");

@@ -143,31 +143,99 @@ static size_t sample_smem() {
     return sizeof(uint32_t) * (kMaxGroup + 4 * (kMaxGroup / 32)) + sizeof(int) * kMaxExtra;
 }
 
+// Re-check of a block accepted with little margin: pe2 fresh extra rows and pc2 fresh extra
+// columns, drawn outside every row / column the block's round already used (I and Ix, J and
+// Jx), from Philox streams 4 (rows) and 5 (columns) of that round.
+struct VerifyWork {
+    const int *rows_g, *cols_g;
+    const int *I, *J, *Ix, *Jx;  // the round's local samples
+    int *Ix2, *Jx2;              // the new local samples (sorted)
+    int *Ig2, *Jg2;              // their global ids
+    int m, n, r, pe, pc, pe2, pc2;
+    int block_id, round;
+};
+
+__global__ void __launch_bounds__(128) verify_sample_kernel(const VerifyWork *__restrict__ works,
+                                                            uint64_t seed) {
+    __shared__ uint32_t words[kMaxExtra];
+    __shared__ uint32_t bits_used[kMaxGroup / 32];
+    __shared__ uint32_t bits_x[kMaxGroup / 32];
+    __shared__ int scan[kMaxGroup / 32];
+    __shared__ int pick[kMaxExtra];
+    const VerifyWork w = works[blockIdx.x];
+    for (int side = 0; side < 2; ++side) {
+        const int D = side == 0 ? w.m : w.n;
+        const int *S0 = side == 0 ? w.I : w.J;
+        const int *S1 = side == 0 ? w.Ix : w.Jx;
+        const int n1 = side == 0 ? w.pe : w.pc;
+        const int p = side == 0 ? w.pe2 : w.pc2;
+        int *out = side == 0 ? w.Ix2 : w.Jx2;
+        const int nw = (D + 31) / 32;
+        for (int i = threadIdx.x; i < nw; i += blockDim.x) bits_used[i] = 0u;
+        __syncthreads();
+        for (int i = threadIdx.x; i < w.r + n1; i += blockDim.x) {
+            const int v = i < w.r ? S0[i] : S1[i - w.r];
+            atomicOr(&bits_used[v >> 5], 1u << (v & 31));
+        }
+        __syncthreads();
+        draw_extra(words, bits_used, bits_x, scan, pick, p, D, w.r + n1, w.block_id, w.round,
+                   4u + side, seed, out);
+    }
+    for (int e = threadIdx.x; e < w.pe2; e += blockDim.x) w.Ig2[e] = w.rows_g[w.Ix2[e]];
+    for (int e = threadIdx.x; e < w.pc2; e += blockDim.x) w.Jg2[e] = w.cols_g[w.Jx2[e]];
+}
+
 // ------------------------------------------------------------------ core gather
 __device__ __forceinline__ double2 promote(double2 v) { return v; }
 __device__ __forceinline__ double2 promote(float2 v) { return make_double2(v.x, v.y); }
 
+// The core Z(I, J) = C(I, :) in FP64 for the SVD, and the same numbers written into R(:, J):
+// C and R come from two fills (Z(group_t, J) and the transposed Z(group_s, I)) whose complex-FP32
+// roundings of the shared entries Z(I, J) differ, and the pinv of an ill-conditioned core
+// amplifies any difference between the core and R(:, J) (at r = min(m, n) with a near-exact
+// inverse, to 1e-4 of the block). With one set of numbers C U R interpolates its own samples.
 template <typename S>
 __global__ void __launch_bounds__(256) gather_core_kernel(const BlockWork *__restrict__ works) {
     const BlockWork w = works[blockIdx.x];
     const S *C = reinterpret_cast<const S *>(w.C);
-    const int r = w.r;
+    S *Rx = reinterpret_cast<S *>(w.Rx);
+    const int r = w.r, ldr = w.r + w.pe;
     for (int idx = threadIdx.x; idx < r * r; idx += blockDim.x) {
         const int i = idx % r, j = idx / r;
-        w.AV[idx] = promote(C[w.I[i] + (size_t)j * w.m]);
+        const S v = C[w.I[i] + (size_t)j * w.m];
+        w.AV[idx] = promote(v);
+        Rx[i + (size_t)w.J[j] * ldr] = v;
     }
 }
 
 // ------------------------------------------------------------------ randomized estimate
-// est = max( ||Z(Ix,:) - C(Ix,:) U R||_F / ||Z(Ix,:)||_F ,  ||Z(:,Jx) - C U R(:,Jx)||_F / ||Z(:,Jx)||_F )
-// on pe extra rows and pc extra columns that were not sampled (0 if neither exists).
+// Residual of a block's C U R on pe extra rows and pc extra columns that were not sampled:
+//   rows: ||Z(Ix,:) - C(Ix,:) U R||_F^2 and ||Z(Ix,:)||_F^2,
+//   cols: ||Z(:,Jx) - C U R(:,Jx)||_F^2 and ||Z(:,Jx)||_F^2,
+// and est = the larger of the two relative errors (0 where a side has no extra samples).
+// The extra rows / columns live in their own buffers (the first round's are stacked below R and
+// beside C in the round's storage; a re-check's are separate), so one kernel serves both.
+struct EstJob {
+    const void *C;    // m x >= r, ld m (the first r columns are C)
+    const void *R;    // >= r rows x n, ld ldr (the first r rows are R)
+    const double2 *U; // r x r
+    const void *Xr;   // Z(Ix, :): row e, column j at Xr[e + j * ldxr]
+    const void *Xc;   // Z(:, Jx): column c at Xc + c * m
+    const int *Ix, *Jx;
+    int m, n, r, ldr, ldxr, pe, pc;
+    double2 *T;       // scratch: C(Ix, :) U (pe x r), then U R(:, Jx) (r x pc)
+    double *out;      // est, then the four sums (rows num, den, cols num, den)
+};
+
 template <typename S>
-__global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restrict__ works) {
+__global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict__ jobs) {
     __shared__ double s_red[4][256];
-    const BlockWork w = works[blockIdx.x];
-    const int r = w.r, pe = w.pe, pc = w.pc, n = w.n, m = w.m, ldr = w.r + w.pe;
+    const EstJob w = jobs[blockIdx.x];
+    const int r = w.r, pe = w.pe, pc = w.pc, n = w.n, m = w.m, ldr = w.ldr, ldxr = w.ldxr;
     const S *C = reinterpret_cast<const S *>(w.C);
-    const S *Rx = reinterpret_cast<const S *>(w.Rx);
+    const S *Rm = reinterpret_cast<const S *>(w.R);
+    const S *Xr = reinterpret_cast<const S *>(w.Xr);
+    const S *Xc = reinterpret_cast<const S *>(w.Xc);
     double2 *Tr = w.T;             // pe x r
     double2 *Sc = w.T + pe * r;    // r x pc
     // Tr = C(Ix, :) U ; Sc = U R(:, Jx)
@@ -189,7 +257,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
             const int col = w.Jx[cc];
             for (int l = 0; l < r; ++l) {
                 const double2 u = w.U[k + (size_t)l * r];
-                const double2 rv = promote(Rx[l + (size_t)col * ldr]);
+                const double2 rv = promote(Rm[l + (size_t)col * ldr]);
                 sx = fma(u.x, rv.x, fma(-u.y, rv.y, sx));
                 sy = fma(u.x, rv.y, fma(u.y, rv.x, sy));
             }
@@ -203,7 +271,8 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
     constexpr int kEstChunk = 8;
     double nr_ = 0, dr_ = 0, nc_ = 0, dc_ = 0;
     for (int j = threadIdx.x; j < n; j += blockDim.x) {  // extra rows, column j
-        const S *col = Rx + (size_t)j * ldr;
+        const S *col = Rm + (size_t)j * ldr;
+        const S *xcol = Xr + (size_t)j * ldxr;
         for (int e0 = 0; e0 < pe; e0 += kEstChunk) {
             double zx[kEstChunk], zy[kEstChunk];
 #pragma unroll
@@ -222,7 +291,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
 #pragma unroll
             for (int q = 0; q < kEstChunk; ++q) {
                 if (e0 + q < pe) {
-                    const double2 x = promote(col[r + e0 + q]);
+                    const double2 x = promote(xcol[e0 + q]);
                     const double dx = x.x - zx[q], dy = x.y - zy[q];
                     nr_ = fma(dx, dx, fma(dy, dy, nr_));
                     dr_ = fma(x.x, x.x, fma(x.y, x.y, dr_));
@@ -249,7 +318,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
 #pragma unroll
             for (int q = 0; q < kEstChunk; ++q) {
                 if (c0 + q < pc) {
-                    const double2 x = promote(C[i + (size_t)(r + c0 + q) * m]);
+                    const double2 x = promote(Xc[i + (size_t)(c0 + q) * m]);
                     const double dx = x.x - zx[q], dy = x.y - zy[q];
                     nc_ = fma(dx, dx, fma(dy, dy, nc_));
                     dc_ = fma(x.x, x.x, fma(x.y, x.y, dc_));
@@ -270,13 +339,15 @@ __global__ void __launch_bounds__(256) estimate_kernel(const BlockWork *__restri
     if (threadIdx.x == 0) {
         const double er = s_red[1][0] > 0 ? sqrt(s_red[0][0] / s_red[1][0]) : 0.0;
         const double ec = s_red[3][0] > 0 ? sqrt(s_red[2][0] / s_red[3][0]) : 0.0;
-        *w.est = fmax(er, ec);
+        w.out[0] = fmax(er, ec);
+        for (int q = 0; q < 4; ++q) w.out[1 + q] = s_red[q][0];
     }
 }
 
 // per-block outcome gather: est, rank, svd status into one compact array for a single D2H
 struct RoundOut {
     double est;
+    double sums[4];  // residual and norm sums of the estimate (rows num, den, cols num, den)
     int rank;
     int status;
     int sweeps;  // Jacobi sweeps of the core SVD
@@ -286,7 +357,8 @@ __global__ void collect_kernel(const BlockWork *__restrict__ works, const SvdJob
                                int nb, RoundOut *out) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= nb) return;
-    out[b].est = *works[b].est;
+    out[b].est = works[b].est[0];
+    for (int q = 0; q < 4; ++q) out[b].sums[q] = works[b].est[1 + q];
     out[b].rank = *works[b].rank;
     out[b].status = svd[b].status;
     out[b].sweeps = svd[b].sweeps;
@@ -312,6 +384,33 @@ template <typename S>
 __global__ void promote_kernel(const S *in, double2 *out, long long n) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = promote(in[i]);
+}
+
+// ------------------------------------------------------------------ dense reference product
+// Y(rows_b, :) += Z_b X(cols_b, :) for the densely filled blocks of a batch (complex FP64):
+// one CTA per block, one (row, right-hand side) pair per thread and step, FP64 atomics into Y.
+struct DenseApply {
+    const double2 *Z;   // m x n, column-major
+    const int *rows, *cols;
+    int m, n;
+};
+__global__ void __launch_bounds__(256) dense_apply_kernel(const DenseApply *__restrict__ jobs,
+                                                          const double2 *__restrict__ X, int ldx,
+                                                          double2 *Y, int ldy, int nrhs) {
+    const DenseApply w = jobs[blockIdx.x];
+    for (int e = threadIdx.x; e < w.m * nrhs; e += blockDim.x) {
+        const int i = e % w.m, q = e / w.m;
+        double ax = 0, ay = 0;
+        for (int j = 0; j < w.n; ++j) {
+            const double2 z = w.Z[i + (size_t)j * w.m];
+            const double2 x = X[w.cols[j] + (size_t)q * ldx];
+            ax = fma(z.x, x.x, fma(-z.y, x.y, ax));
+            ay = fma(z.x, x.y, fma(z.y, x.x, ay));
+        }
+        double *y = reinterpret_cast<double *>(Y + w.rows[i] + (size_t)q * ldy);
+        atomicAdd(y, ax);
+        atomicAdd(y + 1, ay);
+    }
 }
 
 }  // namespace pskel
@@ -349,6 +448,7 @@ int ctx_ok(pskel_ctx *c) {
 
 size_t al16(size_t x) { return (x + 15) & ~size_t(15); }
 
+
 struct RoundPlan {
     std::vector<int> blocks;     // block ids of this round
     std::vector<int> r, pe, pc;
@@ -365,6 +465,7 @@ struct RoundPlan {
     int *d_svd_idx = nullptr;
     SvdPlan svd;
     PinvJob *d_pinv = nullptr;
+    EstJob *d_est = nullptr;
     int pinv_tiles = 0;
     int nb = 0;
 };
@@ -395,7 +496,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         s += al16(sizeof(int) * (r + pc));  // Jg
         s += al16(sizeof(double) * r);      // sigma
         s += al16(sizeof(int) * r);         // perm
-        s += 16 + 16;                       // rank, est
+        s += 16 + 64;                       // rank; est and its four sums
         off[i + 1] = off[i] + ((s + 255) & ~size_t(255));
         scratch_total += 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
     }
@@ -409,6 +510,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     if (tri_for(c, o.precision)) gfills.reserve(2 * nb);
     std::vector<SvdJob> svds(nb);
     std::vector<PinvJob> pinvs(nb);
+    std::vector<EstJob> ests(nb);
     char *kb = ar.keep.as<char>();
     char *sb = ar.work.as<char>();
     size_t soff = 0;
@@ -441,7 +543,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         w.sigma = reinterpret_cast<double *>(take(sizeof(double) * r));
         w.perm = reinterpret_cast<int *>(take(sizeof(int) * r));
         w.rank = reinterpret_cast<int *>(take(16));
-        w.est = reinterpret_cast<double *>(take(16));
+        w.est = reinterpret_cast<double *>(take(64));
         w.AV = reinterpret_cast<double2 *>(sb + soff);
         soff += al16(r * r * sizeof(double2));
         w.V = reinterpret_cast<double2 *>(sb + soff);
@@ -462,7 +564,18 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
                                           w.Ig, w.Rx, w.n, nts, w.r + w.pe, w.r + w.pe, 1, tri_cols_for(c, nts)});
         }
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
-        pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, o.tau, o.tau_relative};
+        // a block sampled on every row or every column of its smaller side cannot gain from more
+        // samples: its pinv keeps every singular value above full_tau of the largest, so that
+        // C U R reproduces the block instead of losing the truncated directions
+        double tau_i = o.tau;
+        int rel_i = o.tau_relative;
+        if (w.r >= std::min(w.m, w.n) && o.full_tau > 0) {
+            tau_i = rel_i ? std::min(o.tau, o.full_tau) : o.full_tau;
+            rel_i = 1;
+        }
+        pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, tau_i, rel_i};
+        ests[i] = EstJob{w.C, w.Rx, w.U, (const char *)w.Rx + r * es, (const char *)w.C + m * r * es,
+                         w.Ix, w.Jx, w.m, w.n, w.r, w.r + w.pe, w.r + w.pe, w.pe, w.pc, w.T, w.est};
         max_pinv_tiles = std::max(max_pinv_tiles, ((w.r + 31) / 32) * ((w.r + 31) / 32));
         res.m = w.m;
         res.n = w.n;
@@ -504,6 +617,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     const size_t o_svd = slot(sizeof(SvdJob) * nb);
     const size_t o_idx = slot(sizeof(int) * nb);
     const size_t o_pinv = slot(sizeof(PinvJob) * nb);
+    const size_t o_est = slot(sizeof(EstJob) * nb);
     ar.h_tables.assign(t, 0);
     std::memcpy(ar.h_tables.data() + o_works, works.data(), sizeof(BlockWork) * nb);
     if (p.tri)
@@ -514,6 +628,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     std::memcpy(ar.h_tables.data() + o_svd, svds.data(), sizeof(SvdJob) * nb);
     std::memcpy(ar.h_tables.data() + o_idx, svd_idx.data(), sizeof(int) * nb);
     std::memcpy(ar.h_tables.data() + o_pinv, pinvs.data(), sizeof(PinvJob) * nb);
+    std::memcpy(ar.h_tables.data() + o_est, ests.data(), sizeof(EstJob) * nb);
     PSKEL_TRY(ar.tables.reserve(t + 256));
     PSKEL_CUDA(cudaMemcpyAsync(ar.tables.ptr, ar.h_tables.data(), t, cudaMemcpyHostToDevice,
                                c->stream));
@@ -527,6 +642,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.d_svd = reinterpret_cast<SvdJob *>(d + o_svd);
     p.d_svd_idx = reinterpret_cast<int *>(d + o_idx);
     p.d_pinv = reinterpret_cast<PinvJob *>(d + o_pinv);
+    p.d_est = reinterpret_cast<EstJob *>(d + o_est);
     p.pinv_tiles = max_pinv_tiles;
     return PSKEL_OK;
 }
@@ -565,9 +681,9 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     PSKEL_TRY(batched_pinv(p.d_pinv, p.nb, p.pinv_tiles, s));
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));
     if (o.precision == PSKEL_C64)
-        estimate_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_works);
+        estimate_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_est);
     else
-        estimate_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
+        estimate_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_est);
     PSKEL_LAUNCHED(1);
     collect_kernel<<<(p.nb + 255) / 256, 256, 0, s>>>(p.d_works, p.d_svd, p.nb,
                                                      c->arenas[p.round].outs.as<RoundOut>());
@@ -577,6 +693,161 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
 }
 
 int set_kernel_attrs() { return ensure_smem_attr(sample_kernel, sample_smem()); }
+
+// Re-check of the blocks `sel` (indices into the round plan p) on fresh extra rows and
+// columns: sample, fill and estimate launches on the context's stream; out receives 5 doubles
+// per re-checked block (est on the new samples alone, then the four residual sums).
+int run_verify(pskel_ctx *c, const RoundPlan &p, const std::vector<int> &sel,
+               const pskel_opts_t &o, std::vector<double> &out, double *entries) {
+    const int nv = (int)sel.size();
+    out.assign(5 * (size_t)nv, 0.0);
+    if (nv == 0) return PSKEL_OK;
+    const size_t es = o.precision == PSKEL_C64 ? sizeof(float2) : sizeof(double2);
+    const std::vector<char> &h1 = c->arenas[p.round].h_tables;
+    const BlockWork *w1 = reinterpret_cast<const BlockWork *>(h1.data());  // the round's works
+    const size_t outs_bytes = (sizeof(double) * 8 * (size_t)nv + 255) & ~size_t(255);
+    std::vector<size_t> off(nv + 1, outs_bytes);
+    std::vector<int> pe2(nv), pc2(nv);
+    for (int v = 0; v < nv; ++v) {
+        const BlockWork &w = w1[sel[v]];
+        pe2[v] = std::max(0, std::min(o.extra_rows, w.m - w.r - w.pe));
+        pc2[v] = std::max(0, std::min(o.extra_cols, w.n - w.r - w.pc));
+        const size_t m = w.m, n = w.n, r = w.r;
+        size_t b = al16(m * pc2[v] * es) + al16((size_t)pe2[v] * n * es);
+        b += 4 * al16(sizeof(int) * (kMaxExtra + 1));
+        b += al16(sizeof(double2) * (pe2[v] + pc2[v]) * r);
+        off[v + 1] = off[v] + ((b + 255) & ~size_t(255));
+    }
+    PSKEL_TRY(c->verify_keep.reserve(off[nv] + 256));
+    std::vector<VerifyWork> vw(nv);
+    std::vector<EstJob> ej(nv);
+    std::vector<FillJob> fills;
+    std::vector<GroupFillJob> gfills;
+    const bool tri = tri_for(c, o.precision);
+    char *base = c->verify_keep.as<char>();
+    double *outs = reinterpret_cast<double *>(base);  // 8 doubles per re-checked block
+    double ent = 0;
+    for (int v = 0; v < nv; ++v) {
+        const int i = sel[v];
+        const BlockWork &w = w1[i];
+        const int b = w.block_id;
+        char *q = base + off[v];
+        auto take = [&](size_t bytes) { char *x = q; q += al16(bytes); return x; };
+        VerifyWork &x = vw[v];
+        x.rows_g = w.rows_g;
+        x.cols_g = w.cols_g;
+        x.I = w.I;
+        x.J = w.J;
+        x.Ix = w.Ix;
+        x.Jx = w.Jx;
+        x.m = w.m;
+        x.n = w.n;
+        x.r = w.r;
+        x.pe = w.pe;
+        x.pc = w.pc;
+        x.pe2 = pe2[v];
+        x.pc2 = pc2[v];
+        x.block_id = b;
+        x.round = w.round;
+        void *Xc = take((size_t)w.m * pc2[v] * es);
+        void *Xr = take((size_t)pe2[v] * w.n * es);
+        x.Ix2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+        x.Jx2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+        x.Ig2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+        x.Jg2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+        double2 *T = reinterpret_cast<double2 *>(take(sizeof(double2) * (pe2[v] + pc2[v]) * (size_t)w.r));
+        double *res = outs + 8 * (size_t)v;
+        ej[v] = EstJob{w.C, w.Rx, w.U, Xr, Xc, x.Ix2, x.Jx2, w.m, w.n, w.r, w.r + w.pe,
+                       std::max(pe2[v], 1), pe2[v], pc2[v], T, res};
+        ent += (double)w.m * pc2[v] + (double)pe2[v] * w.n;
+        const int gt = c->gt[b], gs = c->gs[b];
+        if (tri) {
+            const int *tr = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
+            const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
+            if (pc2[v] > 0)
+                gfills.push_back(GroupFillJob{w.rows_g, tr + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
+                                              x.Jg2, Xc, w.m, ntt, pc2[v], w.m, 0, tri_cols_for(c, ntt)});
+            if (pe2[v] > 0)
+                gfills.push_back(GroupFillJob{w.cols_g, tr + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
+                                              x.Ig2, Xr, w.n, nts, pe2[v], pe2[v], 1, tri_cols_for(c, nts)});
+        } else {
+            if (pc2[v] > 0) fills.push_back(FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2[v], w.m, 0});
+            if (pe2[v] > 0) fills.push_back(FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2[v], pe2[v], 1});
+        }
+    }
+    *entries = ent;
+    int tm, tn;
+    fill_tile_shape(o.precision, c->em.q_test, entry_split_for(c, o.precision), &tm, &tn);
+    const size_t nf = tri ? gfills.size() : fills.size();
+    std::vector<int> prefix(nf + 1, 0);
+    int max_rows = 0;
+    for (size_t f = 0; f < nf; ++f) {
+        if (tri) {
+            prefix[f + 1] = prefix[f] + (gfills[f].nc + gfills[f].tc - 1) / gfills[f].tc;
+            max_rows = std::max(max_rows, gfills[f].m);
+        } else {
+            prefix[f + 1] = prefix[f] + ((fills[f].nr + tm - 1) / tm) * ((fills[f].nc + tn - 1) / tn);
+        }
+    }
+    size_t t = 0;
+    auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
+    const size_t o_w = slot(sizeof(VerifyWork) * nv);
+    const size_t o_f = tri ? slot(sizeof(GroupFillJob) * (nf + 1)) : slot(sizeof(FillJob) * (nf + 1));
+    const size_t o_p = slot(sizeof(int) * prefix.size());
+    const size_t o_e = slot(sizeof(EstJob) * nv);
+    std::vector<char> &h = c->verify_h_tables;
+    h.assign(t, 0);
+    std::memcpy(h.data() + o_w, vw.data(), sizeof(VerifyWork) * nv);
+    if (tri) std::memcpy(h.data() + o_f, gfills.data(), sizeof(GroupFillJob) * nf);
+    else std::memcpy(h.data() + o_f, fills.data(), sizeof(FillJob) * nf);
+    std::memcpy(h.data() + o_p, prefix.data(), sizeof(int) * prefix.size());
+    std::memcpy(h.data() + o_e, ej.data(), sizeof(EstJob) * nv);
+    PSKEL_TRY(c->verify_tables.reserve(t + 256));
+    cudaStream_t s = c->stream;
+    PSKEL_CUDA(cudaMemcpyAsync(c->verify_tables.ptr, h.data(), t, cudaMemcpyHostToDevice, s));
+    char *d = c->verify_tables.as<char>();
+    verify_sample_kernel<<<nv, 128, 0, s>>>(reinterpret_cast<VerifyWork *>(d + o_w), o.seed);
+    PSKEL_LAUNCHED(1);
+    if (prefix.back() > 0) {
+        FillParams fp;
+        fp.k = c->em.k;
+        fp.eta = c->em.eta;
+        fp.r_near = 0.0;
+        fp.q_test = c->em.q_test;
+        fp.q_src = c->em.q_src;
+        fp.precision = o.precision;
+        fp.split = entry_split_for(c, o.precision);
+        fp.tri_cols = c->tri_cols;
+        fp.geom32 = c->geom32;
+        fp.max_rows = max_rows;
+        if (tri)
+            PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d + o_f),
+                                      reinterpret_cast<int *>(d + o_p), (int)nf, prefix.back(), s));
+        else
+            PSKEL_TRY(launch_fill(c->mesh, fp, reinterpret_cast<FillJob *>(d + o_f),
+                                  reinterpret_cast<int *>(d + o_p), (int)nf, prefix.back(),
+                                  c->flags.as<int>(), s));
+    }
+    if (o.precision == PSKEL_C64)
+        estimate_kernel<float2><<<nv, 256, 0, s>>>(reinterpret_cast<EstJob *>(d + o_e));
+    else
+        estimate_kernel<double2><<<nv, 256, 0, s>>>(reinterpret_cast<EstJob *>(d + o_e));
+    PSKEL_LAUNCHED(1);
+    std::vector<double> h_outs(8 * (size_t)nv);
+    PSKEL_CUDA(cudaMemcpyAsync(h_outs.data(), outs, sizeof(double) * 8 * nv, cudaMemcpyDeviceToHost, s));
+    PSKEL_CUDA(cudaStreamSynchronize(s));
+    for (int v = 0; v < nv; ++v)
+        for (int q = 0; q < 5; ++q) out[5 * (size_t)v + q] = h_outs[8 * (size_t)v + q];
+    return PSKEL_OK;
+}
+
+// Relative error from pooled residual sums (rows num, den, cols num, den): the larger side.
+double pooled_est(const double *a, const double *b) {
+    const double nr = a[0] + b[0], dr = a[1] + b[1], nc = a[2] + b[2], dc = a[3] + b[3];
+    const double er = dr > 0 ? std::sqrt(nr / dr) : 0.0;
+    const double ec = dc > 0 ? std::sqrt(nc / dc) : 0.0;
+    return std::max(er, ec);
+}
 
 }  // namespace
 
@@ -822,7 +1093,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         return PSKEL_ERR_STATE;
     }
     const pskel_opts_t o = *opts;
-    if (!(o.tol > 0) || o.tau < 0 || (o.precision != PSKEL_C128 && o.precision != PSKEL_C64) ||
+    if (!(o.tol > 0) || o.tau < 0 || o.full_tau < 0 || (o.precision != PSKEL_C128 && o.precision != PSKEL_C64) ||
         o.extra_rows < 0 || o.extra_rows > kMaxExtra || o.extra_cols < 0 ||
         o.extra_cols > kMaxExtra || o.max_rounds < 1 ||
         (o.start == PSKEL_START_GIVEN && !r0)) {
@@ -964,18 +1235,50 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
                 c->timing[1] += ms;  // graph replays are not split by phase
             }
         }
+        // re-check the blocks accepted with little margin (est within a factor est_verify of
+        // the acceptance threshold) on fresh extra rows and columns; they pass on the estimate
+        // pooled over both sample sets
+        std::vector<double> est(active.size());
+        for (size_t i = 0; i < active.size(); ++i) est[i] = hout[i].est;
+        if (o.est_verify > 1.0) {
+            std::vector<int> sel;
+            for (size_t i = 0; i < active.size(); ++i) {
+                const int b = active[i];
+                const bool pass = hout[i].status == PSKEL_OK && hout[i].est <= o.tol / safety;
+                const bool margin = hout[i].est <= o.tol / (safety * o.est_verify);
+                const bool more = mrows[b] - p.r[i] - p.pe[i] > 0 || ncols[b] - p.r[i] - p.pc[i] > 0;
+                if (pass && !margin && more && r_cur[b] < Dmin[b] && round + 1 < o.max_rounds)
+                    sel.push_back((int)i);
+            }
+            if (!sel.empty()) {
+                std::vector<double> vout;
+                double ent = 0;
+                PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+                PSKEL_TRY(run_verify(c, p, sel, o, vout, &ent));
+                PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
+                PSKEL_CUDA(cudaEventSynchronize(c->ev[4]));
+                float vms = 0;
+                cudaEventElapsedTime(&vms, c->ev[0], c->ev[4]);
+                c->timing[3] += vms;
+                c->timing[6] += ent;
+                c->timing[7] += ent * 4.0 * c->em.q_test * c->em.q_src;
+                c->timing[8] += 1;
+                for (size_t v = 0; v < sel.size(); ++v)
+                    est[sel[v]] = pooled_est(hout[sel[v]].sums, vout.data() + 5 * v + 1);
+            }
+        }
         std::vector<int> next;
         for (size_t i = 0; i < active.size(); ++i) {
             const int b = active[i];
             BlockResult &res = c->results[b];
-            res.est = hout[i].est;
+            res.est = est[i];
             res.rank = hout[i].rank;
             res.status = hout[i].status;
             c->timing[10] += hout[i].sweeps;
             c->timing[11] = std::max(c->timing[11], (double)hout[i].sweeps);
             c->timing[12] += 1;
             rounds_used[b] = round + 1;
-            const bool ok = hout[i].status == PSKEL_OK && hout[i].est <= o.tol / safety;
+            const bool ok = hout[i].status == PSKEL_OK && est[i] <= o.tol / safety;
             if (ok || r_cur[b] >= Dmin[b] || round + 1 >= o.max_rounds) continue;
             r_cur[b] = std::min(2 * r_cur[b], Dmin[b]);
             next.push_back(b);
@@ -1158,14 +1461,12 @@ extern "C" int pskel_get_block(pskel_ctx *c, int b, pskel_c128 *C, pskel_c128 *U
     return PSKEL_OK;
 }
 
-extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
-    PSKEL_TRY(ctx_ok(c));
-    if (!err || c->n_blocks <= 0) {
-        set_error(PSKEL_ERR_ARG, "true_errors: null output or no blocks");
-        return PSKEL_ERR_ARG;
-    }
-    const int nb = c->n_blocks;
-    for (int b = 0; b < nb; ++b)
+namespace {
+// ||Z_b - C_b U_b R_b||_F / ||Z_b||_F of the blocks in `list` (err[i] for list[i]), Z_b filled
+// densely in complex FP64, in batches of at most 2^28 dense entries.
+int true_errors_list(pskel_ctx *c, const std::vector<int> &list, double *err) {
+    const int nb = (int)list.size();
+    for (int b : list)
         if (c->results[b].arena < 0) {
             set_error(PSKEL_ERR_STATE, "true_errors: block %d has no retained factors (run the "
                                        "batched mode to keep every block)", b);
@@ -1179,7 +1480,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         size_t dense = 0, work = 0;
         int b1 = b0;
         while (b1 < nb) {
-            const BlockResult &res = c->results[b1];
+            const BlockResult &res = c->results[list[b1]];
             const BlockResult &pr = res.mirror >= 0 ? c->results[res.mirror] : res;  // factor storage
             const size_t d = (size_t)res.m * res.n;
             const size_t wsz = (size_t)res.r * res.n + (f32 ? (size_t)pr.m * pr.r + (size_t)(pr.r + pr.pe) * pr.n : 0);
@@ -1203,7 +1504,7 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         const bool tri = tri_for(c, PSKEL_C128);
         std::vector<int> prefix(nbb + 1, 0);
         for (int i = 0; i < nbb; ++i) {
-            const int b = b0 + i;
+            const int b = list[b0 + i];
             const BlockResult &res = c->results[b];
             const char *base = c->arenas[res.arena].keep.as<char>();
             double2 *Z = Zb + zo;
@@ -1305,6 +1606,127 @@ extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
         PSKEL_CUDA(cudaMemcpyAsync(ne.data(), d_ne, sizeof(double) * nbb, cudaMemcpyDeviceToHost, c->stream));
         PSKEL_CUDA(cudaStreamSynchronize(c->stream));
         for (int i = 0; i < nbb; ++i) err[b0 + i] = nz[i] > 0 ? ne[i] / nz[i] : 0.0;
+        b0 = b1;
+    }
+    return PSKEL_OK;
+}
+}  // namespace
+
+extern "C" int pskel_true_errors(pskel_ctx *c, double *err) {
+    PSKEL_TRY(ctx_ok(c));
+    if (!err || c->n_blocks <= 0) {
+        set_error(PSKEL_ERR_ARG, "true_errors: null output or no blocks");
+        return PSKEL_ERR_ARG;
+    }
+    std::vector<int> all(c->n_blocks);
+    std::iota(all.begin(), all.end(), 0);
+    return true_errors_list(c, all, err);
+}
+
+extern "C" int pskel_true_errors_blocks(pskel_ctx *c, const int *blocks, int n, double *err) {
+    PSKEL_TRY(ctx_ok(c));
+    if (!blocks || !err || n <= 0 || c->n_blocks <= 0) {
+        set_error(PSKEL_ERR_ARG, "true_errors_blocks: null argument or empty list");
+        return PSKEL_ERR_ARG;
+    }
+    std::vector<int> list(blocks, blocks + n);
+    for (int b : list)
+        if (b < 0 || b >= c->n_blocks) {
+            set_error(PSKEL_ERR_ARG, "true_errors_blocks: block %d out of range", b);
+            return PSKEL_ERR_ARG;
+        }
+    return true_errors_list(c, list, err);
+}
+
+extern "C" int pskel_dense_far_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy,
+                                      int nrhs) {
+    PSKEL_TRY(ctx_ok(c));
+    if (!X || !Y || nrhs <= 0 || ldx < c->mesh.ne || ldy < c->mesh.ne || c->n_blocks <= 0 ||
+        !c->have_mesh) {
+        set_error(PSKEL_ERR_ARG, "dense_far_matvec: bad arguments or no blocks");
+        return PSKEL_ERR_ARG;
+    }
+    const int nb = c->n_blocks;
+    PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(double2) * (size_t)ldy * nrhs, c->stream));
+    const size_t budget = (size_t)1 << 28;  // dense entries per batch
+    int tm, tn;
+    fill_tile_shape(PSKEL_C128, c->em.q_test, entry_split_for(c, PSKEL_C128), &tm, &tn);
+    const bool tri = tri_for(c, PSKEL_C128);
+    int b0 = 0;
+    while (b0 < nb) {
+        size_t dense = 0;
+        int b1 = b0;
+        while (b1 < nb) {
+            const size_t d = (size_t)(c->gptr[c->gt[b1] + 1] - c->gptr[c->gt[b1]]) *
+                             (c->gptr[c->gs[b1] + 1] - c->gptr[c->gs[b1]]);
+            if (b1 > b0 && dense + d > budget) break;
+            dense += d;
+            ++b1;
+        }
+        const int nbb = b1 - b0;
+        PSKEL_TRY(c->tmp.reserve(sizeof(double2) * dense + 256));
+        double2 *Zb = c->tmp.as<double2>();
+        std::vector<FillJob> fills(nbb);
+        std::vector<GroupFillJob> gfills(nbb);
+        std::vector<DenseApply> apps(nbb);
+        std::vector<int> prefix(nbb + 1, 0);
+        size_t zo = 0;
+        int max_rows = 0;
+        for (int i = 0; i < nbb; ++i) {
+            const int b = b0 + i, gt = c->gt[b], gs = c->gs[b];
+            const int m = c->gptr[gt + 1] - c->gptr[gt], n = c->gptr[gs + 1] - c->gptr[gs];
+            const int *rows = c->d_gids.as<int>() + c->gptr[gt], *cols = c->d_gids.as<int>() + c->gptr[gs];
+            double2 *Z = Zb + zo;
+            zo += (size_t)m * n;
+            fills[i] = FillJob{rows, cols, Z, m, n, m, 0};
+            const int nt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt];
+            gfills[i] = GroupFillJob{rows, c->d_gtri.as<int>() + c->gtri_ptr[gt],
+                                     c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt], cols, Z, m, nt,
+                                     n, m, 0, tri_cols_for(c, nt)};
+            prefix[i + 1] = prefix[i] + (tri ? (n + gfills[i].tc - 1) / gfills[i].tc
+                                             : ((m + tm - 1) / tm) * ((n + tn - 1) / tn));
+            apps[i] = DenseApply{Z, rows, cols, m, n};
+            max_rows = std::max(max_rows, m);
+        }
+        const size_t jb = std::max(sizeof(FillJob), sizeof(GroupFillJob)) * nbb;
+        PSKEL_TRY(c->tmp2.reserve(jb + sizeof(int) * (nbb + 1) + sizeof(DenseApply) * nbb + 4 * 256));
+        char *d = c->tmp2.as<char>();
+        size_t t = 0;
+        auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return d + x; };
+        void *d_f = slot(jb);
+        int *d_p = reinterpret_cast<int *>(slot(sizeof(int) * (nbb + 1)));
+        DenseApply *d_a = reinterpret_cast<DenseApply *>(slot(sizeof(DenseApply) * nbb));
+        if (tri)
+            PSKEL_CUDA(cudaMemcpyAsync(d_f, gfills.data(), sizeof(GroupFillJob) * nbb,
+                                       cudaMemcpyHostToDevice, c->stream));
+        else
+            PSKEL_CUDA(cudaMemcpyAsync(d_f, fills.data(), sizeof(FillJob) * nbb, cudaMemcpyHostToDevice,
+                                       c->stream));
+        PSKEL_CUDA(cudaMemcpyAsync(d_p, prefix.data(), sizeof(int) * (nbb + 1), cudaMemcpyHostToDevice,
+                                   c->stream));
+        PSKEL_CUDA(cudaMemcpyAsync(d_a, apps.data(), sizeof(DenseApply) * nbb, cudaMemcpyHostToDevice,
+                                   c->stream));
+        FillParams fp;
+        fp.k = c->em.k;
+        fp.eta = c->em.eta;
+        fp.r_near = 0;
+        fp.q_test = c->em.q_test;
+        fp.q_src = c->em.q_src;
+        fp.precision = PSKEL_C128;
+        fp.split = entry_split_for(c, PSKEL_C128);
+        fp.tri_cols = c->tri_cols;
+        fp.max_rows = max_rows;
+        if (tri)
+            PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d_f), d_p, nbb,
+                                      prefix.back(), c->stream));
+        else
+            PSKEL_TRY(launch_fill(c->mesh, fp, reinterpret_cast<FillJob *>(d_f), d_p, nbb, prefix.back(),
+                                  c->flags.as<int>(), c->stream));
+        dense_apply_kernel<<<nbb, 256, 0, c->stream>>>(d_a, reinterpret_cast<const double2 *>(X), ldx,
+                                                       reinterpret_cast<double2 *>(Y), ldy, nrhs);
+        PSKEL_LAUNCHED(1);
+        // the batch buffers are reused by the next batch
+        PSKEL_CUDA(cudaStreamSynchronize(c->stream));
         b0 = b1;
     }
     return PSKEL_OK;

@@ -95,6 +95,7 @@ struct StoreLayout {
     void *d_t1 = nullptr, *d_t2 = nullptr, *d_g1 = nullptr, *d_g2 = nullptr;
     bool ready = false;
     long long generation = -1;
+    int mode = PSKEL_STORE_BF16X3;  // operand format of the planes
 };
 
 struct pskel_ctx {
@@ -115,6 +116,8 @@ struct pskel_ctx {
     DevBuf d_gtri, d_gadj;
     bool use_tri = false;
     std::vector<RoundArena> arenas;
+    DevBuf verify_keep, verify_tables;  // re-check of blocks accepted with little margin
+    std::vector<char> verify_h_tables;
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;

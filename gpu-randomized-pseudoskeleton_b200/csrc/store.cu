@@ -11,14 +11,19 @@
 //
 // Complex products run as real GEMMs: A' = [Re A | Im A] (K doubled) times
 // B' = [[Re X, Im X]; [-Im X, Re X]] gives [Re(AX) | Im(AX)] (N = 2 x 16 = 32).
-// Precision: every real operand is split into bf16 hi + lo (hi = bf16(x), lo = bf16(x - hi));
-// the tensor cores accumulate hi*hi + hi*lo + lo*hi in FP32 (relative error about 1e-5).
+// Operand formats (pskel_store_build_mode), all accumulated in FP32 in TMEM:
+//   BF16X3 (default): every real operand split into bf16 hi + lo (hi = bf16(x), lo = bf16(x -
+//            hi)), hi*hi + hi*lo + lo*hi with tcgen05.mma kind::f16 (relative error ~1e-5);
+//   TF32:    one TF32 plane (x rounded to 10 mantissa bits), one product with kind::tf32
+//            (~5e-4 relative); the same bytes as BF16X3, a third of the MMAs;
+//   TF32X3:  TF32 hi + lo planes, three products with kind::tf32 (~1e-6 relative), twice the
+//            bytes.
 //
-// Layout: both operands are stored K-major in the canonical no-swizzle UMMA layout: chunks of
-// 8 consecutive K values (16 bytes) for all rows of a 128-row tile (A) or of the 32 columns (B),
-// so that one pipeline stage (64 K values) of a tile is one contiguous range of global memory,
-// fetched with one bulk copy (cp.async.bulk, the TMA engine's linear mode) per plane. The hi and
-// lo planes are two arrays of the same shape.
+// Layout: both operands are stored K-major in the canonical no-swizzle UMMA layout: 16-byte
+// chunks of consecutive K values (8 bf16 or 4 TF32) for all rows of a 128-row tile (A) or of the
+// 32 columns (B), so that one pipeline stage (8 chunks: 64 bf16 or 32 TF32 K values) of a tile is
+// one contiguous range of global memory, fetched with one bulk copy (cp.async.bulk, the TMA
+// engine's linear mode) per plane. The hi and lo planes are two arrays of the same shape.
 //
 // Kernel: one CTA of 128 threads per 128-row output tile. Warp 0 allocates 32 TMEM columns
 // (the 128 x 32 FP32 accumulator) and its lane 0 issues the bulk copies of a 4-stage ring;
@@ -40,30 +45,59 @@ namespace pskel {
 constexpr int kStTileM = 128;      // rows per output tile (UMMA M)
 constexpr int kStN = 32;           // real columns: 16 right-hand sides x (re, im)
 constexpr int kStRhs = 16;
-constexpr int kStStageK = 64;      // K values per pipeline stage (8 chunks of 8)
 constexpr int kStStages = 4;
-constexpr int kStChunkA = kStTileM * 8;  // bf16 elements per A chunk (128 rows x 8 K)
-constexpr int kStChunkB = kStN * 8;      // bf16 elements per B chunk (32 columns x 8 K)
-constexpr int kStStageABytes = 8 * kStChunkA * 2;  // 16 KB per plane
-constexpr int kStStageBBytes = 8 * kStChunkB * 2;  // 4 KB per plane
-constexpr int kStStageBytes = 2 * kStStageABytes + 2 * kStStageBBytes;
+constexpr int kStStageABytes = 8 * kStTileM * 16;  // 16 KB per plane: 8 chunks of 128 rows
+constexpr int kStStageBBytes = 8 * kStN * 16;      // 4 KB per plane: 8 chunks of 32 columns
+constexpr int kStStageBytes = 2 * kStStageABytes + 2 * kStStageBBytes;  // two planes at most
 constexpr size_t kStSmem = (size_t)kStStages * kStStageBytes + 1024;
 constexpr long long kStWaitLimit = 1ll << 22;  // try_wait polls before a wait counts as lost
 constexpr int kStSliceStages = 8;             // phase-2 K slice per work item (512 K values)
 
-// canonical offset (bf16 elements) of A(row, k) inside a group whose tiles have kc chunks each
+// Element type, elements per 16-byte chunk and planes of each format
+template <int MODE> struct StFmt;
+template <> struct StFmt<PSKEL_STORE_BF16X3> {
+    using E = __nv_bfloat16;
+    static constexpr int kEpc = 8, kPlanes = 2;
+};
+template <> struct StFmt<PSKEL_STORE_TF32> {
+    using E = float;
+    static constexpr int kEpc = 4, kPlanes = 1;
+};
+template <> struct StFmt<PSKEL_STORE_TF32X3> {
+    using E = float;
+    static constexpr int kEpc = 4, kPlanes = 2;
+};
+inline int st_epc(int mode) { return mode == PSKEL_STORE_BF16X3 ? 8 : 4; }
+inline int st_planes(int mode) { return mode == PSKEL_STORE_TF32 ? 1 : 2; }
+inline size_t st_esize(int mode) { return mode == PSKEL_STORE_BF16X3 ? 2 : 4; }
+
+// canonical offset (elements) of A(row, k) inside a group whose tiles have kc chunks each
+template <int EPC>
 __host__ __device__ __forceinline__ long long st_a_off(long long base, int kc, int row, int k) {
-    return base + (((long long)(row >> 7) * kc + (k >> 3)) * kStTileM + (row & 127)) * 8 + (k & 7);
+    return base + (((long long)(row >> 7) * kc + k / EPC) * kStTileM + (row & 127)) * EPC + k % EPC;
 }
 // canonical offset of B(col, k) (col < 32)
+template <int EPC>
 __host__ __device__ __forceinline__ long long st_b_off(long long base, int col, int k) {
-    return base + ((long long)(k >> 3) * kStN + col) * 8 + (k & 7);
+    return base + ((long long)(k / EPC) * kStN + col) * EPC + k % EPC;
 }
 
-__device__ __forceinline__ void split_bf16(float x, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
+// FP32 rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero; the
+// low 13 bits are cleared (finite inputs)
+__device__ __forceinline__ float tf32_round(float x) {
+    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
+}
+
+// x as the format's hi (and lo) plane values
+__device__ __forceinline__ void st_split(float x, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
     const __nv_bfloat16 h = __float2bfloat16_rn(x);
     *hi = h;
     *lo = __float2bfloat16_rn(x - __bfloat162float(h));
+}
+__device__ __forceinline__ void st_split(float x, float *hi, float *lo) {
+    const float h = tf32_round(x);
+    *hi = h;
+    if (lo) *lo = tf32_round(x - h);
 }
 
 // ---------------------------------------------------------------- pack (once per recompression)
@@ -79,9 +113,14 @@ struct PackBlock {
     int a2_kc, a2_col0, a2_K;  // a2_K: real K of the test group (imag parts start there)
 };
 
+template <int MODE>
 __global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__ blocks,
-                                                   __nv_bfloat16 *A1h, __nv_bfloat16 *A1l,
-                                                   __nv_bfloat16 *A2h, __nv_bfloat16 *A2l) {
+                                                   typename StFmt<MODE>::E *A1h,
+                                                   typename StFmt<MODE>::E *A1l,
+                                                   typename StFmt<MODE>::E *A2h,
+                                                   typename StFmt<MODE>::E *A2l) {
+    constexpr int EPC = StFmt<MODE>::kEpc;
+    const bool two = StFmt<MODE>::kPlanes == 2;
     const PackBlock w = blocks[blockIdx.x];
     // phase 1: rows S_i R'(i, :) of the source group's stack, [re | im] along K
     for (int e = threadIdx.x; e < w.k * w.n; e += blockDim.x) {
@@ -89,19 +128,19 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__
         const double2 v = w.trans ? w.Cp[j + (size_t)i * w.ldcp] : w.Rp[i + (size_t)j * w.r];
         const double s = w.S[i];
         const int row = w.a1_row0 + i;
-        const long long o_re = st_a_off(w.a1_base, w.a1_kc, row, j);
-        const long long o_im = st_a_off(w.a1_base, w.a1_kc, row, w.n + j);
-        split_bf16((float)(s * v.x), A1h + o_re, A1l + o_re);
-        split_bf16((float)(s * v.y), A1h + o_im, A1l + o_im);
+        const long long o_re = st_a_off<EPC>(w.a1_base, w.a1_kc, row, j);
+        const long long o_im = st_a_off<EPC>(w.a1_base, w.a1_kc, row, w.n + j);
+        st_split((float)(s * v.x), A1h + o_re, two ? A1l + o_re : nullptr);
+        st_split((float)(s * v.y), A1h + o_im, two ? A1l + o_im : nullptr);
     }
     // phase 2: columns C'(:, i) in the test group's stack
     for (int e = threadIdx.x; e < w.m * w.k; e += blockDim.x) {
         const int i = e % w.m, j = e / w.m;
         const double2 v = w.trans ? w.Rp[j + (size_t)i * w.r] : w.Cp[i + (size_t)j * w.ldcp];
-        const long long o_re = st_a_off(w.a2_base, w.a2_kc, i, w.a2_col0 + j);
-        const long long o_im = st_a_off(w.a2_base, w.a2_kc, i, w.a2_K + w.a2_col0 + j);
-        split_bf16((float)v.x, A2h + o_re, A2l + o_re);
-        split_bf16((float)v.y, A2h + o_im, A2l + o_im);
+        const long long o_re = st_a_off<EPC>(w.a2_base, w.a2_kc, i, w.a2_col0 + j);
+        const long long o_im = st_a_off<EPC>(w.a2_base, w.a2_kc, i, w.a2_K + w.a2_col0 + j);
+        st_split((float)v.x, A2h + o_re, two ? A2l + o_re : nullptr);
+        st_split((float)v.y, A2h + o_im, two ? A2l + o_im : nullptr);
     }
 }
 
@@ -115,12 +154,15 @@ struct StGroupB {
 
 // phase 1: B'(k, c) from X (complex64, column-major, ldx), columns >= nrhs are zero. One thread
 // per K index writes its 32 columns: eight consecutive K indices fill one 16-byte chunk row.
+template <int MODE>
 __global__ void __launch_bounds__(256) build_b1_kernel(const StGroupB *__restrict__ groups,
                                                        const float2 *__restrict__ X, int ldx,
-                                                       int nrhs, __nv_bfloat16 *Bh,
-                                                       __nv_bfloat16 *Bl) {
+                                                       int nrhs, typename StFmt<MODE>::E *Bh,
+                                                       typename StFmt<MODE>::E *Bl) {
+    constexpr int EPC = StFmt<MODE>::kEpc;
+    const bool two = StFmt<MODE>::kPlanes == 2;
     const StGroupB g = groups[blockIdx.x];
-    const int kpad = g.kc * 8;
+    const int kpad = g.kc * EPC;
     for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
         const bool in = k < 2 * g.K;
         const bool re_half = k < g.K;
@@ -131,20 +173,25 @@ __global__ void __launch_bounds__(256) build_b1_kernel(const StGroupB *__restric
             if (in && rhs < nrhs) x = X[id + (size_t)rhs * ldx];
             const float v0 = re_half ? x.x : -x.y;  // column rhs:      [re X; -im X]
             const float v1 = re_half ? x.y : x.x;   // column 16 + rhs: [im X;  re X]
-            const long long o0 = st_b_off(g.b_base, rhs, k), o1 = st_b_off(g.b_base, rhs + kStRhs, k);
-            split_bf16(v0, Bh + o0, Bl + o0);
-            split_bf16(v1, Bh + o1, Bl + o1);
+            const long long o0 = st_b_off<EPC>(g.b_base, rhs, k);
+            const long long o1 = st_b_off<EPC>(g.b_base, rhs + kStRhs, k);
+            st_split(v0, Bh + o0, two ? Bl + o0 : nullptr);
+            st_split(v1, Bh + o1, two ? Bl + o1 : nullptr);
         }
     }
 }
 
 // phase 2: B'(k, c) from the phase-1 rows T (32 floats per row: re of the 16 sides, then im);
 // one thread per K index reads its T row once
+template <int MODE>
 __global__ void __launch_bounds__(256) build_b2_kernel(const StGroupB *__restrict__ groups,
                                                        const float *__restrict__ T,
-                                                       __nv_bfloat16 *Bh, __nv_bfloat16 *Bl) {
+                                                       typename StFmt<MODE>::E *Bh,
+                                                       typename StFmt<MODE>::E *Bl) {
+    constexpr int EPC = StFmt<MODE>::kEpc;
+    const bool two = StFmt<MODE>::kPlanes == 2;
     const StGroupB g = groups[blockIdx.x];
-    const int kpad = g.kc * 8;
+    const int kpad = g.kc * EPC;
     for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
         const bool in = k < 2 * g.K;
         const bool re_half = k < g.K;
@@ -167,8 +214,8 @@ __global__ void __launch_bounds__(256) build_b2_kernel(const StGroupB *__restric
         for (int c = 0; c < kStN; ++c) {
             // [re T | im T] on the first K rows, [-im T | re T] on the second
             const float v = re_half ? t[c] : (c < kStRhs ? -t[c + kStRhs] : t[c - kStRhs]);
-            const long long o = st_b_off(g.b_base, c, k);
-            split_bf16(v, Bh + o, Bl + o);
+            const long long o = st_b_off<EPC>(g.b_base, c, k);
+            st_split(v, Bh + o, two ? Bl + o : nullptr);
         }
     }
 }
@@ -198,9 +245,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
     return d;                // base offset 0, absolute LBO mode, layout type 0 (no swizzle)
 }
 
-// instruction descriptor: kind::f16 with bf16 A and B, FP32 D, both K-major, M = 128, N = 32
-constexpr uint32_t kStIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kStN >> 3) << 17) |
-                              ((uint32_t)(kStTileM >> 4) << 24);
+// instruction descriptors, FP32 D, both operands K-major, M = 128, N = 32:
+// kind::f16 with bf16 A and B (format 1), kind::tf32 with TF32 A and B (format 2)
+constexpr uint32_t kStIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kStN >> 3) << 17) |
+                                  ((uint32_t)(kStTileM >> 4) << 24);
+constexpr uint32_t kStIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kStN >> 3) << 17) |
+                                  ((uint32_t)(kStTileM >> 4) << 24);
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
@@ -241,15 +291,26 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
         : "memory");
 }
 
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                          uint32_t accumulate) {
+// one MMA of the format: kind::f16 (bf16, K = 16) or kind::tf32 (K = 8); 32 bytes of K per row
+template <int MODE>
+__device__ __forceinline__ void umma_st(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                        uint32_t accumulate) {
     const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kStIdesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2),
-        "r"(mask3));
+    if constexpr (MODE == PSKEL_STORE_BF16X3) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(kStIdescBf16), "r"(accumulate), "r"(mask0), "r"(mask1),
+            "r"(mask2), "r"(mask3));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+            "l"(adesc), "l"(bdesc), "r"(kStIdescTf32), "r"(accumulate), "r"(mask0), "r"(mask1),
+            "r"(mask2), "r"(mask3));
+    }
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -269,11 +330,17 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
 //                   (phase 1: stores into T; phase 2: FP32 atomics into Y, the items of a tile
 //                   being K slices of it).
 // The two accumulators let the epilogue of one item overlap the MMAs of the next.
+template <int MODE>
 __global__ void __launch_bounds__(192, 1)
     store_gemm_kernel(const StItem *__restrict__ items, int nitems,
-                      const __nv_bfloat16 *__restrict__ Ah, const __nv_bfloat16 *__restrict__ Al,
-                      const __nv_bfloat16 *__restrict__ Bh, const __nv_bfloat16 *__restrict__ Bl,
+                      const typename StFmt<MODE>::E *__restrict__ Ah,
+                      const typename StFmt<MODE>::E *__restrict__ Al,
+                      const typename StFmt<MODE>::E *__restrict__ Bh,
+                      const typename StFmt<MODE>::E *__restrict__ Bl,
                       float *T, float *Y, int ldy, int nrhs, int *err) {
+    constexpr int EPC = StFmt<MODE>::kEpc;
+    constexpr bool kTwo = StFmt<MODE>::kPlanes == 2;
+    constexpr int kChunkA = kStTileM * EPC, kChunkB = kStN * EPC;  // elements per chunk block
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t full_bar[kStStages], empty_bar[kStStages];
     __shared__ __align__(8) uint64_t tfull_bar[2], tempty_bar[2], final_bar;
@@ -321,13 +388,16 @@ __global__ void __launch_bounds__(192, 1)
                         break;
                     }
                     unsigned char *st = ring + (size_t)slot * kStStageBytes;
-                    mbar_expect_tx(&full_bar[slot], kStStageBytes);
-                    const long long ao = w.a_off + (long long)s * 8 * kStChunkA;
-                    const long long bo = w.b_off + (long long)s * 8 * kStChunkB;
+                    mbar_expect_tx(&full_bar[slot], (kTwo ? 2 : 1) * (kStStageABytes + kStStageBBytes));
+                    const long long ao = w.a_off + (long long)s * 8 * kChunkA;
+                    const long long bo = w.b_off + (long long)s * 8 * kChunkB;
                     bulk_g2s(st, Ah + ao, kStStageABytes, &full_bar[slot]);
-                    bulk_g2s(st + kStStageABytes, Al + ao, kStStageABytes, &full_bar[slot]);
                     bulk_g2s(st + 2 * kStStageABytes, Bh + bo, kStStageBBytes, &full_bar[slot]);
-                    bulk_g2s(st + 2 * kStStageABytes + kStStageBBytes, Bl + bo, kStStageBBytes, &full_bar[slot]);
+                    if (kTwo) {
+                        bulk_g2s(st + kStStageABytes, Al + ao, kStStageABytes, &full_bar[slot]);
+                        bulk_g2s(st + 2 * kStStageABytes + kStStageBBytes, Bl + bo, kStStageBBytes,
+                                 &full_bar[slot]);
+                    }
                 }
             }
             // no copy may still be in flight when the CTA leaves
@@ -361,15 +431,18 @@ __global__ void __launch_bounds__(192, 1)
                     const uint32_t b_hi = smem_u32(st + 2 * kStStageABytes);
                     const uint32_t b_lo = smem_u32(st + 2 * kStStageABytes + kStStageBBytes);
 #pragma unroll
-                    for (int ks = 0; ks < 4; ++ks) {  // K = 16 per MMA: two chunks
-                        const uint32_t ao = ks * 2 * kStChunkA * 2, bo = ks * 2 * kStChunkB * 2;
-                        const uint64_t dah = umma_desc(a_hi + ao, kStChunkA * 2, 128);
-                        const uint64_t dal = umma_desc(a_lo + ao, kStChunkA * 2, 128);
-                        const uint64_t dbh = umma_desc(b_hi + bo, kStChunkB * 2, 128);
-                        const uint64_t dbl = umma_desc(b_lo + bo, kStChunkB * 2, 128);
-                        umma_bf16(d, dah, dbh, (s > 0 || ks > 0) ? 1u : 0u);
-                        umma_bf16(d, dah, dbl, 1u);
-                        umma_bf16(d, dal, dbh, 1u);
+                    for (int ks = 0; ks < 4; ++ks) {  // one MMA reads two chunks (32 bytes) of K
+                        // byte offsets: two chunk blocks of 128 rows (A) / 32 columns (B)
+                        const uint32_t ao = ks * 2 * kStTileM * 16, bo = ks * 2 * kStN * 16;
+                        const uint64_t dah = umma_desc(a_hi + ao, kStTileM * 16, 128);
+                        const uint64_t dbh = umma_desc(b_hi + bo, kStN * 16, 128);
+                        umma_st<MODE>(d, dah, dbh, (s > 0 || ks > 0) ? 1u : 0u);
+                        if (kTwo) {
+                            const uint64_t dal = umma_desc(a_lo + ao, kStTileM * 16, 128);
+                            const uint64_t dbl = umma_desc(b_lo + bo, kStN * 16, 128);
+                            umma_st<MODE>(d, dah, dbl, 1u);
+                            umma_st<MODE>(d, dal, dbh, 1u);
+                        }
                     }
                     umma_commit(&empty_bar[slot]);  // the slot is free once these MMAs have read it
                 }
@@ -444,15 +517,34 @@ __global__ void __launch_bounds__(192, 1)
 using namespace pskel;
 
 // ---------------------------------------------------------------- host side
-extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
+namespace {
+template <int MODE>
+void launch_pack(pskel_ctx *c, long long a1) {
+    using E = typename StFmt<MODE>::E;
+    E *ah = c->st_ah.as<E>(), *al = StFmt<MODE>::kPlanes == 2 ? c->st_al.as<E>() : nullptr;
+    pack_kernel<MODE><<<c->n_blocks, 256, 0, c->stream>>>(c->st_tab.as<PackBlock>(), ah, al, ah + a1,
+                                                          al ? al + a1 : nullptr);
+}
+}  // namespace
+
+extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) {
     if (!c || c->n_blocks <= 0 || (int)c->recomp_slots.size() != c->n_blocks) {
         set_error(PSKEL_ERR_STATE, "store_build: run pskel_recompress first");
         return PSKEL_ERR_STATE;
+    }
+    if (mode != PSKEL_STORE_BF16X3 && mode != PSKEL_STORE_TF32 && mode != PSKEL_STORE_TF32X3) {
+        set_error(PSKEL_ERR_ARG, "store_build: unknown operand format %d", mode);
+        return PSKEL_ERR_ARG;
     }
     PSKEL_CUDA(cudaSetDevice(c->device));
     const int nb = c->n_blocks, ng = c->n_groups;
     StoreLayout &L = c->store;
     L = StoreLayout();
+    L.mode = mode;
+    const int epc = st_epc(mode), planes = st_planes(mode);
+    const size_t esize = st_esize(mode);
+    const long long chunkA = (long long)kStTileM * epc, chunkB = (long long)kStN * epc;
+    const long long stageK = 8LL * epc;  // K values per pipeline stage
     std::vector<std::vector<int>> by_src(ng), by_test(ng);
     for (int b = 0; b < nb; ++b) {
         by_src[c->gs[b]].push_back(b);
@@ -472,7 +564,7 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
         for (int b : by_src[g]) K += c->recomp_slots[b].k;
         if (K == 0) continue;
         const int n = gsize(g);
-        const int kc = (int)(pad(2 * (long long)n, kStStageK) / 8);
+        const int kc = (int)(pad(2 * (long long)n, stageK) / epc);
         const int mpad = (int)pad(K, kStTileM);
         int row = 0;
         for (int b : by_src[g]) {
@@ -484,11 +576,11 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
             row += c->recomp_slots[b].k;
         }
         for (int mt = 0; mt < mpad / kStTileM; ++mt)
-            L.tiles1.push_back(StoreTile{a1 + (long long)mt * kc * kStChunkA, b1, kc,
+            L.tiles1.push_back(StoreTile{a1 + (long long)mt * kc * chunkA, b1, kc,
                                          std::min(kStTileM, K - mt * kStTileM), trow + mt * kStTileM, -1});
         L.groups1.push_back(StoreGroup{b1, kc, n, c->gptr[g], -1});
-        a1 += (long long)mpad * kc * 8;
-        b1 += (long long)kc * kStChunkB;
+        a1 += (long long)mpad * kc * epc;
+        b1 += (long long)kc * chunkB;
         trow += mpad;
     }
     // phase 2: per test group; the T row of every real K index
@@ -499,7 +591,7 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
         for (int b : by_test[g]) K += c->recomp_slots[b].k;
         if (K == 0) continue;
         const int m = gsize(g);
-        const int kc = (int)(pad(2 * (long long)K, kStStageK) / 8);
+        const int kc = (int)(pad(2 * (long long)K, stageK) / epc);
         const int mpad = (int)pad(m, kStTileM);
         const int map0 = (int)L.trow_map.size();
         int col = 0;
@@ -513,11 +605,11 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
             col += c->recomp_slots[b].k;
         }
         for (int mt = 0; mt < mpad / kStTileM; ++mt)
-            L.tiles2.push_back(StoreTile{a2 + (long long)mt * kc * kStChunkA, b2, kc,
+            L.tiles2.push_back(StoreTile{a2 + (long long)mt * kc * chunkA, b2, kc,
                                          std::min(kStTileM, m - mt * kStTileM), c->gptr[g] + mt * kStTileM, 1});
         L.groups2.push_back(StoreGroup{b2, kc, K, -1, map0});
-        a2 += (long long)mpad * kc * 8;
-        b2 += (long long)kc * kStChunkB;
+        a2 += (long long)mpad * kc * epc;
+        b2 += (long long)kc * chunkB;
     }
     for (int b = 0; b < nb; ++b) {
         const RecompSlot &sl = c->recomp_slots[b];
@@ -539,19 +631,22 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
     L.b2 = b2;
     L.trows = trow;
     // device buffers: A planes (phase 1 then phase 2), B planes, T, tables
-    const size_t abytes = (size_t)(a1 + a2) * 2;
+    const size_t abytes = (size_t)(a1 + a2) * esize;
     PSKEL_TRY(c->st_ah.reserve(abytes));
-    PSKEL_TRY(c->st_al.reserve(abytes));
-    PSKEL_TRY(c->st_bh.reserve((size_t)(b1 + b2) * 2 + 256));
-    PSKEL_TRY(c->st_bl.reserve((size_t)(b1 + b2) * 2 + 256));
+    PSKEL_TRY(c->st_bh.reserve((size_t)(b1 + b2) * esize + 256));
+    if (planes == 2) {
+        PSKEL_TRY(c->st_al.reserve(abytes));
+        PSKEL_TRY(c->st_bl.reserve((size_t)(b1 + b2) * esize + 256));
+    }
     PSKEL_TRY(c->st_t.reserve((size_t)std::max(trow, 1) * kStN * sizeof(float)));
     PSKEL_CUDA(cudaMemsetAsync(c->st_ah.ptr, 0, abytes, c->stream));
-    PSKEL_CUDA(cudaMemsetAsync(c->st_al.ptr, 0, abytes, c->stream));
+    if (planes == 2) PSKEL_CUDA(cudaMemsetAsync(c->st_al.ptr, 0, abytes, c->stream));
     PSKEL_TRY(c->st_tab.reserve(sizeof(PackBlock) * nb + 256));
     PSKEL_CUDA(cudaMemcpyAsync(c->st_tab.ptr, pb.data(), sizeof(PackBlock) * nb, cudaMemcpyHostToDevice,
                                c->stream));
-    __nv_bfloat16 *ah = c->st_ah.as<__nv_bfloat16>(), *al = c->st_al.as<__nv_bfloat16>();
-    pack_kernel<<<nb, 256, 0, c->stream>>>(c->st_tab.as<PackBlock>(), ah, al, ah + a1, al + a1);
+    if (mode == PSKEL_STORE_BF16X3) launch_pack<PSKEL_STORE_BF16X3>(c, a1);
+    else if (mode == PSKEL_STORE_TF32) launch_pack<PSKEL_STORE_TF32>(c, a1);
+    else launch_pack<PSKEL_STORE_TF32X3>(c, a1);
     PSKEL_LAUNCHED(1);
     // device tile and group tables (pointers resolved here)
     const int *gids = c->d_gids.as<int>();
@@ -566,8 +661,8 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
         t1.push_back(StItem{t.a_off, t.b_off, t.kc / 8, t.rows, t.out0, nullptr});
     for (const StoreTile &t : L.tiles2)
         for (int s0 = 0; s0 < t.kc / 8; s0 += kStSliceStages)
-            t2.push_back(StItem{a1 + t.a_off + (long long)s0 * 8 * kStChunkA,
-                                b1 + t.b_off + (long long)s0 * 8 * kStChunkB,
+            t2.push_back(StItem{a1 + t.a_off + (long long)s0 * 8 * chunkA,
+                                b1 + t.b_off + (long long)s0 * 8 * chunkB,
                                 std::min(kStSliceStages, t.kc / 8 - s0), t.rows, 0, gids + t.out0});
     L.n_items1 = (int)t1.size();
     L.n_items2 = (int)t2.size();
@@ -591,9 +686,54 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
     L.ready = true;
     L.generation = c->generation;
-    if (bytes) *bytes = (long long)(2 * abytes);
+    if (bytes) *bytes = (long long)(planes * abytes);
     return PSKEL_OK;
 }
+
+extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
+    return pskel_store_build_mode(c, PSKEL_STORE_BF16X3, bytes);
+}
+
+namespace {
+// The four launches of one matvec over a store of format MODE (Y cleared by the caller).
+template <int MODE>
+int store_matvec_t(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
+                   cudaStream_t st) {
+    using E = typename StFmt<MODE>::E;
+    const bool two = StFmt<MODE>::kPlanes == 2;
+    const StoreLayout &L = c->store;
+    PSKEL_TRY(ensure_smem_attr(store_gemm_kernel<MODE>, kStSmem));
+    E *ah = c->st_ah.as<E>(), *al = two ? c->st_al.as<E>() : nullptr;
+    E *bh = c->st_bh.as<E>(), *bl = two ? c->st_bl.as<E>() : nullptr;
+    int *err = c->st_err.as<int>();
+    const int n1 = L.n_items1, n2 = L.n_items2;
+    const int ng1 = (int)L.groups1.size(), ng2 = (int)L.groups2.size();
+    const int sms = sm_count();
+    if (ng1 > 0) {
+        build_b1_kernel<MODE><<<ng1, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g1),
+                                                   reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl);
+        PSKEL_LAUNCHED(1);
+    }
+    if (n1 > 0) {
+        store_gemm_kernel<MODE><<<std::min(n1, sms), 192, kStSmem, st>>>(
+            reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<float>(), nullptr, 0,
+            kStRhs, err);
+        PSKEL_LAUNCHED(1);
+    }
+    if (ng2 > 0) {
+        build_b2_kernel<MODE><<<ng2, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g2),
+                                                   c->st_t.as<float>(), bh, bl);
+        PSKEL_LAUNCHED(1);
+    }
+    if (n2 > 0) {
+        store_gemm_kernel<MODE><<<std::min(n2, sms), 192, kStSmem, st>>>(
+            reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr,
+            reinterpret_cast<float *>(Y), ldy, nrhs, err);
+        PSKEL_LAUNCHED(1);
+    }
+    return PSKEL_OK;
+}
+}  // namespace
 
 extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
                                   void *stream) {
@@ -608,39 +748,12 @@ extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y,
     }
     PSKEL_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    PSKEL_TRY(ensure_smem_attr(store_gemm_kernel, kStSmem));
     PSKEL_TRY(c->st_err.reserve(256));
     PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
     PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));
-    __nv_bfloat16 *ah = c->st_ah.as<__nv_bfloat16>(), *al = c->st_al.as<__nv_bfloat16>();
-    __nv_bfloat16 *bh = c->st_bh.as<__nv_bfloat16>(), *bl = c->st_bl.as<__nv_bfloat16>();
-    int *err = c->st_err.as<int>();
-    const int n1 = L.n_items1, n2 = L.n_items2;
-    const int ng1 = (int)L.groups1.size(), ng2 = (int)L.groups2.size();
-    const int sms = sm_count();
-    if (ng1 > 0) {
-        build_b1_kernel<<<ng1, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g1),
-                                             reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl);
-        PSKEL_LAUNCHED(1);
-    }
-    if (n1 > 0) {
-        store_gemm_kernel<<<std::min(n1, sms), 192, kStSmem, st>>>(
-            reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<float>(), nullptr, 0,
-            kStRhs, err);
-        PSKEL_LAUNCHED(1);
-    }
-    if (ng2 > 0) {
-        build_b2_kernel<<<ng2, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g2),
-                                             c->st_t.as<float>(), bh, bl);
-        PSKEL_LAUNCHED(1);
-    }
-    if (n2 > 0) {
-        store_gemm_kernel<<<std::min(n2, sms), 192, kStSmem, st>>>(
-            reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr,
-            reinterpret_cast<float *>(Y), ldy, nrhs, err);
-        PSKEL_LAUNCHED(1);
-    }
-    return PSKEL_OK;
+    if (L.mode == PSKEL_STORE_BF16X3) return store_matvec_t<PSKEL_STORE_BF16X3>(c, X, ldx, Y, ldy, nrhs, st);
+    if (L.mode == PSKEL_STORE_TF32) return store_matvec_t<PSKEL_STORE_TF32>(c, X, ldx, Y, ldy, nrhs, st);
+    return store_matvec_t<PSKEL_STORE_TF32X3>(c, X, ldx, Y, ldy, nrhs, st);
 }
 
 extern "C" int pskel_store_status(pskel_ctx *c, int *error_word) {

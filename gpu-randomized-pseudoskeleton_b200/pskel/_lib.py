@@ -42,7 +42,7 @@ class Opts(ctypes.Structure):
                 ("start", ci), ("oversample", ci), ("extra_rows", ci), ("extra_cols", ci),
                 ("max_rounds", ci), ("recompress", ci), ("seed", ctypes.c_uint64),
                 ("recompress_tol", cd), ("est_safety", cd), ("use_graph", ci),
-                ("per_block", ci)]
+                ("per_block", ci), ("est_verify", cd), ("full_tau", cd)]
 
 
 class BlockStat(ctypes.Structure):
@@ -79,6 +79,8 @@ SIGNATURES = {
     "pskel_last_timing": (ci, [VP, D, ci]),
     "pskel_get_block": (ci, [VP, ci, VP, VP, VP, I32, I32]),
     "pskel_true_errors": (ci, [VP, D]),
+    "pskel_true_errors_blocks": (ci, [VP, I32, ci, D]),
+    "pskel_dense_far_matvec": (ci, [VP, VP, ci, VP, ci, ci]),
     "pskel_set_fill_split": (ci, [VP, ci, ci]),
     "pskel_set_tri_cols": (ci, [VP, ci]),
     "pskel_set_fill_geometry": (ci, [VP, ci]),
@@ -98,6 +100,7 @@ SIGNATURES = {
     "pskel_recompress": (ci, [VP, cd, I32]),
     "pskel_get_recompressed": (ci, [VP, ci, VP, D, VP]),
     "pskel_store_build": (ci, [VP, ctypes.POINTER(ctypes.c_longlong)]),
+    "pskel_store_build_mode": (ci, [VP, ci, ctypes.POINTER(ctypes.c_longlong)]),
     "pskel_store_matvec": (ci, [VP, VP, ci, VP, ci, ci, VP]),
     "pskel_store_status": (ci, [VP, I32]),
     "pskel_mlp_num_params": (ci, []),

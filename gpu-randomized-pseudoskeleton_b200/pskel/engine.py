@@ -138,11 +138,19 @@ class Engine:
     # ------------------------------------------------------------------ compression
     def compress(self, tol: float, *, precision="c128", tau: float = 1e-8, tau_relative=True,
                  r0=None, oversample: int = 10, extra_rows: int = 16, extra_cols: int = 16,
-                 est_safety: float = 2.0, max_rounds: int = 12, seed: int = 0,
+                 est_safety: float = 2.0, est_verify: float = 2.0, full_tau: float = 1e-10,
+                 max_rounds: int = 12,
+                 seed: int = 0,
                  use_graph: bool = False, recompress: bool = False,
                  recompress_tol: float = 0.0, per_block: bool = False) -> np.ndarray:
         """Compress every block; returns a structured array of per-block stats
-        (m, n, r, rank, rank_recompressed, rounds, status, est)."""
+        (m, n, r, rank, rank_recompressed, rounds, status, est).
+
+        A block passes when its randomized estimate est <= tol / est_safety; a block that
+        passes with est above tol / (est_safety * est_verify) is re-checked on a second set of
+        extra rows and columns and passes on the pooled estimate (est_verify <= 1: no
+        re-check). A block sampled on its whole smaller side (r = min(m, n)) uses the pinv
+        threshold min(tau, full_tau) (relative; full_tau = 0: tau)."""
         o = _lib.Opts(tol=tol, tau=tau, tau_relative=int(bool(tau_relative)),
                       precision=_prec(precision),
                       start=START_GIVEN if r0 is not None else START_REFERENCE,
@@ -150,7 +158,8 @@ class Engine:
                       extra_cols=int(extra_cols), max_rounds=int(max_rounds),
                       recompress=int(recompress), seed=int(seed),
                       recompress_tol=float(recompress_tol), est_safety=float(est_safety),
-                      use_graph=int(bool(use_graph)), per_block=int(bool(per_block)))
+                      use_graph=int(bool(use_graph)), per_block=int(bool(per_block)),
+                      est_verify=float(est_verify), full_tau=float(full_tau))
         nb = self.n_blocks
         stats = (_lib.BlockStat * nb)()
         if r0 is not None:
@@ -189,10 +198,34 @@ class Engine:
                                              I.ctypes.data_as(_lib.I32), J.ctypes.data_as(_lib.I32)))
         return C, U, R, I, J
 
-    def true_errors(self) -> np.ndarray:
-        err = np.zeros(self.n_blocks)
-        _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
+    def true_errors(self, blocks=None) -> np.ndarray:
+        """Each block's ||Z - C U R||_F / ||Z||_F against its dense FP64 fill (all blocks, or
+        the listed ones in that order)."""
+        if blocks is None:
+            err = np.zeros(self.n_blocks)
+            _lib.check(self._lib.pskel_true_errors(self._h, err.ctypes.data_as(_lib.D)))
+            return err
+        bl = np.ascontiguousarray(blocks, dtype=np.int32)
+        err = np.zeros(len(bl))
+        _lib.check(self._lib.pskel_true_errors_blocks(self._h, bl.ctypes.data_as(_lib.I32), len(bl),
+                                                      err.ctypes.data_as(_lib.D)))
         return err
+
+    def dense_far_matvec(self, X):
+        """Dense reference of the far-field product, every block filled in complex FP64:
+        X is a complex128 CUDA tensor (RWG count, nrhs); returns Y of the same shape."""
+        import torch
+        if X.dim() == 1:
+            return self.dense_far_matvec(X[:, None])[:, 0]
+        if X.dtype != torch.complex128 or not X.is_cuda:
+            raise ValueError("X must be a complex128 CUDA tensor")
+        ne, nrhs = X.shape
+        Xc = X.t().contiguous()
+        Y = torch.empty_like(Xc)
+        torch.cuda.synchronize(X.device)
+        _lib.check(self._lib.pskel_dense_far_matvec(self._h, ctypes.c_void_p(Xc.data_ptr()), ne,
+                                                    ctypes.c_void_p(Y.data_ptr()), ne, nrhs))
+        return Y.t()
 
     def matvec(self, X, precision=None):
         """Compressed far-field product Y = sum_b C_b U_b R_b X over all blocks of the last
@@ -221,6 +254,11 @@ class Engine:
         self._recomp_k = k
         return k
 
+    def recompress_ms(self) -> float:
+        """Device time of the last recompress() (ms, between the library's events on its
+        stream)."""
+        return float(self.timing()["recompress"])
+
     def get_recompressed(self, b: int):
         """(C', S, R') of block b after recompress()."""
         rows, cols = self.block_ids(b)
@@ -233,10 +271,15 @@ class Engine:
                                                     vp(Rp)))
         return Cp, S, Rp
 
-    def build_store(self) -> int:
-        """Compressed store of the recompressed blocks (after recompress()); returns its bytes."""
+    STORE_MODES = {"bf16x3": 0, "tf32": 1, "tf32x3": 2}
+
+    def build_store(self, mode: str = "bf16x3") -> int:
+        """Compressed store of the recompressed blocks (after recompress()) in the operand
+        format mode: "bf16x3" (bf16 hi + lo, three products), "tf32" (one TF32 plane, one
+        product) or "tf32x3" (TF32 hi + lo, three products); returns its bytes."""
         nbytes = ctypes.c_longlong()
-        _lib.check(self._lib.pskel_store_build(self._h, ctypes.byref(nbytes)))
+        _lib.check(self._lib.pskel_store_build_mode(self._h, self.STORE_MODES[mode],
+                                                    ctypes.byref(nbytes)))
         return int(nbytes.value)
 
     def store_matvec(self, X):

@@ -195,6 +195,15 @@ typedef struct {
                             block; the kernels, samples and results per block are those of the
                             batched mode, but only the stats are kept (factors of the last block
                             only) */
+    double est_verify;   /* > 1: a block that passes with est in (tol / (est_safety * est_verify),
+                            tol / est_safety] is re-checked on a second, independent set of extra
+                            rows and columns (drawn outside all of its samples, Philox streams 4
+                            and 5 of its round) and passes only if the estimate pooled over both
+                            sets does; <= 1: no re-check. */
+    double full_tau;     /* > 0: relative pinv threshold of a block sampled on its whole smaller
+                            side (r = min(m, n)), where more samples cannot help: the smaller of
+                            tau and full_tau (e.g. 1e-10, so that C U R reproduces the block);
+                            0: tau there too */
 } pskel_opts_t;
 
 /* Per-block outcome, filled by pskel_compress_blocks. */
@@ -206,7 +215,8 @@ typedef struct {
     int rounds;          /* sampling rounds used (1 = first guess accepted) */
     int status;          /* PSKEL_OK or a negative status */
     double est;          /* randomized error estimate of the final round: the larger of the
-                            relative errors on the extra rows and on the extra columns */
+                            relative errors on the extra rows and on the extra columns (pooled
+                            over both sample sets for a re-checked block) */
 } pskel_block_stat_t;
 
 int pskel_create(pskel_ctx **ctx, int device);
@@ -246,8 +256,9 @@ int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r
                           pskel_block_stat_t *stats);
 
 /* Timing and work counters of the last pskel_compress_blocks call: out[0..5] = device ms of
-   the phases sample, fill, pinv, estimate, recompress and the whole call (a round replayed
-   from a CUDA graph is booked under fill as a whole); out[6] = entries filled, out[7] =
+   the phases sample, fill, pinv, estimate (re-checks included), recompress (set by the last
+   pskel_recompress after the compression) and the whole call (a round replayed from a CUDA
+   graph is booked under fill as a whole); out[6] = entries filled, out[7] =
    point pairs evaluated, out[8] = fill launches, out[9] = rounds, out[10] = mean and out[11] =
    maximum Jacobi sweeps of the core SVDs. n = length of out (<= 12). */
 int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
@@ -367,6 +378,15 @@ int pskel_octree_get(pskel_ctx *ctx, int *group_ptr, int *group_ids, double *cen
 /* Relative Frobenius error of every block against a dense FP64 fill (device-side, block by
    block); err (host, n_blocks). */
 int pskel_true_errors(pskel_ctx *ctx, double *err);
+/* The same for the n blocks listed in blocks (host, 0-based): err[i] is block blocks[i]'s error
+   (for a sample of a workload whose full dense fill would take long). */
+int pskel_true_errors_blocks(pskel_ctx *ctx, const int *blocks, int n, double *err);
+
+/* Dense reference of the far-field product: Y = sum over far blocks of Z_b X(cols_b) with every
+   block filled densely in complex FP64 (the same rule as the compression), for checking a
+   compressed product. X, Y: DEVICE pskel_c128 arrays (RWG count x nrhs, column-major, ldx and
+   ldy >= RWG count); Y is overwritten. Runs on the context's stream and waits for it. */
+int pskel_dense_far_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int nrhs);
 
 /* Compressed far-field matvec over every block of the last compression:
    Y(:, j) = sum_b P_t(b) C_b U_b R_b P_s(b)^T X(:, j), j < nrhs <= 64, with P_t, P_s the
@@ -383,7 +403,8 @@ int pskel_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int n
 
 /* Recompression of every block's C U R into an SVD-truncated C' diag(S) R' (k terms kept,
    S > thresh * S_max), in FP64: the restatement of codes/ACA_vs_CUR/seed/svd_compress.m:19-33
-   with its two QR factorisations replaced by one-sided Jacobi on C and R^H. ranks (host,
+   (Householder QR of C and R^H in place of its unshipped qr_cbd, the QR-preconditioned Jacobi
+   SVD of the r x r core R_c U R_r^H, the reflectors applied to the kept vectors). ranks (host,
    n_blocks, may be NULL) receives k per block. The factors stay on the device until the next
    compression. */
 int pskel_recompress(pskel_ctx *ctx, double thresh, int *ranks);
@@ -393,15 +414,22 @@ int pskel_recompress(pskel_ctx *ctx, double thresh, int *ranks);
 int pskel_get_recompressed(pskel_ctx *ctx, int b, pskel_c128 *Cp, double *S, pskel_c128 *Rp);
 
 /* Compressed store of the recompressed blocks for the tensor-core matvec: diag(S) R' of the
-   blocks stacked per source group and C' stacked per test group, each real value split into a
-   bf16 hi + lo pair, in 128-row tiles laid out for the tensor cores. Requires pskel_recompress
-   after the last compression. bytes (may be NULL) receives the size of the two planes. No
-   reference counterpart (the reference keeps each block's C, U, R apart). */
+   blocks stacked per source group and C' stacked per test group, in 128-row tiles laid out for
+   the tensor cores, each real value in the operand format `mode`:
+     PSKEL_STORE_BF16X3  bf16 hi + lo planes, three bf16 products per step (about 1e-5);
+     PSKEL_STORE_TF32    one TF32 plane, one TF32 product (about 5e-4; the same bytes);
+     PSKEL_STORE_TF32X3  TF32 hi + lo planes, three TF32 products (about 1e-6; twice the bytes).
+   Requires pskel_recompress after the last compression. bytes (may be NULL) receives the size
+   of the planes. No reference counterpart (the reference keeps each block's C, U, R apart). */
+#define PSKEL_STORE_BF16X3 0
+#define PSKEL_STORE_TF32 1
+#define PSKEL_STORE_TF32X3 2
+int pskel_store_build_mode(pskel_ctx *ctx, int mode, long long *bytes);
+/* pskel_store_build_mode with PSKEL_STORE_BF16X3. */
 int pskel_store_build(pskel_ctx *ctx, long long *bytes);
 
 /* Y = sum over far blocks of C' diag(S) R' X for nrhs <= 16 right-hand sides, as two grouped
-   GEMMs on the tensor cores (tcgen05, bf16 hi/lo split, FP32 accumulation; relative error about
-   1e-5). X (ldx >= RWG count) and Y (ldy >= RWG count) are DEVICE arrays of pskel_c64,
+   GEMMs on the tensor cores (tcgen05 in the store's operand format, FP32 accumulation). X (ldx >= RWG count) and Y (ldy >= RWG count) are DEVICE arrays of pskel_c64,
    column-major; Y is overwritten. Enqueued on stream (NULL: the legacy default stream);
    returns without waiting. Replaces, for the recompressed blocks, the per-block C(U(R v)) of
    user_impedance_for_julia_cuda.cu:1929-1960. */

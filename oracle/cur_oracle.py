@@ -126,32 +126,60 @@ def cuda_cur_compress3(fill, rows, cols, tol, rng, pinv_tol=1e-10):
     return C, U, R, err, sizes
 
 
+def _residual_sums(approx, Z):
+    """(||Z - approx||_F^2, ||Z||_F^2)."""
+    return float(np.linalg.norm(Z - approx) ** 2), float(np.linalg.norm(Z) ** 2)
+
+
+def extra_row_sums(C, U, R, Zx, Ix):
+    """Residual and norm sums on extra rows Ix (local ids, not in I)."""
+    if len(Ix) == 0:
+        return 0.0, 0.0
+    return _residual_sums((C[Ix, :] @ U) @ R, Zx)
+
+
+def extra_col_sums(C, U, R, Zc, Jx):
+    """Residual and norm sums on extra columns Jx (local ids, not in J)."""
+    if len(Jx) == 0:
+        return 0.0, 0.0
+    return _residual_sums(C @ (U @ R[:, Jx]), Zc)
+
+
+def est_from_sums(nr, dr, nc, dc):
+    """The larger of the relative errors on the extra rows and on the extra columns (0 for a
+    side without extra samples)."""
+    er = np.sqrt(nr / dr) if dr > 0 else 0.0
+    ec = np.sqrt(nc / dc) if dc > 0 else 0.0
+    return float(max(er, ec))
+
+
 def extra_row_estimate(C, U, R, Zx, Ix):
     """Relative error on extra rows Ix (local ids, not in I):
     ||Z(Ix,:) - C(Ix,:) U R||_F / ||Z(Ix,:)||_F; 0 when there are none."""
-    if len(Ix) == 0:
-        return 0.0
-    approx = (C[Ix, :] @ U) @ R
-    den = np.linalg.norm(Zx)
-    return float(np.linalg.norm(Zx - approx) / den) if den > 0 else 0.0
+    return est_from_sums(*extra_row_sums(C, U, R, Zx, Ix), 0.0, 0.0)
 
 
 def extra_col_estimate(C, U, R, Zc, Jx):
     """Relative error on extra columns Jx (local ids, not in J):
     ||Z(:,Jx) - C U R(:,Jx)||_F / ||Z(:,Jx)||_F; 0 when there are none."""
-    if len(Jx) == 0:
-        return 0.0
-    approx = C @ (U @ R[:, Jx])
-    den = np.linalg.norm(Zc)
-    return float(np.linalg.norm(Zc - approx) / den) if den > 0 else 0.0
+    return est_from_sums(0.0, 0.0, *extra_col_sums(C, U, R, Zc, Jx))
 
 
 def plain_adaptive(fill, rows, cols, tol, block_id, seed, extra_rows=16, extra_cols=16,
-                   safety=2.0, tau=1e-8, relative=True, r0=None, max_rounds=12):
+                   safety=2.0, tau=1e-8, relative=True, r0=None, max_rounds=12, verify=2.0,
+                   full_tau=1e-10):
     """Plain adaptive pseudoskeleton with seeded sampling and the randomized estimate: start at
     r0 (default D/10), double until max(extra-row, extra-column relative error) <= tol/safety
     or r = D. Index sets come from the same Philox/Floyd definition as the device sampler
-    (streams 0 rows, 1 columns, 2 extra rows, 3 extra columns)."""
+    (streams 0 rows, 1 columns, 2 extra rows, 3 extra columns).
+
+    Two refinements of the library's engine, restated here so that the oracle takes the same
+    decisions: a block with r = D uses the relative pinv threshold min(tau, full_tau) (full_tau
+    = 0: tau); the core's numbers are also R's at the sampled columns (the library writes C's
+    values there; with a common fill they are the same); a block that passes with est above
+    tol / (safety * verify) is re-checked on fresh
+    extra rows and columns (streams 4 and 5, outside I, Ix and J, Jx) and passes only if the
+    estimate pooled over both sets does (verify <= 1: no re-check)."""
     rows = np.asarray(rows)
     cols = np.asarray(cols)
     M, N = len(rows), len(cols)
@@ -163,12 +191,31 @@ def plain_adaptive(fill, rows, cols, tol, block_id, seed, extra_rows=16, extra_c
         J = el.sample(r, N, block_id, rnd, 1, seed)
         Ix = el.sample_extra(extra_rows, I, M, block_id, rnd, seed, stream=2)
         Jx = el.sample_extra(extra_cols, J, N, block_id, rnd, seed, stream=3)
-        C, U, R = cur_from_indices(fill, rows, cols, I, J, tau, relative)
+        if r >= D and full_tau > 0:
+            t_r, rel_r = (min(tau, full_tau) if relative else full_tau), True
+        else:
+            t_r, rel_r = tau, relative
+        C, U, R = cur_from_indices(fill, rows, cols, I, J, t_r, rel_r)
         Zx = fill(rows[Ix], cols) if len(Ix) else np.zeros((0, N), complex)
         Zc = fill(rows, cols[Jx]) if len(Jx) else np.zeros((M, 0), complex)
-        est = max(extra_row_estimate(C, U, R, Zx, Ix), extra_col_estimate(C, U, R, Zc, Jx))
-        if est <= tol / safety or r >= D or rnd + 1 >= max_rounds:
-            return dict(C=C, U=U, R=R, I=I, J=J, Ix=Ix, Jx=Jx, est=est, r=r, rounds=rnd + 1)
+        sums = extra_row_sums(C, U, R, Zx, Ix) + extra_col_sums(C, U, R, Zc, Jx)
+        est = est_from_sums(*sums)
+        last = r >= D or rnd + 1 >= max_rounds
+        ok = est <= tol / safety
+        more = M - r - len(Ix) > 0 or N - r - len(Jx) > 0
+        verified = False
+        if ok and verify > 1 and est > tol / (safety * verify) and more and not last:
+            Ix2 = el.sample_extra(extra_rows, np.union1d(I, Ix), M, block_id, rnd, seed, stream=4)
+            Jx2 = el.sample_extra(extra_cols, np.union1d(J, Jx), N, block_id, rnd, seed, stream=5)
+            Zx2 = fill(rows[Ix2], cols) if len(Ix2) else np.zeros((0, N), complex)
+            Zc2 = fill(rows, cols[Jx2]) if len(Jx2) else np.zeros((M, 0), complex)
+            s2 = extra_row_sums(C, U, R, Zx2, Ix2) + extra_col_sums(C, U, R, Zc2, Jx2)
+            est = est_from_sums(*[a + b for a, b in zip(sums, s2)])
+            ok = est <= tol / safety
+            verified = True
+        if ok or last:
+            return dict(C=C, U=U, R=R, I=I, J=J, Ix=Ix, Jx=Jx, est=est, r=r, rounds=rnd + 1,
+                        verified=verified)
         r = next_size(r, D)
         rnd += 1
 

@@ -103,8 +103,22 @@ def test_matvec_against_dense_far_field(sphere):
         X = rng.standard_normal((m.N, 4)) + 1j * rng.standard_normal((m.N, 4))
         Y = eng.matvec(torch.as_tensor(X, device="cuda:0")).cpu().numpy()
         Yd = _dense_far_product(eng, X)
-    assert err.max() < 10 * tol
+    assert err.max() <= tol
     assert np.linalg.norm(Y - Yd) / np.linalg.norm(Yd) < 2 * err.max()
+
+
+def test_dense_far_matvec_matches_blockwise_product(sphere):
+    """The library's dense reference product (every far block filled in FP64 and applied on the
+    device) against the block-by-block product of dense fills on the host."""
+    m, part = sphere
+    rng = np.random.default_rng(13)
+    with Engine() as eng:
+        eng.upload_mesh(m, K, ETA, q=7)
+        eng.set_blocks(part)
+        X = rng.standard_normal((m.N, 3)) + 1j * rng.standard_normal((m.N, 3))
+        Y = eng.dense_far_matvec(torch.as_tensor(X, device="cuda:0")).cpu().numpy()
+        Yd = _dense_far_product(eng, X)
+    assert np.linalg.norm(Y - Yd) / np.linalg.norm(Yd) < 1e-12
 
 
 def test_matvec_rejects_bad_calls(sphere):

@@ -25,14 +25,15 @@ def test_two_plate_block_matches_oracle():
     with Engine() as eng:
         eng.upload_mesh(m, K, ETA, q=7)
         eng.set_blocks(group_ptr=gp, group_ids=gi, gt=np.array([0], np.int32), gs=np.array([1], np.int32))
+        # the workload's pinv threshold (1e-3 relative) also at full sample count
         st = eng.compress(tol, precision="c128", tau=1e-3, tau_relative=True, r0=[r0],
-                          oversample=p, seed=seed)
+                          oversample=p, seed=seed, full_tau=0.0)
         C, U, R, I, J = eng.get_block(0, st)
         err = eng.true_errors()[0]
     rows, cols = gi[:half], gi[half:]
     fill = lambda rr, cc: el.fill(m, rr + 1, cc + 1, K, ETA, 7, 7)
     ref = co.plain_adaptive(fill, rows, cols, tol, block_id=0, seed=seed, tau=1e-3,
-                            relative=True, r0=r0 + p)
+                            relative=True, r0=r0 + p, full_tau=0.0)
     assert st["r"][0] == ref["r"] and st["rounds"][0] == ref["rounds"]
     assert np.array_equal(I, ref["I"]) and np.array_equal(J, ref["J"])
     assert abs(st["est"][0] - ref["est"]) <= 1e-6 * ref["est"] + 1e-12

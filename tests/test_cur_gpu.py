@@ -68,7 +68,12 @@ def test_adaptive_driver_meets_tolerance(spheres768):
 def test_reference_two_sphere_benchmark():
     """The reference's logged run (codes/GPU_implementation/seed/compres_single_block_spheres.txt:
     19-50): two R = 1 m octahedral spheres with Ne = 3072 each, 12 m apart, tol 1e-1; sizes
-    307 -> 614 and a final relative Frobenius error of 3.6e-8..3.8e-8 against the dense block."""
+    307 -> 614 and a final relative Frobenius error of 3.6e-8..3.8e-8 against the dense block.
+    The sizes are reproduced exactly; the error lands below the logged one (about 3e-9 here,
+    for every wavelength tried from 0.5 to 4 m, with the numpy restatement on the same mesh),
+    so the bar is the logged error's order of magnitude. The log's wavelength is not printed;
+    the fixed-sample-count curves of the lambda sweep pin the error level instead
+    (test_lambda_sweep_gpu.py)."""
     m = pmesh.two_spheres(1.0, 12.0, 3072)
     em = api.EMData.for_wavelength(2.0)
     r1, r2 = np.arange(1, 3073), np.arange(3073, 6145)
@@ -76,4 +81,4 @@ def test_reference_two_sphere_benchmark():
     C, U, R, rs, cs, err, t = api.cuda_cur_compress3(r1, r2, 1e-1, m, em, rng=np.random.default_rng(0))
     assert C.shape == (3072, 614)
     e = co.rel_fro_error(Z, C, U, R)
-    assert e < 1e-6, e
+    assert e < 1e-7, e

@@ -74,7 +74,11 @@ def test_true_error_matches_oracle(small_sphere):
             C, U, R, I, J = eng.get_block(b, st)
             Z = el.fill(m, rows + 1, cols + 1, k, eta, 7, 7)
             e = co.rel_fro_error(Z, C, U, R)
-            assert abs(e - err[b]) <= 1e-6 * max(e, 1e-12) + 1e-12
+            # forming C U R rounds at eps |C| |U| |R| (U inverts an ill-conditioned core); the
+            # two errors agree to that scale (relative to |Z|) or to 1e-6 of themselves
+            scale = (np.linalg.norm(C, 2) * np.linalg.norm(U, 2) * np.linalg.norm(R, 2)
+                     / np.linalg.norm(Z))
+            assert abs(e - err[b]) <= 1e-6 * e + 1e-13 * scale + 1e-15, (b, e, err[b], scale)
 
 
 def test_adaptive_rounds_match_oracle(small_sphere):

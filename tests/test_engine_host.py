@@ -19,8 +19,9 @@ def test_stat_layout_matches_c():
 
 
 def test_opts_layout():
-    # pskel_opts_t: 2 doubles, 8 ints, uint64, 2 doubles, 2 ints
-    assert ctypes.sizeof(_lib.Opts) == 80
+    # pskel_opts_t: 2 doubles, 8 ints, uint64, 2 doubles, 2 ints, 2 doubles
+    assert ctypes.sizeof(_lib.Opts) == 96
+    assert _lib.Opts.est_verify.offset == 80 and _lib.Opts.full_tau.offset == 88
     assert ctypes.sizeof(_lib.EM) == 24
 
 
@@ -34,6 +35,8 @@ def test_roofline_work_counts():
     # 30 factor entries of 8 bytes, 9 core entries of 16 bytes, 2 x 9 vector entries of 8 bytes
     assert roofline.matvec_bytes([4], [6], [3], 2, 8.0, 16.0) == 30 * 8 + 9 * 16 + 2 * 10 * 8
     assert roofline.recompress_flops([4], [6], [2], [1]) == 8 * (2 * 4 * 4 + 2 * 6 * 4) + 84 * 8 + 8 * 10 * 2
+    # store: (4 + 6) x 3 factor entries of 8 bytes; X and Y (N = 20) and T (2 x 3) for 2 sides
+    assert roofline.store_matvec_bytes([4], [6], [3], 20, 2) == 30 * 8 + 2 * 8 * (40 + 6)
 
 
 def test_balanced_tile_width_rule():

@@ -32,8 +32,7 @@ def test_learned_sampling_gain_on_heldout_geometry():
         t_l = eng.timing()
         err = eng.true_errors()
     assert np.all(err <= tol), err.max()
-    # the plain baseline shares the randomized estimator; it is reported, not required here
-    assert np.mean(err_plain > tol) < 0.01
+    assert np.all(err_plain <= tol), err_plain.max()
     assert t_l["point_pairs"] < 0.8 * t_plain["point_pairs"], (t_l, t_plain)
     assert st["rounds"].mean() < st_plain["rounds"].mean()
     assert np.mean(st["rounds"] == 1) > 0.7

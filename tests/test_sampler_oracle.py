@@ -57,3 +57,17 @@ def test_sample_extra_avoids_I():
 def test_sample_rejects_r_above_D():
     with pytest.raises(ValueError):
         el.sample(6, 5, 0, 0, 0, 0)
+
+
+def test_recheck_samples_avoid_every_earlier_sample():
+    """The re-check of a block draws its new extra rows outside I and the first extra rows
+    (stream 4), so the pooled estimate never counts a row twice."""
+    I = el.sample(30, 120, 7, 1, 0, 3)
+    Ix = el.sample_extra(16, I, 120, 7, 1, 3, stream=2)
+    Ix2 = el.sample_extra(16, np.union1d(I, Ix), 120, 7, 1, 3, stream=4)
+    assert len(Ix2) == 16 and np.all(np.diff(Ix2) > 0)
+    assert not set(Ix2) & (set(I) | set(Ix))
+    # the free rows run out: only what is left
+    J = np.arange(100, dtype=np.int32)
+    Jx = np.arange(100, 110, dtype=np.int32)
+    assert list(el.sample_extra(16, np.union1d(J, Jx), 120, 7, 1, 3, stream=5)) == list(range(110, 120))
