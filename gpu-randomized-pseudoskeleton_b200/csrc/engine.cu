@@ -427,6 +427,11 @@ int tri_cols_for(const pskel_ctx *c, int nt) {
 }
 
 
+// the per-(triangle, slot) table of group g for the triangle-moment fill
+const double *guse_of(const pskel_ctx *c, int g) {
+    return c->d_guse.as<double>() + 12 * (size_t)c->gtri_ptr[g];
+}
+
 // fill variant actually used for a precision: the triangle-moment kernel when asked for and
 // every group fits it, else the per-entry kernel (two rows per thread when 8 was asked for)
 bool tri_for(const pskel_ctx *c, int precision) {
@@ -559,9 +564,11 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
             const int *tri = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
             const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
             gfills.push_back(GroupFillJob{w.rows_g, tri + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                          w.Jg, w.C, w.m, ntt, w.r + w.pc, w.m, 0, tri_cols_for(c, ntt)});
+                                          w.Jg, w.C, w.m, ntt, w.r + w.pc, w.m, 0, tri_cols_for(c, ntt),
+                                          guse_of(c, gt)});
             gfills.push_back(GroupFillJob{w.cols_g, tri + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                          w.Ig, w.Rx, w.n, nts, w.r + w.pe, w.r + w.pe, 1, tri_cols_for(c, nts)});
+                                          w.Ig, w.Rx, w.n, nts, w.r + w.pe, w.r + w.pe, 1, tri_cols_for(c, nts),
+                                          guse_of(c, gs)});
         }
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         // a block sampled on every row or every column of its smaller side cannot gain from more
@@ -766,10 +773,12 @@ int run_verify(pskel_ctx *c, const RoundPlan &p, const std::vector<int> &sel,
             const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
             if (pc2[v] > 0)
                 gfills.push_back(GroupFillJob{w.rows_g, tr + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                              x.Jg2, Xc, w.m, ntt, pc2[v], w.m, 0, tri_cols_for(c, ntt)});
+                                              x.Jg2, Xc, w.m, ntt, pc2[v], w.m, 0, tri_cols_for(c, ntt),
+                                              guse_of(c, gt)});
             if (pe2[v] > 0)
                 gfills.push_back(GroupFillJob{w.cols_g, tr + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                              x.Ig2, Xr, w.n, nts, pe2[v], pe2[v], 1, tri_cols_for(c, nts)});
+                                              x.Ig2, Xr, w.n, nts, pe2[v], pe2[v], 1, tri_cols_for(c, nts),
+                                              guse_of(c, gs)});
         } else {
             if (pc2[v] > 0) fills.push_back(FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2[v], w.m, 0});
             if (pe2[v] > 0) fills.push_back(FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2[v], pe2[v], 1});
@@ -818,7 +827,7 @@ int run_verify(pskel_ctx *c, const RoundPlan &p, const std::vector<int> &sel,
         fp.precision = o.precision;
         fp.split = entry_split_for(c, o.precision);
         fp.tri_cols = c->tri_cols;
-        fp.geom32 = c->geom32;
+            fp.geom32 = c->geom32;
         fp.max_rows = max_rows;
         if (tri)
             PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d + o_f),
@@ -925,6 +934,9 @@ extern "C" int pskel_upload_mesh(pskel_ctx *c, const double *vertex, int nv, con
     }
     c->h_edges.resize(4 * (size_t)ne);
     for (size_t i = 0; i < 4 * (size_t)ne; ++i) c->h_edges[i] = (int)edges[i] - 1;
+    c->h_vertex.assign(vertex, vertex + 3 * (size_t)nv);
+    c->h_ln.assign(ln, ln + ne);
+    c->h_cent.assign(cent, cent + 3 * (size_t)nt);
     c->em = *em;
     c->have_mesh = true;
     if (c->graph) {
@@ -1068,6 +1080,30 @@ extern "C" int pskel_set_blocks(pskel_ctx *c, const int *group_ptr, const int *g
             c->gtri_ptr[g + 1] = (int)tri.size();
         }
         c->use_tri = max_rows <= kTriFillMaxRows;
+        // per (triangle, slot) of each group: the RWG's free vertex minus the triangle centroid
+        // and the signed edge length, the numbers the fill's per-item scatter needs (looked up
+        // here once instead of through dependent loads in every item)
+        std::vector<double> use(12 * tri.size(), 0.0);
+        for (int g = 0; g < n_groups; ++g)
+            for (int sl = c->gtri_ptr[g]; sl < c->gtri_ptr[g + 1]; ++sl)
+                for (int u = 0; u < 3; ++u) {
+                    const int a = adj[3 * (size_t)sl + u];
+                    if (a < 0) continue;
+                    const int ml = a >> 1, side = a & 1;
+                    const int e = group_ids[group_ptr[g] + ml], t = tri[sl];
+                    const int vo = c->h_edges[4 * (size_t)e + 2 + side];
+                    if (vo < 0 || 3 * (size_t)vo + 2 >= c->h_vertex.size()) {
+                        set_error(PSKEL_ERR_RANGE, "edges: vertex id out of range");
+                        return PSKEL_ERR_RANGE;
+                    }
+                    double *o = &use[12 * (size_t)sl + 4 * u];
+                    for (int d = 0; d < 3; ++d)
+                        o[d] = c->h_vertex[3 * (size_t)vo + d] - c->h_cent[3 * (size_t)t + d];
+                    o[3] = (side ? -1.0 : 1.0) * c->h_ln[e];
+                }
+        PSKEL_TRY(c->d_guse.reserve(sizeof(double) * (use.size() + 1)));
+        PSKEL_CUDA(cudaMemcpyAsync(c->d_guse.ptr, use.data(), sizeof(double) * use.size(),
+                                   cudaMemcpyHostToDevice, c->stream));
         PSKEL_TRY(c->d_gtri.reserve(sizeof(int) * (tri.size() + 1)));
         PSKEL_TRY(c->d_gadj.reserve(sizeof(int) * (adj.size() + 1)));
         PSKEL_CUDA(cudaMemcpyAsync(c->d_gtri.ptr, tri.data(), sizeof(int) * tri.size(),
@@ -1516,7 +1552,8 @@ int true_errors_list(pskel_ctx *c, const std::vector<int> &list, double *err) {
                                      c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt],
                                      c->d_gids.as<int>() + c->gptr[c->gs[b]], Z, res.m,
                                      c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], res.n, res.m, 0,
-                                     tri_cols_for(c, c->gtri_ptr[gt + 1] - c->gtri_ptr[gt])};
+                                     tri_cols_for(c, c->gtri_ptr[gt + 1] - c->gtri_ptr[gt]),
+                                     guse_of(c, gt)};
             prefix[i + 1] = prefix[i] + (tri ? (res.n + gfills[i].tc - 1) / gfills[i].tc
                                                      : ((res.m + tm - 1) / tm) * ((res.n + tn - 1) / tn));
             mats[i] = Z;
@@ -1590,7 +1627,7 @@ int true_errors_list(pskel_ctx *c, const std::vector<int> &list, double *err) {
         fp.precision = PSKEL_C128;
         fp.split = entry_split_for(c, PSKEL_C128);
         fp.tri_cols = c->tri_cols;
-        if (tri)
+            if (tri)
             PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d_f), d_p, nbb,
                                       prefix.back(), c->stream));
         else
@@ -1682,7 +1719,7 @@ extern "C" int pskel_dense_far_matvec(pskel_ctx *c, const void *X, int ldx, void
             const int nt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt];
             gfills[i] = GroupFillJob{rows, c->d_gtri.as<int>() + c->gtri_ptr[gt],
                                      c->d_gadj.as<int>() + 3 * (size_t)c->gtri_ptr[gt], cols, Z, m, nt,
-                                     n, m, 0, tri_cols_for(c, nt)};
+                                     n, m, 0, tri_cols_for(c, nt), guse_of(c, gt)};
             prefix[i + 1] = prefix[i] + (tri ? (n + gfills[i].tc - 1) / gfills[i].tc
                                              : ((m + tm - 1) / tm) * ((n + tn - 1) / tn));
             apps[i] = DenseApply{Z, rows, cols, m, n};
@@ -1715,7 +1752,7 @@ extern "C" int pskel_dense_far_matvec(pskel_ctx *c, const void *X, int ldx, void
         fp.precision = PSKEL_C128;
         fp.split = entry_split_for(c, PSKEL_C128);
         fp.tri_cols = c->tri_cols;
-        fp.max_rows = max_rows;
+            fp.max_rows = max_rows;
         if (tri)
             PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d_f), d_p, nbb,
                                       prefix.back(), c->stream));

@@ -27,6 +27,28 @@ struct BlockWork {
     double *est;
 };
 
+// One core of a round with r <= 32 for warp_core_kernel (csrc/warp_core.cu): the core is
+// gathered from C, its numbers written into R(:, J), and its truncated pseudo-inverse formed by
+// one warp.
+constexpr int kWarpCoreMaxN = 32;
+constexpr int kWarpCoreThreads = 128;
+struct WarpCoreJob {
+    const void *C;       // m x (r + pc), ld m (storage type of the round)
+    void *Rx;            // (r + pe) x n, ld ldr
+    const int *I, *J;    // local samples
+    double2 *U;          // n x n out: the pinv
+    double2 *refl;       // n x n scratch: reflector tails
+    double2 *qw;         // n x n scratch: Q W
+    double *sigma;       // n out (column order of the Jacobi)
+    int *rank;           // out
+    int m, ldr, n;
+    double tau;
+    int relative;
+    int svd_index;       // entry of the round's SvdJob table that receives status and sweeps
+};
+int launch_warp_core(const WarpCoreJob *d_jobs, int count, SvdJob *d_svd, int max_sweeps,
+                     int precision, cudaStream_t stream);
+
 // Single-level octree partition of the uploaded mesh's RWG basis centres and its far-pair list,
 // built on the device (csrc/octree.cu). Group ids, extents and the far list stay in device
 // memory; offsets and centres are kept on the host as well.
@@ -114,6 +136,8 @@ struct pskel_ctx {
     std::vector<int> h_edges;            // T+, T-, v+, v- per RWG (0-based), host copy
     std::vector<int> gtri_ptr;           // CSR offsets into gtri / (3x) gadj
     DevBuf d_gtri, d_gadj;
+    DevBuf d_guse;                       // per (group triangle, slot): free vertex - centroid, s l
+    std::vector<double> h_vertex, h_ln, h_cent;  // host copies of the mesh arrays it is built from
     bool use_tri = false;
     std::vector<RoundArena> arenas;
     DevBuf verify_keep, verify_tables;  // re-check of blocks accepted with little margin

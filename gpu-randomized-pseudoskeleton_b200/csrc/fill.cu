@@ -437,13 +437,13 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     auto kern = fill2_kernel<T, Q, TM, TN>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
-    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = (long long)sm_count() * per_sm;
     if (grid > total_tiles) grid = total_tiles;
     if (grid < 1) return PSKEL_OK;
     const double pi = 3.14159265358979323846;
-    kern<<<(int)grid, NT, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
+    kern<<<(int)grid, 256, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
                                           (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)),
                                           p.r_near > 0 ? p.r_near * p.r_near : 0.0, d_flags);
     PSKEL_LAUNCHED(1);
@@ -462,7 +462,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     auto kern = fill_kernel<T, Q, TM, TN, SPLIT>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
-    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = (long long)sm_count() * per_sm;
     if (grid > total_tiles) grid = total_tiles;
@@ -473,7 +473,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     const double kphase = sizeof(T) == 8 ? p.k / pi : p.k / (2.0 * pi);
     const T scale = (T)(p.eta / (4.0 * pi));
     const double rn2 = p.r_near > 0 ? p.r_near * p.r_near : 0.0;
-    kern<<<(int)grid, NT, smem, stream>>>(rec_t, rec_s, d_jobs, d_prefix, njobs, total_tiles, k,
+    kern<<<(int)grid, 256, smem, stream>>>(rec_t, rec_s, d_jobs, d_prefix, njobs, total_tiles, k,
                                           kinv, kphase, scale, rn2, d_flags);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;
@@ -724,11 +724,21 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
                 const int a = ad[u];
                 if (a < 0) continue;
                 const int ml = a >> 1, side = a & 1;
-                const int e = job.rows[ml];
-                const int vo = (int)edges[4 * (size_t)e + 2 + side] - 1;
-                const T vl[3] = {(T)(vertex[3 * (size_t)vo] - cx), (T)(vertex[3 * (size_t)vo + 1] - cy),
-                                 (T)(vertex[3 * (size_t)vo + 2] - cz)};
-                const T sl = (side ? -1 : 1) * (T)ln[e];
+                T vl[3], sl;
+                if (job.use) {  // free vertex - centroid and s l, looked up once per group
+                    const double *uz = job.use + 4 * (3 * (size_t)t + u);
+                    vl[0] = (T)uz[0];
+                    vl[1] = (T)uz[1];
+                    vl[2] = (T)uz[2];
+                    sl = (T)uz[3];
+                } else {
+                    const int e = job.rows[ml];
+                    const int vo = (int)edges[4 * (size_t)e + 2 + side] - 1;
+                    vl[0] = (T)(vertex[3 * (size_t)vo] - cx);
+                    vl[1] = (T)(vertex[3 * (size_t)vo + 1] - cy);
+                    vl[2] = (T)(vertex[3 * (size_t)vo + 2] - cz);
+                    sl = (side ? -1 : 1) * (T)ln[e];
+                }
                 const T hk = (T)0.5 * k;
                 T br = bxr, bi = bxi;
 #pragma unroll

@@ -156,18 +156,22 @@ struct GroupFillJob {
     void *out;
     int m, nt, nc, ld, trans;
     int tc;           // columns per CTA tile for this job (<= the launch's tile width)
+    const double *use;  // 4 doubles per (triangle, adjacency slot): the RWG's free vertex minus
+                        // the triangle centroid (x, y, z) and the signed edge length s l; null:
+                        // looked up in the mesh arrays
 };
 constexpr int kTriFillMaxRows = 512;  // largest group the triangle-moment fill accepts
 // Columns per tile for a job of nt triangles: the width in [4, max_cols] whose (triangle, column)
 // item count fills the 256 threads of a CTA best (the last round of items is the idle part),
 // the widest among equals. max_cols < 4 returns max_cols.
 inline int tri_tile_cols(int nt, int max_cols) {
+    constexpr int threads = 256;
     if (max_cols < 4) return max_cols < 1 ? 1 : max_cols;
     int best = max_cols;
     double best_eff = -1.0;
     for (int c = max_cols; c >= 4; --c) {
         const long long items = (long long)nt * c;
-        const long long slots = (items + 255) / 256 * 256;
+        const long long slots = (items + threads - 1) / threads * threads;
         const double eff = (double)items / (double)slots;
         if (eff > best_eff + 1e-9) {
             best_eff = eff;

@@ -55,9 +55,9 @@ def test_batched_compression_errors(small_sphere, prec):
         err = eng.true_errors()
     assert np.all(np.isfinite(err))
     assert np.median(err) < tol
-    assert np.max(err) < 10 * tol, np.max(err)
-    # every block either met the estimate or ran out of room
-    ok = (st["est"] <= tol) | (st["r"] == np.minimum(st["m"], st["n"]))
+    assert np.max(err) <= tol, np.max(err)
+    # every block met the estimate's threshold or was sampled on its whole smaller side
+    ok = (st["est"] <= tol / 2) | (st["r"] == np.minimum(st["m"], st["n"]))
     assert np.all(ok)
 
 

@@ -39,9 +39,11 @@ def test_mirror_blocks(sphere, prec):
             p = mir[b]
             assert st["m"][b] == st["n"][p] and st["n"][b] == st["m"][p]
             assert st["r"][b] == st["r"][p] and st["est"][b] == st["est"][p]
-        # mirror error equals the primary's (Z symmetric to rounding)
-        np.testing.assert_allclose(err, err[mir], rtol=1e-6, atol=1e-9)
-        assert np.median(err) < tol and err.max() < 3 * tol
+        # mirror error equals the primary's (Z symmetric to rounding); blocks sampled on their
+        # whole smaller side reproduce Z to ~1e-9, where the two dense fills' roundings, through
+        # the core's inverse, set the difference
+        np.testing.assert_allclose(err, err[mir], rtol=1e-6, atol=1e-7)
+        assert np.median(err) < tol and err.max() <= tol
         # factors of a mirror are the transposes, with swapped samples
         b = int(np.argmax(mir < np.arange(eng.n_blocks)))  # a block whose partner is primary
         p = mir[b]
