@@ -473,7 +473,15 @@ struct RoundPlan {
     EstJob *d_est = nullptr;
     int pinv_tiles = 0;
     int nb = 0;
+    // pipeline chunks: blocks [cb[k], cb[k+1]) of the works order; each chunk has its own fill
+    // tile prefix (from 0), SVD plan (index map into the round's SvdJob table) and pinv tiles
+    std::vector<int> cb;
+    std::vector<int> ch_tiles, ch_pinv_tiles;
+    std::vector<int *> ch_prefix, ch_idx;
+    std::vector<SvdPlan> ch_svd;
 };
+
+constexpr int kPipeMinBlocks = 2048;  // smaller rounds run as one chunk
 
 // Lay out the round's storage, build all job tables on the host and upload them in one copy.
 int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
@@ -614,6 +622,41 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     }
     PSKEL_TRY(svd_plan(svds, p.svd));
     const std::vector<int> &svd_idx = p.svd.idx;
+    // pipeline chunks, each with its own tables, of decreasing fill work: chunk k ends at the
+    // fraction 1 - (1 - k/K)^2 of the tiles, so the early chunks' pinv and estimate run beside
+    // the many later fills and the last chunk, whose pinv and estimate run alone, is small
+    const int K = (nb >= kPipeMinBlocks && c->pipe_chunks > 1) ? std::min(c->pipe_chunks, pskel_ctx::kMaxChunks) : 1;
+    p.cb.assign(1, 0);
+    {
+        const long long total = prefix.back();
+        int b = 0;
+        for (int k = 1; k < K; ++k) {
+            const double left = 1.0 - (double)k / K;
+            const long long want = (long long)((1.0 - left * left) * (double)total);
+            while (b < nb && prefix[2 * (size_t)b] < want) ++b;
+            if (b > p.cb.back()) p.cb.push_back(b);
+        }
+        p.cb.push_back(nb);
+    }
+    const int nch = (int)p.cb.size() - 1;
+    std::vector<int> ch_prefix_all, ch_idx_all;
+    std::vector<size_t> ch_pref_off(nch), ch_idx_off(nch);
+    p.ch_svd.assign(nch, SvdPlan());
+    p.ch_tiles.assign(nch, 0);
+    p.ch_pinv_tiles.assign(nch, 0);
+    for (int k = 0; k < nch; ++k) {
+        const int b0 = p.cb[k], b1 = p.cb[k + 1];
+        ch_pref_off[k] = ch_prefix_all.size();
+        for (int j = 2 * b0; j <= 2 * b1; ++j) ch_prefix_all.push_back(prefix[j] - prefix[2 * b0]);
+        p.ch_tiles[k] = prefix[2 * b1] - prefix[2 * b0];
+        std::vector<SvdJob> sub(svds.begin() + b0, svds.begin() + b1);
+        PSKEL_TRY(svd_plan(sub, p.ch_svd[k]));
+        for (int &x : p.ch_svd[k].idx) x += b0;  // into the round's SvdJob table
+        ch_idx_off[k] = ch_idx_all.size();
+        ch_idx_all.insert(ch_idx_all.end(), p.ch_svd[k].idx.begin(), p.ch_svd[k].idx.end());
+        for (int i = b0; i < b1; ++i)
+            p.ch_pinv_tiles[k] = std::max(p.ch_pinv_tiles[k], ((p.r[i] + 31) / 32) * ((p.r[i] + 31) / 32));
+    }
     // pack tables
     size_t t = 0;
     auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
@@ -625,6 +668,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     const size_t o_idx = slot(sizeof(int) * nb);
     const size_t o_pinv = slot(sizeof(PinvJob) * nb);
     const size_t o_est = slot(sizeof(EstJob) * nb);
+    const size_t o_cpref = slot(sizeof(int) * ch_prefix_all.size());
+    const size_t o_cidx = slot(sizeof(int) * (ch_idx_all.size() + 1));
     ar.h_tables.assign(t, 0);
     std::memcpy(ar.h_tables.data() + o_works, works.data(), sizeof(BlockWork) * nb);
     if (p.tri)
@@ -636,6 +681,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     std::memcpy(ar.h_tables.data() + o_idx, svd_idx.data(), sizeof(int) * nb);
     std::memcpy(ar.h_tables.data() + o_pinv, pinvs.data(), sizeof(PinvJob) * nb);
     std::memcpy(ar.h_tables.data() + o_est, ests.data(), sizeof(EstJob) * nb);
+    std::memcpy(ar.h_tables.data() + o_cpref, ch_prefix_all.data(), sizeof(int) * ch_prefix_all.size());
+    std::memcpy(ar.h_tables.data() + o_cidx, ch_idx_all.data(), sizeof(int) * ch_idx_all.size());
     PSKEL_TRY(ar.tables.reserve(t + 256));
     PSKEL_CUDA(cudaMemcpyAsync(ar.tables.ptr, ar.h_tables.data(), t, cudaMemcpyHostToDevice,
                                c->stream));
@@ -650,11 +697,21 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.d_svd_idx = reinterpret_cast<int *>(d + o_idx);
     p.d_pinv = reinterpret_cast<PinvJob *>(d + o_pinv);
     p.d_est = reinterpret_cast<EstJob *>(d + o_est);
+    p.ch_prefix.assign(nch, nullptr);
+    p.ch_idx.assign(nch, nullptr);
+    for (int k = 0; k < nch; ++k) {
+        p.ch_prefix[k] = reinterpret_cast<int *>(d + o_cpref) + ch_pref_off[k];
+        p.ch_idx[k] = reinterpret_cast<int *>(d + o_cidx) + ch_idx_off[k];
+    }
     p.pinv_tiles = max_pinv_tiles;
     return PSKEL_OK;
 }
 
-// All kernels of one round (no host synchronisation inside: capturable).
+// All kernels of one round (no host synchronisation inside: capturable). A round of several
+// chunks is pipelined: the fill of chunk k + 1 (one CTA per tile) on the context's stream
+// overlaps the gather, SVD, pinv and estimate of chunk k on the high-priority pipeline stream,
+// whose CTAs take the SMs' free slots as fill CTAs retire (the fill is bound by FP32 issue, the
+// Jacobi SVD by FP64 latency).
 int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool events) {
     cudaStream_t s = c->stream;
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[0], s));
@@ -672,26 +729,50 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
     fp.tri_cols = c->tri_cols;
     fp.geom32 = c->geom32;
     fp.max_rows = p.tri_rows;
-    if (p.tri)
-        PSKEL_TRY(launch_tri_fill(c->mesh, fp, p.d_gfill, p.d_fill_prefix, p.fill_jobs,
-                                  p.fill_tiles, s));
-    else
-        PSKEL_TRY(launch_fill(c->mesh, fp, p.d_fill, p.d_fill_prefix, p.fill_jobs, p.fill_tiles,
-                              c->flags.as<int>(), s));
-    if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
-    if (o.precision == PSKEL_C64)
-        gather_core_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_works);
-    else
-        gather_core_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_works);
-    PSKEL_LAUNCHED(1);
-    PSKEL_TRY(svd_launch(p.d_svd, p.d_svd_idx, p.svd, 60, s, &c->svd_par));
-    PSKEL_TRY(batched_pinv(p.d_pinv, p.nb, p.pinv_tiles, s));
-    if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));
-    if (o.precision == PSKEL_C64)
-        estimate_kernel<float2><<<p.nb, 256, 0, s>>>(p.d_est);
-    else
-        estimate_kernel<double2><<<p.nb, 256, 0, s>>>(p.d_est);
-    PSKEL_LAUNCHED(1);
+    const int nch = (int)p.cb.size() - 1;
+    auto fill = [&](int job0, const int *prefix, int njobs, int tiles, cudaStream_t st) -> int {
+        if (p.tri)
+            return launch_tri_fill(c->mesh, fp, p.d_gfill + job0, prefix, njobs, tiles, st);
+        return launch_fill(c->mesh, fp, p.d_fill + job0, prefix, njobs, tiles, c->flags.as<int>(), st);
+    };
+    auto pinv_est = [&](int b0, int cnt, const SvdPlan &plan, const int *idx, int ptiles,
+                        cudaStream_t st, cudaEvent_t between) -> int {
+        if (o.precision == PSKEL_C64)
+            gather_core_kernel<float2><<<cnt, 256, 0, st>>>(p.d_works + b0);
+        else
+            gather_core_kernel<double2><<<cnt, 256, 0, st>>>(p.d_works + b0);
+        PSKEL_LAUNCHED(1);
+        PSKEL_TRY(svd_launch(p.d_svd, idx, plan, 60, st, &c->svd_par));
+        PSKEL_TRY(batched_pinv(p.d_pinv + b0, cnt, ptiles, st));
+        if (between) PSKEL_CUDA(cudaEventRecord(between, st));
+        if (o.precision == PSKEL_C64)
+            estimate_kernel<float2><<<cnt, 256, 0, st>>>(p.d_est + b0);
+        else
+            estimate_kernel<double2><<<cnt, 256, 0, st>>>(p.d_est + b0);
+        PSKEL_LAUNCHED(1);
+        return PSKEL_OK;
+    };
+    if (nch <= 1) {
+        PSKEL_TRY(fill(0, p.d_fill_prefix, p.fill_jobs, p.fill_tiles, s));
+        if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
+        PSKEL_TRY(pinv_est(0, p.nb, p.svd, p.d_svd_idx, p.pinv_tiles, s, events ? c->ev[3] : nullptr));
+    } else {
+        cudaStream_t s2 = c->pipe_stream;
+        fp.persistent = false;
+        for (int k = 0; k < nch; ++k) {
+            const int b0 = p.cb[k], cnt = p.cb[k + 1] - b0;
+            PSKEL_TRY(fill(2 * b0, p.ch_prefix[k], 2 * cnt, p.ch_tiles[k], s));
+            PSKEL_CUDA(cudaEventRecord(c->pipe_ev[k], s));
+            PSKEL_CUDA(cudaStreamWaitEvent(s2, c->pipe_ev[k], 0));
+            PSKEL_TRY(pinv_est(b0, cnt, p.ch_svd[k], p.ch_idx[k], p.ch_pinv_tiles[k], s2, nullptr));
+        }
+        if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));  // the last fill
+        PSKEL_CUDA(cudaEventRecord(c->pipe_ev[pskel_ctx::kMaxChunks], s2));
+        PSKEL_CUDA(cudaStreamWaitEvent(s, c->pipe_ev[pskel_ctx::kMaxChunks], 0));
+        if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));  // the last chunk's pinv and estimate
+    }
+    // (pipelined: ev[1..2] = the fills with the earlier chunks' pinv and estimate beside them,
+    // ev[2..3] = the last chunk's pinv and estimate, ev[3..4] = the collect)
     collect_kernel<<<(p.nb + 255) / 256, 256, 0, s>>>(p.d_works, p.d_svd, p.nb,
                                                      c->arenas[p.round].outs.as<RoundOut>());
     PSKEL_LAUNCHED(1);
@@ -881,6 +962,17 @@ extern "C" int pskel_create(pskel_ctx **out, int device) {
             set_error(PSKEL_ERR_CUDA, "event creation failed");
             return fail(PSKEL_ERR_CUDA);
         }
+    int lo_pri = 0, hi_pri = 0;
+    cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri);
+    if (cudaStreamCreateWithPriority(&c->pipe_stream, cudaStreamNonBlocking, hi_pri) != cudaSuccess) {
+        set_error(PSKEL_ERR_CUDA, "stream creation failed");
+        return fail(PSKEL_ERR_CUDA);
+    }
+    for (auto &e : c->pipe_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            set_error(PSKEL_ERR_CUDA, "event creation failed");
+            return fail(PSKEL_ERR_CUDA);
+        }
     int st = c->flags.reserve(256);
     if (st != PSKEL_OK) return fail(st);
     st = svd_streams_create(c->svd_par);
@@ -894,6 +986,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     if (!c) return PSKEL_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    if (c->pipe_stream) cudaStreamSynchronize(c->pipe_stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     for (auto &e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -909,6 +1002,9 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     octree_release(c->octree);
     c->near_jobs.release(); c->near_mom.release(); c->near_data.release(); c->near_tab.release();
     c->aca_buf.release(); c->aca_tab.release();
+    for (auto &e : c->pipe_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->pipe_stream) cudaStreamDestroy(c->pipe_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return PSKEL_OK;
@@ -1204,6 +1300,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back(o.tau_relative);
             key.push_back(c->split[0] * 8 + c->split[1] + (c->use_tri ? 1000 : 0));
             key.push_back(c->tri_cols + 100 * c->geom32);
+            key.push_back(c->pipe_chunks);
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -1403,6 +1500,16 @@ extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
         return PSKEL_ERR_ARG;
     }
     c->tri_cols = cols;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_set_pipeline(pskel_ctx *c, int chunks) {
+    PSKEL_TRY(ctx_ok(c));
+    if (chunks < 1 || chunks > pskel_ctx::kMaxChunks) {
+        set_error(PSKEL_ERR_ARG, "pipeline chunks must be 1 .. %d", pskel_ctx::kMaxChunks);
+        return PSKEL_ERR_ARG;
+    }
+    c->pipe_chunks = chunks;
     return PSKEL_OK;
 }
 

@@ -125,6 +125,12 @@ struct pskel_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
     pskel::SvdStreams svd_par;  // side streams of the concurrent SVD size classes
+    // pipelined round: the blocks split into chunks; the pinv and estimate of chunk k run on a
+    // high-priority stream while the fill of chunk k + 1 runs on the context's stream
+    static constexpr int kMaxChunks = 8;
+    cudaStream_t pipe_stream = nullptr;
+    cudaEvent_t pipe_ev[kMaxChunks + 1] = {};
+    int pipe_chunks = 4;        // chunks of a round with at least kPipeMinBlocks blocks (1: off)
     DevMesh mesh;
     pskel_em_t em{};
     bool have_mesh = false;

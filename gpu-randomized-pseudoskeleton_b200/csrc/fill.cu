@@ -439,7 +439,7 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;
-    long long grid = (long long)sm_count() * per_sm;
+    long long grid = p.persistent ? (long long)sm_count() * per_sm : (long long)total_tiles;
     if (grid > total_tiles) grid = total_tiles;
     if (grid < 1) return PSKEL_OK;
     const double pi = 3.14159265358979323846;
@@ -464,7 +464,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;
-    long long grid = (long long)sm_count() * per_sm;
+    long long grid = p.persistent ? (long long)sm_count() * per_sm : (long long)total_tiles;
     if (grid > total_tiles) grid = total_tiles;
     if (grid < 1) return PSKEL_OK;
     const double pi = 3.14159265358979323846;
@@ -781,7 +781,7 @@ static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillP
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
     if (per_sm < 1) per_sm = 1;
-    long long grid = (long long)sm_count() * per_sm;
+    long long grid = p.persistent ? (long long)sm_count() * per_sm : (long long)total_tiles;
     if (grid > total_tiles) grid = total_tiles;
     if (grid < 1) return PSKEL_OK;
     double wall[7];

@@ -590,8 +590,12 @@ int svd_resident_attr() {
 
 int svd_streams_create(SvdStreams &p) {
     if (p.ready) return PSKEL_OK;
+    // high priority: in a pipelined round the SVD classes take the SM slots that retiring fill
+    // CTAs free before further fill CTAs do
+    int lo_pri = 0, hi_pri = 0;
+    PSKEL_CUDA(cudaDeviceGetStreamPriorityRange(&lo_pri, &hi_pri));
     for (int i = 0; i < kSvdAux; ++i) {
-        PSKEL_CUDA(cudaStreamCreateWithFlags(&p.aux[i], cudaStreamNonBlocking));
+        PSKEL_CUDA(cudaStreamCreateWithPriority(&p.aux[i], cudaStreamNonBlocking, hi_pri));
         PSKEL_CUDA(cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming));
     }
     PSKEL_CUDA(cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming));

@@ -121,6 +121,9 @@ struct FillParams {
     int tri_cols = kTriFillColsDefault;  // columns per CTA of the triangle-moment fill (4, 8, 16)
     int geom32 = 0;    // complex-FP32 triangle-moment fill: FP32 pair geometry from item offsets
     int max_rows = kTriFillMaxRowsDefaultForParams;  // largest group in a triangle-moment launch
+    bool persistent = true;  // grid of SM count x occupancy striding over the tiles; false: one
+                             // CTA per tile (CTAs retire continually, so kernels on other streams
+                             // can take their place)
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the

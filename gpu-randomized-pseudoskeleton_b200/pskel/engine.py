@@ -359,6 +359,11 @@ class Engine:
         """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
+    def set_pipeline(self, chunks: int):
+        """Chunks of a pipelined compression round (1 = off; default 4): the fill of one chunk
+        overlaps the SVD, pinv and estimate of the previous one."""
+        _lib.check(self._lib.pskel_set_pipeline(self._h, int(chunks)))
+
     def set_symmetric(self, on: bool = True):
         """Compress one block of each (t, s) / (s, t) pair and take the other as its transpose
         (Galerkin symmetry Z = Z^T)."""

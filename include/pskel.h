@@ -263,6 +263,14 @@ int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r
    maximum Jacobi sweeps of the core SVDs. n = length of out (<= 12). */
 int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 
+/* Pipelining of a compression round of at least 2048 blocks: the blocks split into `chunks`
+   (1 .. 8; default 4; 1 = off) of about equal fill work; the fill of chunk k + 1 (one CTA per
+   tile) overlaps the core SVD, pinv and estimate of chunk k, which run on a high-priority
+   stream. The results are those of the unpipelined round. In a pipelined round the timing's
+   fill phase covers all fills with the earlier chunks' pinv and estimate beside them, and the
+   pinv phase the last chunk's pinv and estimate. */
+int pskel_set_pipeline(pskel_ctx *ctx, int chunks);
+
 /* Copy block b's factors to host buffers (complex128): C m x r, U r x r, R r x n, 0-based
    local samples I (r) and J (r). Any pointer may be NULL. */
 int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,

@@ -122,3 +122,30 @@ def test_fill_variants_agree(small_sphere, prec, bar):
         for (C, U, R), (C8, U8, R8) in zip(out[v], out[8]):
             assert np.abs(C - C8).max() <= bar * np.abs(C8).max()
             assert np.abs(R - R8).max() <= bar * np.abs(R8).max()
+
+
+def test_pipelined_round_gives_the_same_result():
+    """A pipelined round (fill of chunk k + 1 beside the SVD, pinv and estimate of chunk k) runs
+    the same kernels on the same data as the unpipelined one: identical sample counts, rounds,
+    estimates and factors, with and without the graph replay of the first round."""
+    m = pmesh.icosphere(2.0, 4)  # 7,680 RWG, 22,312 blocks: above the pipelining threshold
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    out = {}
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        for chunks in (1, 4, 3):
+            eng.set_pipeline(chunks)
+            for graph in (False, True, True):  # eager, capture, replay
+                st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=6, use_graph=graph)
+            picks = (0, 7777, eng.n_blocks - 1)
+            out[chunks] = (st, [eng.get_block(b, st) for b in picks])
+    for chunks in (4, 3):
+        st, blocks = out[chunks]
+        st1, blocks1 = out[1]
+        for k in ("r", "rounds", "rank", "est"):
+            np.testing.assert_array_equal(st[k], st1[k])
+        for f, f1 in zip(blocks, blocks1):
+            for a, b in zip(f, f1):
+                np.testing.assert_array_equal(a, b)
