@@ -317,33 +317,63 @@ def run_ours(args, rank, world, dev):
     # plain FP64 GPU pseudoskeleton (the drop-in baseline): start at min(m,n)/10 and double,
     # driven one block at a time as the reference's drivers call its GPU CUR; same kernels,
     # samples and estimator as the batched modes
+    large = args.large or args.workload == "sphere122k"
     plain_pb = without_symmetry(lambda: eng.compress(TOL, per_block=True, **PLAIN))
-    plain_ms, _, _, _ = timed(plain_pb, 1, 1)
+    plain_ms = None if large else timed(plain_pb, 1, 1)[0]
     # ablations, all blocks batched per round, every block compressed (no symmetry): plain FP64,
     # mixed precision only, learned only, learned + mixed
     plain = without_symmetry(lambda: eng.compress(TOL, **PLAIN))
-    plain_b_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
-    t_plain = eng.timing()
+    if not large:
+        plain_b_ms, st_plain, _, _ = timed(plain, max(1, min(2, args.steps)), 1)
+        t_plain = eng.timing()
+    else:
+        plain_b_ms, st_plain, t_plain = None, None, None
 
     # the same plain method with the symmetric mode: the product against it isolates what the
     # three patterns (learned, mixed precision, batched + graph) gain on their own
     def plain_symmetric():
         eng.set_symmetric(True)
         return eng.compress(TOL, **PLAIN)
-    plain_sym_ms, _, _, _ = timed(plain_symmetric, max(1, min(2, args.steps)), 1)
-    mixed_only = without_symmetry(lambda: eng.compress(TOL, **dict(PLAIN, precision="c64")))
-    mixed_ms, _, _, _ = timed(mixed_only, 1, 1)
-    learned_only = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
-                                                         **dict(PRODUCT, precision="c128")))
-    learned_ms, _, _, _ = timed(learned_only, 1, 2)
-    lm_nosym = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True, **PRODUCT))
-    lm_nosym_ms, _, _, _ = timed(lm_nosym, 1, 2)
-    # learned + batched + symmetric in complex FP64: the same-precision counterpart of the ACA
-    # comparison (which computes in complex FP64)
-    def learned_sym_c128():
-        eng.set_symmetric(True)
-        return eng.compress(TOL, r0=predict_r0(), use_graph=True, **dict(PRODUCT, precision="c128"))
-    lsym128_ms, _, _, _ = timed(learned_sym_c128, 1, 2)
+    if not large:
+        plain_sym_ms, _, _, _ = timed(plain_symmetric, max(1, min(2, args.steps)), 1)
+    else:
+        # the complex-FP64 plain rounds of every block do not fit the device's memory at once:
+        # the blocks (both directions of each pair together) in four batches, one batched call
+        # each, the device times summed
+        plain_sym_ms, pairs = 0.0, 0.0
+        for q in range(4):
+            sel = shard_blocks(sub_gt, sub_gs, q, 4)
+            eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt[sel], gs=sub_gs[sel])
+            eng.set_symmetric(True)
+            eng.compress(TOL, **PLAIN)  # warm-up of this batch's tables
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.compress(TOL, **PLAIN)
+            e1.record()
+            torch.cuda.synchronize()
+            plain_sym_ms += e0.elapsed_time(e1)
+            pairs += eng.timing()["point_pairs"]
+        t_plain = dict(point_pairs=pairs)
+        eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt, gs=sub_gs)
+    mixed_ms = learned_ms = lm_nosym_ms = lsym128_ms = None
+    if not large:
+        mixed_only = without_symmetry(lambda: eng.compress(TOL, **dict(PLAIN, precision="c64")))
+        mixed_ms, _, _, _ = timed(mixed_only, 1, 1)
+        learned_only = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True,
+                                                             **dict(PRODUCT, precision="c128")))
+        learned_ms, _, _, _ = timed(learned_only, 1, 2)
+        lm_nosym = without_symmetry(lambda: eng.compress(TOL, r0=predict_r0(), use_graph=True, **PRODUCT))
+        lm_nosym_ms, _, _, _ = timed(lm_nosym, 1, 2)
+
+        # learned + batched + symmetric in complex FP64: the same-precision counterpart of the
+        # ACA comparison (which computes in complex FP64)
+        def learned_sym_c128():
+            eng.set_symmetric(True)
+            return eng.compress(TOL, r0=predict_r0(), use_graph=True, **dict(PRODUCT, precision="c128"))
+        lsym128_ms, _, _, _ = timed(learned_sym_c128, 1, 2)
     # per-phase timing of the product without the graph (roofline of the fill)
     eng.set_symmetric(True)
     r0 = predict_r0()
@@ -357,15 +387,16 @@ def run_ours(args, rank, world, dev):
     st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     err = eng.true_errors()
     err_plain = None
-    if not args.no_plain_errors:
+    if not (args.no_plain_errors or large):
         eng.set_symmetric(False)
         st_plain = eng.compress(TOL, **PLAIN)
         err_plain = eng.true_errors()
         eng.set_symmetric(True)
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
-    blockops = run_blockops(eng, st, m, flush)
+    blockops = run_blockops(eng, st, m, flush, recompress=not large)
+    footprint = run_footprint(eng, st, part, blockops)
     config3 = None
-    if not args.no_config3:
+    if not (args.no_config3 or large):
         def r0_for(tol):
             fe = features(sp, K_WAVE, tol)
             y = pred.predict_log2(fe)
@@ -374,7 +405,7 @@ def run_ours(args, rank, world, dev):
         eng.set_symmetric(True)
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     octree_t = run_octree(args, m, part, dev) if rank == 0 else None
-    aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only) else None
+    aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only and not large) else None
     # e2e: the public call path from host buffers: mesh + groups + features up, stats down
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
                                    fill_choice=tune["choice"])
@@ -398,17 +429,15 @@ def run_ours(args, rank, world, dev):
                     symmetry="one block of each (t,s)/(s,t) pair compressed, the other taken as its "
                              "transpose (Galerkin Z = Z^T); every block's error measured against its "
                              "own dense FP64 fill"),
-        plain_ms=round(plain_ms, 3), speedup_vs_plain=round(plain_ms / ms, 3),
+        plain_ms=None if plain_ms is None else round(plain_ms, 3),
+        speedup_vs_plain=None if plain_ms is None else round(plain_ms / ms, 3),
         plain_desc="plain FP64 GPU pseudoskeleton: start min(m,n)/10, doubling, same estimator, "
                    "driven one block at a time (the reference's per-block driving)",
-        ablation_ms=dict(plain_batched=round(plain_b_ms, 3),
-                         plain_batched_symmetric=round(plain_sym_ms, 3),
-                         mixed_batched=round(mixed_ms, 3),
-                         learned_batched=round(learned_ms, 3),
-                         learned_mixed_batched=round(lm_nosym_ms, 3),
-                         learned_mixed_batched_symmetric=round(ms, 3),
-                         learned_batched_symmetric_c128=round(lsym128_ms, 3)),
-        speedup_vs_plain_batched=round(plain_b_ms / ms, 3),
+        ablation_ms={k: (None if v is None else round(v, 3)) for k, v in dict(
+            plain_batched=plain_b_ms, plain_batched_symmetric=plain_sym_ms, mixed_batched=mixed_ms,
+            learned_batched=learned_ms, learned_mixed_batched=lm_nosym_ms,
+            learned_mixed_batched_symmetric=ms, learned_batched_symmetric_c128=lsym128_ms).items()},
+        speedup_vs_plain_batched=None if plain_b_ms is None else round(plain_b_ms / ms, 3),
         speedup_three_patterns=round(plain_sym_ms / ms, 3),
         speedup_three_patterns_desc="plain FP64 batched with the symmetric mode / the product: the "
                                     "learned first sample count, complex-FP32 fill and graph "
@@ -422,7 +451,8 @@ def run_ours(args, rank, world, dev):
                      err_max=float(err.max()), err_median=float(np.median(err)),
                      blocks_over_tol=int((err > TOL).sum()),
                      fill_point_pairs=float(tph["point_pairs"])),
-        plain=dict(r_mean=float(st_plain["r"].mean()), rounds_mean=float(st_plain["rounds"].mean()),
+        plain=dict(r_mean=None if st_plain is None else float(st_plain["r"].mean()),
+                   rounds_mean=None if st_plain is None else float(st_plain["rounds"].mean()),
                    fill_point_pairs=float(t_plain["point_pairs"]),
                    err_max=None if err_plain is None else float(err_plain.max()),
                    blocks_over_tol=None if err_plain is None else int((err_plain > TOL).sum())),
@@ -445,6 +475,7 @@ def run_ours(args, rank, world, dev):
                  d2h_bytes_per_step=int(d2h)),
         clocks=clocks, gpu_launches=int(launches),
         blockops=blockops,
+        footprint=footprint,
         mixed_precision=config3,
         octree=octree_t,
         aca=aca_t,
@@ -453,7 +484,7 @@ def run_ours(args, rank, world, dev):
     return out
 
 
-def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
+def run_blockops(eng, st, m, flush, nrhs=16, reps=10, recompress=True):
     """Compressed far-field matvec (nrhs right-hand sides, complex64 like the stored factors)
     and FP64 recompression of every block, after the product compression."""
     import torch
@@ -484,6 +515,16 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     flops = roofline.matvec_flops(mm, nn, rr, nrhs)
     peak = _hbm_peak()
     gbs = (factor_bytes + vec_bytes) / (mv_ms * 1e-3) / 1e9
+    matvec_out = dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),
+                      factor_bytes=factor_bytes, vector_bytes=vec_bytes,
+                      achieved_gbs=round(gbs, 1), peak_gbs=peak, frac=round(gbs / peak, 4),
+                      gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
+                      bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
+                            "once each per call (algorithmic)")
+    if not recompress:
+        return dict(matvec=matvec_out, store_matvec=None, recompress=None,
+                    note="recompression and store skipped: the recompression workspace of every "
+                         "block does not fit the device at this size")
     # recompression to the compression tolerance (device time of its launches, from the
     # library's own events on its stream)
     eng.recompress(TOL)
@@ -519,12 +560,7 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
     st_alg_bytes = roofline.store_matvec_bytes(mm, nn, kk, m.N, nrhs)
     st_gbs = st_alg_bytes / (st_ms * 1e-3) / 1e9
     return dict(
-        matvec=dict(ms=round(mv_ms, 4), nrhs=nrhs, arithmetic="complex64", launches=int(mv_launches),
-                    factor_bytes=factor_bytes, vector_bytes=vec_bytes,
-                    achieved_gbs=round(gbs, 1), peak_gbs=peak, frac=round(gbs / peak, 4),
-                    gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
-                    bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
-                          "once each per call (algorithmic)"),
+        matvec=matvec_out,
         store_matvec=dict(ms=round(st_ms, 4), nrhs=nrhs, launches=int(st_launches),
                           status=int(st_status), store_bytes=store_bytes,
                           build_ms=round(build_ms, 3), algorithmic_bytes=st_alg_bytes,
@@ -543,6 +579,34 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10):
 
 
 STORE_ENTRY_BYTES = {"bf16x3": 8.0, "tf32": 8.0, "tf32x3": 16.0}  # per complex factor entry
+
+
+def run_footprint(eng, st, part, blockops):
+    """Memory of the compressed far field against the dense far-field blocks (complex FP64)."""
+    mirror = eng.mirror_of()
+    own = np.array([p < 0 or b < p for b, p in enumerate(mirror)]) if eng_symmetric(eng) else \
+        np.ones(len(mirror), dtype=bool)
+    sz = part.sizes().astype(np.float64)
+    dense_far = float((sz[part.gt] * sz[part.gs]).sum()) * 16
+    mm, nn, rr = (st[k][own].astype(np.float64) for k in ("m", "n", "r"))
+    cur = float(((mm + nn) * rr * 8 + rr * rr * 16).sum())  # C, R complex64; U complex128
+    recomp = store = None
+    if blockops.get("store_matvec"):
+        kk = np.asarray(eng._recomp_k, dtype=np.float64)[own]
+        recomp = float(((mm + nn) * kk * 16 + kk * 8).sum())    # C', R' complex128; S
+        store = float(blockops["store_matvec"]["store_bytes"])
+    frac = lambda x: None if x is None else x / dense_far
+    return dict(dense_far_bytes=dense_far, dense_all_bytes=float(eng.mesh.N) ** 2 * 16,
+                cur_bytes=cur, cur_frac=cur / dense_far, recompressed_bytes=recomp,
+                recompressed_frac=frac(recomp), store_bytes=store, store_frac=frac(store),
+                desc="blocks that keep factors (a mirrored block is its partner's transpose): CUR "
+                     "factors as compressed (C, R complex64, U complex128), recompressed C' S R' in "
+                     "FP64, and the bf16 hi/lo tensor-core store; against the far blocks' dense "
+                     "complex-FP64 entries")
+
+
+def eng_symmetric(eng) -> bool:
+    return bool(getattr(eng, "_symmetric", False))
 
 
 def run_config3(eng, m, r0_for, nrhs=16, reps=5):
@@ -844,6 +908,9 @@ def main():
     ap.add_argument("--no-plain-errors", action="store_true",
                     help="skip the dense-fill error check of the plain baseline's blocks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--large", action="store_true",
+                    help="skip the per-block plain run, the ablations beside plain batched, ACA and "
+                         "the mixed-precision report (automatic for sphere122k)")
     ap.add_argument("--no-config3", action="store_true",
                     help="skip the mixed-precision report (store formats against the dense product)")
     ap.add_argument("--fill-variant", default=None,

@@ -130,7 +130,7 @@ struct pskel_ctx {
     static constexpr int kMaxChunks = 8;
     cudaStream_t pipe_stream = nullptr;
     cudaEvent_t pipe_ev[kMaxChunks + 1] = {};
-    int pipe_chunks = 4;        // chunks of a round with at least kPipeMinBlocks blocks (1: off)
+    int pipe_chunks = 2;        // chunks of a round with at least kPipeMinBlocks blocks (1: off)
     DevMesh mesh;
     pskel_em_t em{};
     bool have_mesh = false;

@@ -360,7 +360,7 @@ class Engine:
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
     def set_pipeline(self, chunks: int):
-        """Chunks of a pipelined compression round (1 = off; default 4): the fill of one chunk
+        """Chunks of a pipelined compression round (1 = off; default 2): the fill of one chunk
         overlaps the SVD, pinv and estimate of the previous one."""
         _lib.check(self._lib.pskel_set_pipeline(self._h, int(chunks)))
 
@@ -368,6 +368,7 @@ class Engine:
         """Compress one block of each (t, s) / (s, t) pair and take the other as its transpose
         (Galerkin symmetry Z = Z^T)."""
         _lib.check(self._lib.pskel_set_symmetric(self._h, int(bool(on))))
+        self._symmetric = bool(on)
 
     def mirror_of(self) -> np.ndarray:
         """Per block: the index of the block with swapped groups (-1 if none)."""

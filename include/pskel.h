@@ -264,7 +264,7 @@ int pskel_compress_blocks(pskel_ctx *ctx, const pskel_opts_t *opts, const int *r
 int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
 
 /* Pipelining of a compression round of at least 2048 blocks: the blocks split into `chunks`
-   (1 .. 8; default 4; 1 = off) of about equal fill work; the fill of chunk k + 1 (one CTA per
+   (1 .. 8; default 2; 1 = off) of decreasing fill work; the fill of chunk k + 1 (one CTA per
    tile) overlaps the core SVD, pinv and estimate of chunk k, which run on a high-priority
    stream. The results are those of the unpipelined round. In a pipelined round the timing's
    fill phase covers all fills with the earlier chunks' pinv and estimate beside them, and the
