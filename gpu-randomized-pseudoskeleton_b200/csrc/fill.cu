@@ -437,13 +437,13 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     auto kern = fill2_kernel<T, Q, TM, TN>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
-    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = p.persistent ? (long long)sm_count() * per_sm : (long long)total_tiles;
     if (grid > total_tiles) grid = total_tiles;
     if (grid < 1) return PSKEL_OK;
     const double pi = 3.14159265358979323846;
-    kern<<<(int)grid, 256, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
+    kern<<<(int)grid, NT, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
                                           (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)),
                                           p.r_near > 0 ? p.r_near * p.r_near : 0.0, d_flags);
     PSKEL_LAUNCHED(1);
@@ -462,7 +462,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     auto kern = fill_kernel<T, Q, TM, TN, SPLIT>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
-    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
+    PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
     if (per_sm < 1) per_sm = 1;
     long long grid = p.persistent ? (long long)sm_count() * per_sm : (long long)total_tiles;
     if (grid > total_tiles) grid = total_tiles;
@@ -473,7 +473,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     const double kphase = sizeof(T) == 8 ? p.k / pi : p.k / (2.0 * pi);
     const T scale = (T)(p.eta / (4.0 * pi));
     const double rn2 = p.r_near > 0 ? p.r_near * p.r_near : 0.0;
-    kern<<<(int)grid, 256, smem, stream>>>(rec_t, rec_s, d_jobs, d_prefix, njobs, total_tiles, k,
+    kern<<<(int)grid, NT, smem, stream>>>(rec_t, rec_s, d_jobs, d_prefix, njobs, total_tiles, k,
                                           kinv, kphase, scale, rn2, d_flags);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;
