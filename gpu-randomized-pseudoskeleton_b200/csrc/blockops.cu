@@ -431,36 +431,24 @@ __global__ void recomp_rp_kernel(const RecompBlock *__restrict__ jobs) {
 
 }  // namespace pskel
 
-extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
-    if (!c || !(thresh >= 0) || c->n_blocks <= 0) {
-        set_error(PSKEL_ERR_ARG, "recompress: bad arguments");
-        return PSKEL_ERR_ARG;
-    }
-    PSKEL_CUDA(cudaSetDevice(c->device));
-    const int nball = c->n_blocks;
+namespace pskel {
+
+// FP64 recompression of the primary blocks `prims` into c->recomp64 (factors and workspace);
+// fills their slots.
+int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh) {
+    const int nb = (int)prims.size();
+    if (nb == 0) return PSKEL_OK;
     const bool f32 = c->precision == PSKEL_C64;
     auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
-    // only blocks with their own factors are recompressed; a mirror block takes its primary's
-    // recompression transposed
-    std::vector<int> prims;
-    for (int b = 0; b < nball; ++b) {
-        if (c->results[b].arena < 0) {
-            set_error(PSKEL_ERR_STATE, "recompress: block %d has no retained factors", b);
-            return PSKEL_ERR_STATE;
-        }
-        if (c->results[b].mirror < 0) prims.push_back(b);
-    }
-    const int nb = (int)prims.size();
     std::vector<size_t> off(nb + 1, 0);
     for (int pi = 0; pi < nb; ++pi) {
-        const int b = prims[pi];
-        const BlockResult &res = c->results[b];
+        const BlockResult &res = c->results[prims[pi]];
         const size_t m = res.m, n = res.n, r = res.r;
         off[pi + 1] = off[pi] + 2 * al(16 * m * r) + 3 * al(16 * n * r) + 8 * al(16 * r * r) +
                      2 * al(16 * r) + 4 * al(8 * r) + al(4 * r) + 256;
     }
-    PSKEL_TRY(c->recomp.reserve(off[nb] + 256));
-    char *base = c->recomp.as<char>();
+    PSKEL_TRY(c->recomp64.reserve(off[nb] + 256));
+    char *base = c->recomp64.as<char>();
     std::vector<RecompBlock> jobs(nb);
     std::vector<QrJob> qrs;
     qrs.reserve(2 * nb);
@@ -469,7 +457,6 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     std::vector<ZgemmJob> g1, g2;
     std::vector<ApplyQJob> aps;
     aps.reserve(2 * nb);
-    c->recomp_slots.assign(nball, {});
     // device job tables (the k table is referenced by the apply jobs)
     const size_t jb = sizeof(RecompBlock) * nb, s2 = sizeof(SvdJob) * nb;
     PSKEL_TRY(c->tmp.reserve(al(jb) + al(s2) + sizeof(int) * nb + 1024));
@@ -522,12 +509,15 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         svds.push_back(SvdJob{w.M, w.Vm, w.sm, w.pm, res.r, res.r, 0, 0});
         aps.push_back(ApplyQJob{w.Bc, w.v0c, w.cc, res.m, res.r, w.Zc, res.r, w.Cp, res.m, res.r, w.kout});
         aps.push_back(ApplyQJob{w.Br, w.v0r, w.cr, res.n, res.r, w.Zr, res.r, w.RpH, res.n, res.r, w.kout});
-        c->recomp_slots[b] = RecompSlot{(size_t)((char *)w.Cp - base), (size_t)((char *)w.Rp - base),
-                                        (size_t)((char *)w.S - base), 0, -1};
+        RecompSlot &sl = c->recomp_slots[b];
+        sl.Cp = w.Cp;
+        sl.Rp = w.Rp;
+        sl.S = w.S;
+        sl.ldrp = res.r;
+        sl.mirror = -1;
     }
     PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, c->stream));
-    PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
     if (f32) recomp_load_kernel<float2><<<nb, 256, 0, c->stream>>>(d_jobs);
     else recomp_load_kernel<double2><<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
@@ -540,24 +530,78 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
     PSKEL_TRY(batched_apply_q(aps, c->stream, c->tmp3));
     recomp_rp_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
     // ranks and SVD statuses back to the host
     std::vector<SvdJob> h2(nb);
     std::vector<int> ks(nb);
     PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaMemcpyAsync(ks.data(), d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
-    {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
-        c->timing[4] = ms;
-    }
     for (const SvdJob &j : h2)
         if (j.status != PSKEL_OK) {
             set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a core did not converge");
             return PSKEL_ERR_NOCONV;
         }
     for (int pi = 0; pi < nb; ++pi) c->recomp_slots[prims[pi]].k = ks[pi];
+    return PSKEL_OK;
+}
+
+}  // namespace pskel
+
+extern "C" int pskel_set_recompress_path(pskel_ctx *c, int path) {
+    if (!c || path < 0 || path > 2) {
+        set_error(PSKEL_ERR_ARG, "set_recompress_path: path must be 0 (auto), 1 (FP64) or 2 (split)");
+        return PSKEL_ERR_ARG;
+    }
+    c->recomp_path = path;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_recompress_split_blocks(pskel_ctx *c, int *split_blocks) {
+    if (!c || !split_blocks) {
+        set_error(PSKEL_ERR_ARG, "recompress_split_blocks: null argument");
+        return PSKEL_ERR_ARG;
+    }
+    *split_blocks = c->recomp_split_blocks;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
+    if (!c || !(thresh >= 0) || !(thresh < 1) || c->n_blocks <= 0) {
+        set_error(PSKEL_ERR_ARG, "recompress: bad arguments");
+        return PSKEL_ERR_ARG;
+    }
+    PSKEL_CUDA(cudaSetDevice(c->device));
+    const int nball = c->n_blocks;
+    // only blocks with their own factors are recompressed; a mirror block takes its primary's
+    // recompression transposed
+    std::vector<int> prims;
+    for (int b = 0; b < nball; ++b) {
+        if (c->results[b].arena < 0) {
+            set_error(PSKEL_ERR_STATE, "recompress: block %d has no retained factors", b);
+            return PSKEL_ERR_STATE;
+        }
+        if (c->results[b].mirror < 0) prims.push_back(b);
+    }
+    c->recomp_slots.assign(nball, RecompSlot{});
+    // the split path (tensor cores, TF32 hi + lo operands) takes the complex-FP32 compressions
+    // at thresholds of 1e-5 and above; it hands back the blocks it cannot take
+    std::vector<int> split, fp64;
+    for (int b : prims)
+        if (recomp_split_eligible(c, b, thresh)) split.push_back(b);
+        else fp64.push_back(b);
+    PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    std::vector<int> rejected;
+    PSKEL_TRY(recompress_split(c, split, thresh, rejected));
+    c->recomp_split_blocks = (int)(split.size() - rejected.size());
+    fp64.insert(fp64.end(), rejected.begin(), rejected.end());
+    PSKEL_TRY(recompress_fp64(c, fp64, thresh));
+    PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
+    PSKEL_CUDA(cudaEventSynchronize(c->ev[4]));
+    {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[4]);
+        c->timing[4] = ms;
+    }
     for (int b = 0; b < nball; ++b) {
         const int mb = c->results[b].mirror;
         if (mb >= 0) {
@@ -591,17 +635,16 @@ extern "C" int pskel_get_recompressed(pskel_ctx *c, int b, pskel_c128 *Cp, doubl
         return PSKEL_OK;
     }
     const BlockResult &res = c->results[b];
-    const char *base = c->recomp.as<char>();
     const size_t k = sl.k;
-    if (Cp) PSKEL_CUDA(cudaMemcpy(Cp, base + sl.offCp, 16 * (size_t)res.m * k, cudaMemcpyDeviceToHost));
-    if (S) PSKEL_CUDA(cudaMemcpy(S, base + sl.offS, 8 * k, cudaMemcpyDeviceToHost));
+    if (Cp) PSKEL_CUDA(cudaMemcpy(Cp, sl.Cp, 16 * (size_t)res.m * k, cudaMemcpyDeviceToHost));
+    if (S) PSKEL_CUDA(cudaMemcpy(S, sl.S, 8 * k, cudaMemcpyDeviceToHost));
     if (Rp) {
-        // R' is stored r x n (ld r): copy its first k rows
-        std::vector<double2> h((size_t)res.r * res.n);
-        PSKEL_CUDA(cudaMemcpy(h.data(), base + sl.offRp, 16 * h.size(), cudaMemcpyDeviceToHost));
+        // R' is stored k x n with leading dimension ldrp >= k: copy its first k rows
+        std::vector<double2> h((size_t)sl.ldrp * res.n);
+        PSKEL_CUDA(cudaMemcpy(h.data(), sl.Rp, 16 * h.size(), cudaMemcpyDeviceToHost));
         for (int j = 0; j < res.n; ++j)
             for (size_t t = 0; t < k; ++t) {
-                const double2 v = h[t + (size_t)j * res.r];
+                const double2 v = h[t + (size_t)j * sl.ldrp];
                 Rp[t + j * k] = pskel_c128{v.x, v.y};
             }
     }

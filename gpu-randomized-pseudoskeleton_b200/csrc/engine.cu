@@ -604,6 +604,10 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         res.offU = (char *)w.U - kb;
         res.offI = (char *)w.I - kb;
         res.offJ = (char *)w.J - kb;
+        res.offAV = (char *)w.AV - sb;
+        res.offV = (char *)w.V - sb;
+        res.offSig = (char *)w.sigma - kb;
+        res.offPerm = (char *)w.perm - kb;
     }
     // fill tile prefix
     int tm, tn;
@@ -995,7 +999,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec1.f64.release();
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
-    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->mv_table.release();
+    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->rc_work.release(); c->rc_tab.release(); c->mv_table.release();
     for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     svd_streams_destroy(c->svd_par);

@@ -27,28 +27,6 @@ struct BlockWork {
     double *est;
 };
 
-// One core of a round with r <= 32 for warp_core_kernel (csrc/warp_core.cu): the core is
-// gathered from C, its numbers written into R(:, J), and its truncated pseudo-inverse formed by
-// one warp.
-constexpr int kWarpCoreMaxN = 32;
-constexpr int kWarpCoreThreads = 128;
-struct WarpCoreJob {
-    const void *C;       // m x (r + pc), ld m (storage type of the round)
-    void *Rx;            // (r + pe) x n, ld ldr
-    const int *I, *J;    // local samples
-    double2 *U;          // n x n out: the pinv
-    double2 *refl;       // n x n scratch: reflector tails
-    double2 *qw;         // n x n scratch: Q W
-    double *sigma;       // n out (column order of the Jacobi)
-    int *rank;           // out
-    int m, ldr, n;
-    double tau;
-    int relative;
-    int svd_index;       // entry of the round's SvdJob table that receives status and sweeps
-};
-int launch_warp_core(const WarpCoreJob *d_jobs, int count, SvdJob *d_svd, int max_sweeps,
-                     int precision, cudaStream_t stream);
-
 // Single-level octree partition of the uploaded mesh's RWG basis centres and its far-pair list,
 // built on the device (csrc/octree.cu). Group ids, extents and the far list stay in device
 // memory; offsets and centres are kept on the host as well.
@@ -74,6 +52,9 @@ struct BlockResult {
     double est = 0;
     int arena = -1;
     size_t offC = 0, offRx = 0, offU = 0, offI = 0, offJ = 0;
+    // the core's SVD from the pinv (offsets in the round arena): A V (work, r x r), V (work,
+    // r x r), sigma and its decreasing order (keep); `rank` columns were kept by the pinv
+    size_t offAV = 0, offV = 0, offSig = 0, offPerm = 0;
     // >= 0: this block is the transpose of block `mirror` (Galerkin symmetry Z = Z^T), whose
     // factors it shares: C = R_p^T, U = U_p^T, R = C_p^T, I = J_p, J = I_p. m and n are this
     // block's own sizes; the other fields describe the primary's storage.
@@ -90,9 +71,12 @@ struct RoundArena {
 };
 
 struct RecompSlot {
-    size_t offCp, offRp, offS;
-    int k;
-    int mirror;  // >= 0: the transpose of that block's recompression (offsets are its)
+    double2 *Cp = nullptr;  // m x k, ld m
+    double2 *Rp = nullptr;  // k x n, ld ldrp (>= k)
+    double *S = nullptr;    // k, decreasing
+    int k = 0;
+    int mirror = -1;  // >= 0: the transpose of that block's recompression (pointers are its)
+    int ldrp = 0;
 };
 
 // Compressed store of the recompressed blocks (csrc/store.cu): host copy of its layout.
@@ -163,8 +147,12 @@ struct pskel_ctx {
     std::vector<int> graph_key;
     std::vector<int> last_key;  // round-0 key of the previous call (capture on a repeat)
     DevBuf tmp, tmp2, tmp3;
-    DevBuf recomp;                          // recompressed factors and their workspace
-    std::vector<RecompSlot> recomp_slots;   // per block: offsets of C', R', S and the rank k
+    DevBuf recomp;                          // recompressed factors (split path, loaded store)
+    DevBuf recomp64;                        // FP64 path: recompressed factors and workspace
+    DevBuf rc_work, rc_tab;                 // split path: workspace and job tables
+    int recomp_path = 0;                    // 0 auto, 1 FP64 only, 2 split whenever eligible
+    int recomp_split_blocks = 0;            // blocks of the last recompression on the split path
+    std::vector<RecompSlot> recomp_slots;   // per block: C', R', S and the rank k
     long long generation = 0;               // incremented by every compression
     DevBuf mv_table;                        // matvec block table (built once per compression)
     long long mv_generation = -1;
@@ -184,3 +172,10 @@ struct pskel_ctx {
     float aca_ms = 0.0f;
 };
 
+namespace pskel {
+// Recompression (csrc/blockops.cu, csrc/recomp_tc.cu) of primary blocks: the FP64 path, and the
+// split-precision tensor-core path with the blocks it hands back to the FP64 one.
+int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh);
+bool recomp_split_eligible(const pskel_ctx *c, int b, double thresh);
+int recompress_split(pskel_ctx *c, const std::vector<int> &blocks, double thresh, std::vector<int> &rejected);
+}  // namespace pskel

@@ -39,6 +39,7 @@
 #include <cuda_bf16.h>
 
 #include "engine_internal.cuh"
+#include "tcgen05.cuh"
 
 namespace pskel {
 
@@ -50,7 +51,6 @@ constexpr int kStStageABytes = 8 * kStTileM * 16;  // 16 KB per plane: 8 chunks 
 constexpr int kStStageBBytes = 8 * kStN * 16;      // 4 KB per plane: 8 chunks of 32 columns
 constexpr int kStStageBytes = 2 * kStStageABytes + 2 * kStStageBBytes;  // two planes at most
 constexpr size_t kStSmem = (size_t)kStStages * kStStageBytes + 1024;
-constexpr long long kStWaitLimit = 1ll << 22;  // try_wait polls before a wait counts as lost
 constexpr int kStSliceStages = 8;             // phase-2 K slice per work item (512 K values)
 
 // Element type, elements per 16-byte chunk and planes of each format
@@ -82,12 +82,6 @@ __host__ __device__ __forceinline__ long long st_b_off(long long base, int col, 
     return base + ((long long)(k / EPC) * kStN + col) * EPC + k % EPC;
 }
 
-// FP32 rounded to TF32 (10 explicit mantissa bits), to nearest with ties away from zero; the
-// low 13 bits are cleared (finite inputs)
-__device__ __forceinline__ float tf32_round(float x) {
-    return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
-}
-
 // x as the format's hi (and lo) plane values
 __device__ __forceinline__ void st_split(float x, __nv_bfloat16 *hi, __nv_bfloat16 *lo) {
     const __nv_bfloat16 h = __float2bfloat16_rn(x);
@@ -105,7 +99,7 @@ struct PackBlock {
     const double2 *Cp;  // m x r (ld ldcp), first k columns
     const double2 *Rp;  // r x n (ld r), first k rows
     const double *S;    // k
-    int m, n, r, k;
+    int m, n, r, k;     // r: leading dimension of Rp
     int trans, ldcp;    // trans: mirror block, Cp and Rp are its primary's (C' = R'_p^T, R' = C'_p^T)
     long long a1_base;  // phase-1 group base (elements) and the block's first row in it
     int a1_kc, a1_row0;
@@ -231,96 +225,17 @@ struct StItem {
     const int *ids;   // phase 2: RWG ids of the tile's rows (null in phase 1)
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// no-swizzle K-major UMMA shared-memory descriptor: start, leading byte offset (distance of the
-// two 16-byte K chunks of one K = 16 step), stride byte offset (distance of 8-row core matrices)
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version of sm_100
-    return d;                // base offset 0, absolute LBO mode, layout type 0 (no swizzle)
-}
-
 // instruction descriptors, FP32 D, both operands K-major, M = 128, N = 32:
 // kind::f16 with bf16 A and B (format 1), kind::tf32 with TF32 A and B (format 2)
-constexpr uint32_t kStIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kStN >> 3) << 17) |
-                                  ((uint32_t)(kStTileM >> 4) << 24);
-constexpr uint32_t kStIdescTf32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kStN >> 3) << 17) |
-                                  ((uint32_t)(kStTileM >> 4) << 24);
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// bounded wait; false when it ran out or the CTA aborted
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, volatile int *abort) {
-    for (long long i = 0; i < kStWaitLimit; ++i) {
-        if (mbar_try(bar, parity)) return true;
-        if (*abort) return false;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
+constexpr uint32_t kStIdescBf16 = umma_idesc(1, kStTileM, kStN);
+constexpr uint32_t kStIdescTf32 = umma_idesc(2, kStTileM, kStN);
 
 // one MMA of the format: kind::f16 (bf16, K = 16) or kind::tf32 (K = 8); 32 bytes of K per row
 template <int MODE>
 __device__ __forceinline__ void umma_st(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                         uint32_t accumulate) {
-    const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
-    if constexpr (MODE == PSKEL_STORE_BF16X3) {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-            "l"(adesc), "l"(bdesc), "r"(kStIdescBf16), "r"(accumulate), "r"(mask0), "r"(mask1),
-            "r"(mask2), "r"(mask3));
-    } else {
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "setp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-            "l"(adesc), "l"(bdesc), "r"(kStIdescTf32), "r"(accumulate), "r"(mask0), "r"(mask1),
-            "r"(mask2), "r"(mask3));
-    }
-}
-
-__device__ __forceinline__ void umma_commit(uint64_t *bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+    if constexpr (MODE == PSKEL_STORE_BF16X3) umma_f16(tmem_d, adesc, bdesc, kStIdescBf16, accumulate);
+    else umma_tf32(tmem_d, adesc, bdesc, kStIdescTf32, accumulate);
 }
 
 // Persistent grouped GEMM, one CTA per SM, warp-specialised:
@@ -364,10 +279,7 @@ __global__ void __launch_bounds__(192, 1)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(&tmem_slot)),
-                     "r"(2 * kStN));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        tmem_alloc(&tmem_slot, 2 * kStN);
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -471,17 +383,7 @@ __global__ void __launch_bounds__(192, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             uint32_t v[32];
             const uint32_t taddr = tmem + (uint32_t)(acc * kStN) + ((uint32_t)(quad * 32) << 16);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-                "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
-                "%28, %29, %30, %31}, [%32];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
-                  "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
-                  "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                : "r"(taddr));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            tmem_ld32(taddr, v);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty_bar[acc]);  // the accumulator may be reused
@@ -509,7 +411,7 @@ __global__ void __launch_bounds__(192, 1)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kStN));
+        tmem_dealloc(tmem, 2 * kStN);
 }
 
 }  // namespace pskel
@@ -553,7 +455,6 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
     auto gsize = [&](int g) { return c->gptr[g + 1] - c->gptr[g]; };
     auto pad = [](long long x, long long a) { return (x + a - 1) / a * a; };
     std::vector<PackBlock> pb(nb);
-    const char *rbase = c->recomp.as<char>();
     // phase 1: per source group
     long long a1 = 0, b1 = 0;
     int trow = 0;
@@ -615,12 +516,12 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
         const RecompSlot &sl = c->recomp_slots[b];
         const BlockResult &res = c->results[b];
         PackBlock &w = pb[b];
-        w.Cp = reinterpret_cast<const double2 *>(rbase + sl.offCp);
-        w.Rp = reinterpret_cast<const double2 *>(rbase + sl.offRp);
-        w.S = reinterpret_cast<const double *>(rbase + sl.offS);
+        w.Cp = sl.Cp;
+        w.Rp = sl.Rp;
+        w.S = sl.S;
         w.m = res.m;
         w.n = res.n;
-        w.r = res.r;
+        w.r = sl.ldrp;  // leading dimension of the (primary's) R
         w.k = sl.k;
         w.trans = sl.mirror >= 0 ? 1 : 0;
         w.ldcp = sl.mirror >= 0 ? c->results[sl.mirror].m : res.m;

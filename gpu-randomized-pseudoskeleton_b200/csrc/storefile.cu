@@ -115,7 +115,6 @@ extern "C" int pskel_store_save(pskel_ctx *c, const char *path, double thresh) {
                             c->recomp_slots[b].mirror};
         w.put(rec, sizeof(rec));
     }
-    const char *base = c->recomp.as<char>();
     std::vector<double2> hbuf;
     std::vector<double> hs;
     int st = PSKEL_OK;
@@ -123,18 +122,18 @@ extern "C" int pskel_store_save(pskel_ctx *c, const char *path, double thresh) {
         const RecompSlot &sl = c->recomp_slots[b];
         if (sl.mirror >= 0) continue;
         const BlockResult &res = c->results[b];
-        const size_t m = res.m, n = res.n, k = sl.k, ld = res.r;
+        const size_t m = res.m, n = res.n, k = sl.k, ld = sl.ldrp;
         hbuf.resize(std::max(m * k, ld * n) + 1);
         hs.resize(k + 1);
-        if (cudaMemcpy(hbuf.data(), base + sl.offCp, 16 * m * k, cudaMemcpyDeviceToHost) != cudaSuccess ||
-            cudaMemcpy(hs.data(), base + sl.offS, 8 * k, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (cudaMemcpy(hbuf.data(), sl.Cp, 16 * m * k, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(hs.data(), sl.S, 8 * k, cudaMemcpyDeviceToHost) != cudaSuccess) {
             st = PSKEL_ERR_CUDA;
             break;
         }
         w.put(hbuf.data(), 16 * m * k);
         w.put(hs.data(), 8 * k);
-        // R' is kept r x n with leading dimension r: write its first k rows
-        if (cudaMemcpy(hbuf.data(), base + sl.offRp, 16 * ld * n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        // R' is kept k x n with leading dimension ldrp >= k: write its first k rows
+        if (cudaMemcpy(hbuf.data(), sl.Rp, 16 * ld * n, cudaMemcpyDeviceToHost) != cudaSuccess) {
             st = PSKEL_ERR_CUDA;
             break;
         }
@@ -279,12 +278,19 @@ static int store_load_impl(pskel_ctx *c, const char *path, int *n_blocks) {
         BlockResult &res = c->results[b];
         res.m = m;
         res.n = n;
-        res.r = k;  // R' is stored with leading dimension k
+        res.r = k;
         res.arena = -1;
         res.mirror = mir;
         if (mir < 0) {
             const size_t cm = al256(16 * (size_t)m * k);
-            c->recomp_slots[b] = RecompSlot{off[b], off[b] + cm + al256(8 * (size_t)k), off[b] + cm, k, -1};
+            char *p = c->recomp.as<char>() + off[b];
+            RecompSlot &sl = c->recomp_slots[b];
+            sl.Cp = reinterpret_cast<double2 *>(p);
+            sl.S = reinterpret_cast<double *>(p + cm);
+            sl.Rp = reinterpret_cast<double2 *>(p + cm + al256(8 * (size_t)k));
+            sl.k = k;
+            sl.ldrp = k;  // R' is stored with leading dimension k
+            sl.mirror = -1;
         }
     }
     for (int b = 0; b < B; ++b) {

@@ -99,6 +99,8 @@ SIGNATURES = {
     "pskel_octree_get": (ci, [VP, I32, I32, D, D, I32, I32]),
     "pskel_matvec": (ci, [VP, VP, ci, VP, ci, ci, ci, VP]),
     "pskel_recompress": (ci, [VP, cd, I32]),
+    "pskel_set_recompress_path": (ci, [VP, ci]),
+    "pskel_recompress_split_blocks": (ci, [VP, I32]),
     "pskel_get_recompressed": (ci, [VP, ci, VP, D, VP]),
     "pskel_store_build": (ci, [VP, ctypes.POINTER(ctypes.c_longlong)]),
     "pskel_store_build_mode": (ci, [VP, ci, ctypes.POINTER(ctypes.c_longlong)]),

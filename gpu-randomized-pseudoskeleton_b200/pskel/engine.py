@@ -246,13 +246,25 @@ class Engine:
                                           ctypes.c_void_p(s)))
         return Y.t()
 
-    def recompress(self, thresh: float) -> np.ndarray:
-        """SVD-truncate every block's C U R to C' diag(S) R' (S > thresh * S_max, FP64);
-        returns the kept rank per block."""
+    RECOMPRESS_PATHS = {"auto": 0, "fp64": 1, "split": 2}
+
+    def recompress(self, thresh: float, path: str | None = None) -> np.ndarray:
+        """SVD-truncate every block's C U R to C' diag(S) R' (S > thresh * S_max); returns the
+        kept rank per block. path: None keeps the context's setting, else "auto" (the split
+        tensor-core path for complex-FP32 compressions at thresh >= 1e-5, FP64 otherwise),
+        "fp64" or "split" (every eligible block, any threshold)."""
+        if path is not None:
+            _lib.check(self._lib.pskel_set_recompress_path(self._h, self.RECOMPRESS_PATHS[path]))
         k = np.zeros(self.n_blocks, dtype=np.int32)
         _lib.check(self._lib.pskel_recompress(self._h, float(thresh), k.ctypes.data_as(_lib.I32)))
         self._recomp_k = k
         return k
+
+    def recompress_split_blocks(self) -> int:
+        """Blocks of the last recompress() that took the split tensor-core path."""
+        n = ctypes.c_int(0)
+        _lib.check(self._lib.pskel_recompress_split_blocks(self._h, ctypes.byref(n)))
+        return int(n.value)
 
     def recompress_ms(self) -> float:
         """Device time of the last recompress() (ms, between the library's events on its

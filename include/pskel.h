@@ -410,12 +410,29 @@ int pskel_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int n
                  int precision, void *stream);
 
 /* Recompression of every block's C U R into an SVD-truncated C' diag(S) R' (k terms kept,
-   S > thresh * S_max), in FP64: the restatement of codes/ACA_vs_CUR/seed/svd_compress.m:19-33
-   (Householder QR of C and R^H in place of its unshipped qr_cbd, the QR-preconditioned Jacobi
-   SVD of the r x r core R_c U R_r^H, the reflectors applied to the kept vectors). ranks (host,
-   n_blocks, may be NULL) receives k per block. The factors stay on the device until the next
-   compression. */
+   S > thresh * S_max, 0 <= thresh < 1): codes/ACA_vs_CUR/seed/svd_compress.m:19-33. Two paths:
+   - FP64: Householder QR of C and R^H (in place of the unshipped qr_cbd), the QR-preconditioned
+     Jacobi SVD of the r x r core R_c U R_r^H, the reflectors applied to the kept vectors;
+   - split (complex-FP32 compressions, cores of rank <= 64): with the core's SVD from the
+     compression, C U R = X S Yh^H where X = C V S^-1 and Yh = R^H W S^-1 are well conditioned;
+     X, Yh and the rebuild C' = X Zx, R'^H = Yh Zy are tensor-core products of TF32 hi + lo
+     operands with FP32 accumulation (~1e-6 relative), their Gram matrices, Cholesky factors,
+     the core M = Lx^H S Ly and its Jacobi SVD are FP64; trailing terms of total weight below
+     1e-2 thresh S_max are left out before the SVD. C' and R'^H are orthonormal to ~1e-6.
+   The path is chosen per block (pskel_set_recompress_path): by default the split path for
+   complex-FP32 compressions at thresh >= 1e-5, FP64 otherwise and for the blocks the split path
+   hands back (rank above 64, a Cholesky breakdown, an unconverged SVD). ranks (host, n_blocks,
+   may be NULL) receives k per block. The factors stay on the device until the next
+   compression; the device time is reported as the "recompress" phase of pskel_last_timing. */
 int pskel_recompress(pskel_ctx *ctx, double thresh, int *ranks);
+
+/* Recompression path: 0 automatic (as above), 1 FP64 for every block, 2 the split path for
+   every complex-FP32 block of rank <= 64 at any threshold. */
+int pskel_set_recompress_path(pskel_ctx *ctx, int path);
+
+/* Blocks of the last pskel_recompress that took the split path (the others, mirrors aside,
+   took FP64). */
+int pskel_recompress_split_blocks(pskel_ctx *ctx, int *split_blocks);
 
 /* Copy block b's recompressed factors to host buffers: C' m x k, S (k, descending),
    R' k x n (complex128, column-major). Any pointer may be NULL. */

@@ -136,18 +136,33 @@ def test_matvec_rejects_bad_calls(sphere):
         assert lib.pskel_matvec(eng._h, None, m.N, None, m.N, 1, 0, None) == -1
 
 
-@pytest.mark.parametrize("prec,tol", [("c128", 1e-7), ("c64", 1e-4)])
-def test_recompress_matches_oracle(sphere, prec, tol):
+# split path (tensor-core products of TF32 hi + lo operands, FP32 accumulation): its singular
+# values and factors carry errors of ~1e-6 of the largest singular value, and its trailing-term
+# cut moves a singular value by at most 1e-2 thresh s_0; the bars allow 2e-5 s_0 and an
+# orthonormality defect of 1e-5
+SPLIT_S_BAR = 2e-5
+SPLIT_ORTH_BAR = 1e-5
+
+
+@pytest.mark.parametrize("prec,tol,path", [("c128", 1e-7, "auto"), ("c64", 1e-4, "fp64"),
+                                           ("c64", 1e-4, "split"), ("c64", 1e-3, "split")])
+def test_recompress_matches_oracle(sphere, prec, tol, path):
     """Device recompression against the oracle's QR-based one on the same factors. C U R is
     formed from an ill-conditioned core inverse, so both results carry rounding errors of
-    order eps ||C|| ||U|| ||R||: the comparisons are scaled by that product."""
+    order eps ||C|| ||U|| ||R||: the comparisons are scaled by that product. The split path
+    adds its FP32-level product errors (relative to the largest singular value)."""
     m, part = sphere
     thresh = tol / 10
     with Engine() as eng:
         eng.upload_mesh(m, K, ETA, q=7)
         eng.set_blocks(part)
         st = eng.compress(tol, precision=prec, tau=1e-8 if prec == "c128" else 1e-7, seed=5)
-        ks = eng.recompress(thresh)
+        ks = eng.recompress(thresh, path=path)
+        split = eng.recompress_split_blocks()
+        if path == "split":
+            assert split == eng.n_blocks  # every block has a core of rank <= 64 here
+        else:
+            assert split == 0
         assert np.all(ks >= 1) and np.all(ks <= st["r"])
         nb = eng.n_blocks
         for b in sorted(set([0, 1, nb // 3, nb // 2, nb - 1])):
@@ -159,6 +174,8 @@ def test_recompress_matches_oracle(sphere, prec, tol):
             scale = np.linalg.norm(C, 2) * np.linalg.norm(U, 2) * np.linalg.norm(R, 2)
             bar = 1e-12 * scale
             s_all = np.linalg.svd(A, compute_uv=False)
+            if path == "split":
+                bar += SPLIT_S_BAR * s_all[0]
             # the kept count agrees with the oracle unless a value lies within rounding of the
             # threshold
             if len(so) != len(S):
@@ -172,5 +189,35 @@ def test_recompress_matches_oracle(sphere, prec, tol):
             assert np.linalg.norm(B - Bo) < 2 * thresh * nA + 10 * bar * np.sqrt(kk)
             assert np.linalg.norm(B - A) < 2 * thresh * nA + 10 * bar * np.sqrt(kk)
             # orthonormal factors
-            assert np.abs(Cp.conj().T @ Cp - np.eye(len(S))).max() < 1e-9
-            assert np.abs(Rp @ Rp.conj().T - np.eye(len(S))).max() < 1e-9
+            orth = SPLIT_ORTH_BAR if path == "split" else 1e-9
+            assert np.abs(Cp.conj().T @ Cp - np.eye(len(S))).max() < orth
+            assert np.abs(Rp @ Rp.conj().T - np.eye(len(S))).max() < orth
+
+
+def test_recompress_split_matches_fp64(sphere):
+    """The split tensor-core path and the FP64 path on the same complex-FP32 compression:
+    equal ranks (up to values within the split path's error of the threshold) and products
+    C' S R' that agree to the split path's error, block by block; the default path at
+    thresh 1e-5 is the split one, at 1e-6 the FP64 one."""
+    m, part = sphere
+    thresh = 1e-5
+    with Engine() as eng:
+        eng.upload_mesh(m, K, ETA, q=7)
+        eng.set_blocks(part)
+        st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=3)
+        k64 = eng.recompress(thresh, path="fp64")
+        f64 = [eng.get_recompressed(b) for b in range(eng.n_blocks)]
+        ks = eng.recompress(thresh, path="auto")
+        assert eng.recompress_split_blocks() == eng.n_blocks
+        assert np.abs(ks - k64).max() <= 1 and np.mean(ks == k64) > 0.95
+        worst = 0.0
+        for b in range(eng.n_blocks):
+            Cp, S, Rp = eng.get_recompressed(b)
+            Cq, Sq, Rq = f64[b]
+            P, Q = (Cp * S) @ Rp, (Cq * Sq) @ Rq
+            worst = max(worst, np.linalg.norm(P - Q, 2) / Sq[0])
+        assert worst < 5 * thresh, worst
+        eng.recompress(1e-6, path="auto")
+        assert eng.recompress_split_blocks() == 0
+        eng.recompress(1e-6, path="split")
+        assert eng.recompress_split_blocks() == eng.n_blocks
