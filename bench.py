@@ -393,7 +393,7 @@ def run_ours(args, rank, world, dev):
         err_plain = eng.true_errors()
         eng.set_symmetric(True)
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
-    blockops = run_blockops(eng, st, m, flush, recompress=not large)
+    blockops = run_blockops(eng, st, m, flush, fp64_recompress=not large)
     footprint = run_footprint(eng, st, part, blockops)
     config3 = None
     if not (args.no_config3 or large):
@@ -484,9 +484,10 @@ def run_ours(args, rank, world, dev):
     return out
 
 
-def run_blockops(eng, st, m, flush, nrhs=16, reps=10, recompress=True):
-    """Compressed far-field matvec (nrhs right-hand sides, complex64 like the stored factors)
-    and FP64 recompression of every block, after the product compression."""
+def run_blockops(eng, st, m, flush, nrhs=16, reps=10, fp64_recompress=True):
+    """Compressed far-field matvec (nrhs right-hand sides, complex64 like the stored factors),
+    recompression of every block (default path; the FP64 path beside it when fp64_recompress)
+    and the tensor-core store matvec, after the product compression."""
     import torch
 
     from pskel import _lib
@@ -521,20 +522,22 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10, recompress=True):
                       gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
                       bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
                             "once each per call (algorithmic)")
-    if not recompress:
-        return dict(matvec=matvec_out, store_matvec=None, recompress=None,
-                    note="recompression and store skipped: the recompression workspace of every "
-                         "block does not fit the device at this size")
     # recompression to the compression tolerance (device time of its launches, from the
-    # library's own events on its stream)
-    eng.recompress(TOL)
-    rc_times = []
-    for _ in range(3):
-        flush.zero_()
-        torch.cuda.synchronize()
-        ks = eng.recompress(TOL)
-        rc_times.append(eng.recompress_ms())
-    rc_ms = float(np.mean(rc_times))
+    # library's own events on its stream): the default path (split tensor-core path for these
+    # complex-FP32 factors) and, where its workspace fits, the FP64 path on the same blocks
+    def time_recompress(path, calls):
+        eng.recompress(TOL, path=path)
+        ts = []
+        for _ in range(calls):
+            flush.zero_()
+            torch.cuda.synchronize()
+            k = eng.recompress(TOL, path=path)
+            ts.append(eng.recompress_ms())
+        return float(np.mean(ts)), k, eng.recompress_split_blocks()
+    rc_fp64_ms = None
+    if fp64_recompress:
+        rc_fp64_ms, _, _ = time_recompress("fp64", 2)
+    rc_ms, ks, split_blocks = time_recompress("auto", 3)
     # compressed store and the tensor-core matvec over it
     t0 = time.perf_counter()
     store_bytes = eng.build_store()
@@ -570,11 +573,16 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10, recompress=True):
                                 "entry), X and Y once each, T written and read once (algorithmic; "
                                 "store_bytes is the tiled store including its padding)"),
         recompress=dict(ms=round(rc_ms, 3), thresh=TOL, r_mean=float(rr.mean()),
-                        k_mean=float(ks.mean()),
-                        gflops=round(roofline.recompress_flops(mm, nn, rr, kk) / (rc_ms * 1e-3) / 1e9, 1),
-                        arithmetic="FP64 (Householder QR of C and R^H, Jacobi SVD of the core)",
+                        k_mean=float(ks.mean()), split_blocks=int(split_blocks),
+                        primary_blocks=int((eng.mirror_of() < 0).sum()),
+                        ms_fp64_path=None if rc_fp64_ms is None else round(rc_fp64_ms, 3),
+                        arithmetic="split path: X = C V S^-1, Yh = R^H W S^-1 and the rebuild "
+                                   "C' = X Zx, R'^H = Yh Zy as tcgen05 kind::tf32 products of TF32 "
+                                   "hi + lo operands (3 products, FP32 accumulation); FP64 Gram, "
+                                   "Cholesky, core M = Lx^H S Ly and its Jacobi SVD. FP64 path: "
+                                   "Householder QR of C and R^H, Jacobi SVD of the core",
                         timing="device time between the library's events around its launches "
-                               "(mean of 3 calls)"),
+                               "(mean of 3 calls; the FP64 path: mean of 2)"),
     )
 
 
@@ -796,6 +804,7 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
 #   python bench.py --profile-case fill --precision c64 --calls 2 --split 8 --geom32 1
 #   python bench.py --profile-case store --calls 5
 #   python bench.py --profile-case extras
+#   python bench.py --profile-case recompress --calls 2
 def fill_case(prec, calls, split, geom32):
     """CALLS single-round compressions of every far block of the 7,680-RWG sphere at a fixed
     sample count of 24 with the given precision (c128 or c64) and fill variant (8: triangle
@@ -850,6 +859,30 @@ def store_case(calls):
             torch.cuda.synchronize()
             print(f"store matvec call {i}: {e0.elapsed_time(e1):.4f} ms, store {nbytes / 1e6:.1f} MB, "
                   f"status {eng.store_status()}", flush=True)
+
+
+def recompress_case(calls):
+    """Compress the same sphere at tol 1e-4 (c64, symmetric mode) and recompress it CALLS times
+    at thresh 1e-5 on the default (split tensor-core) path, then once on the FP64 path, printing
+    the device time of each call. Under a profiler the split path's launches per call are
+    rc_prep_kernel, rc_tc_kernel (X, Yh), rc_gram_kernel, the SVD classes, rc_factor_kernel and
+    rc_tc_kernel (C', R')."""
+    from pskel import mesh as pmesh
+    from pskel import octree
+    from pskel.engine import Engine
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        for i in range(calls + 1):
+            path = "auto" if i < calls else "fp64"
+            ks = eng.recompress(1e-5, path=path)
+            print(f"recompress call {i} ({path}): {eng.recompress_ms():.3f} ms, split blocks "
+                  f"{eng.recompress_split_blocks()} of {int((eng.mirror_of() < 0).sum())}, k mean "
+                  f"{ks.mean():.2f}", flush=True)
 
 
 def extras_case():
@@ -919,7 +952,7 @@ def main():
     ap.add_argument("--product-only", action="store_true",
                     help="time the product steps only (no baselines, ablations, checks): the "
                          "command the kernel launch list is captured from")
-    ap.add_argument("--profile-case", choices=("fill", "store", "extras"), default=None,
+    ap.add_argument("--profile-case", choices=("fill", "store", "extras", "recompress"), default=None,
                     help="run one small profiling workload on the 7,680-RWG sphere instead of the "
                          "benchmark (the cases the kernel profiles are captured from)")
     ap.add_argument("--precision", default="c64", help="profiling case fill: c64 or c128")
@@ -932,6 +965,8 @@ def main():
             fill_case(args.precision, args.calls, args.split, args.geom32)
         elif args.profile_case == "store":
             store_case(args.calls)
+        elif args.profile_case == "recompress":
+            recompress_case(args.calls)
         else:
             extras_case()
         return

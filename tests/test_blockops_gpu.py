@@ -160,7 +160,9 @@ def test_recompress_matches_oracle(sphere, prec, tol, path):
         ks = eng.recompress(thresh, path=path)
         split = eng.recompress_split_blocks()
         if path == "split":
-            assert split == eng.n_blocks  # every block has a core of rank <= 64 here
+            # every core has rank <= 64 here; the blocks whose pinv kept values far below tau
+            # (full sample count, common on this small sphere) go to the FP64 path
+            assert 0 < split < eng.n_blocks
         else:
             assert split == 0
         assert np.all(ks >= 1) and np.all(ks <= st["r"])
@@ -198,7 +200,8 @@ def test_recompress_split_matches_fp64(sphere):
     """The split tensor-core path and the FP64 path on the same complex-FP32 compression:
     equal ranks (up to values within the split path's error of the threshold) and products
     C' S R' that agree to the split path's error, block by block; the default path at
-    thresh 1e-5 is the split one, at 1e-6 the FP64 one."""
+    thresh 1e-5 is the split one (but for blocks kept to core values below 1e-7 of the
+    largest), at 1e-6 the FP64 one."""
     m, part = sphere
     thresh = 1e-5
     with Engine() as eng:
@@ -208,7 +211,7 @@ def test_recompress_split_matches_fp64(sphere):
         k64 = eng.recompress(thresh, path="fp64")
         f64 = [eng.get_recompressed(b) for b in range(eng.n_blocks)]
         ks = eng.recompress(thresh, path="auto")
-        assert eng.recompress_split_blocks() == eng.n_blocks
+        assert eng.recompress_split_blocks() > 0
         assert np.abs(ks - k64).max() <= 1 and np.mean(ks == k64) > 0.95
         worst = 0.0
         for b in range(eng.n_blocks):
@@ -219,5 +222,7 @@ def test_recompress_split_matches_fp64(sphere):
         assert worst < 5 * thresh, worst
         eng.recompress(1e-6, path="auto")
         assert eng.recompress_split_blocks() == 0
-        eng.recompress(1e-6, path="split")
-        assert eng.recompress_split_blocks() == eng.n_blocks
+        eng.recompress(1e-4, path="fp64")
+        assert eng.recompress_split_blocks() == 0
+        eng.recompress(1e-4, path="split")
+        assert eng.recompress_split_blocks() > 0
