@@ -574,7 +574,7 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10, fp64_recompress=True):
                                 "store_bytes is the tiled store including its padding)"),
         recompress=dict(ms=round(rc_ms, 3), thresh=TOL, r_mean=float(rr.mean()),
                         k_mean=float(ks.mean()), split_blocks=int(split_blocks),
-                        primary_blocks=int((eng.mirror_of() < 0).sum()),
+                        primary_blocks=primary_blocks(eng),
                         ms_fp64_path=None if rc_fp64_ms is None else round(rc_fp64_ms, 3),
                         arithmetic="split path: X = C V S^-1, Yh = R^H W S^-1 and the rebuild "
                                    "C' = X Zx, R'^H = Yh Zy as tcgen05 kind::tf32 products of TF32 "
@@ -615,6 +615,15 @@ def run_footprint(eng, st, part, blockops):
 
 def eng_symmetric(eng) -> bool:
     return bool(getattr(eng, "_symmetric", False))
+
+
+def primary_blocks(eng) -> int:
+    """Blocks that keep their own factors: all of them, or in the symmetric mode one block of
+    each (t, s) / (s, t) pair (the one with the smaller index) and the blocks without a pair."""
+    if not eng_symmetric(eng):
+        return int(eng.n_blocks)
+    mir = eng.mirror_of()
+    return int(np.sum((mir < 0) | (np.arange(len(mir)) < mir)))
 
 
 def run_config3(eng, m, r0_for, nrhs=16, reps=5):
@@ -881,7 +890,7 @@ def recompress_case(calls):
             path = "auto" if i < calls else "fp64"
             ks = eng.recompress(1e-5, path=path)
             print(f"recompress call {i} ({path}): {eng.recompress_ms():.3f} ms, split blocks "
-                  f"{eng.recompress_split_blocks()} of {int((eng.mirror_of() < 0).sum())}, k mean "
+                  f"{eng.recompress_split_blocks()} of {primary_blocks(eng)}, k mean "
                   f"{ks.mean():.2f}", flush=True)
 
 

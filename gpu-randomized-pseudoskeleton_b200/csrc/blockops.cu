@@ -433,9 +433,14 @@ __global__ void recomp_rp_kernel(const RecompBlock *__restrict__ jobs) {
 
 namespace pskel {
 
-// FP64 recompression of the primary blocks `prims` into c->recomp64 (factors and workspace);
-// fills their slots.
-int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh) {
+// FP64 recompression of the primary blocks `prims` into `buf` (factors and workspace), enqueued
+// on stream st (job tables in c->tmp; scratch c->tmp2, c->tmp3); fills their slots but k, which
+// recompress_fp64_finish reads back.
+int recompress_fp64_enqueue(pskel_ctx *c, const std::vector<int> &prims, double thresh, cudaStream_t st,
+                            DevBuf &buf, Fp64Recomp &out) {
+    out = Fp64Recomp();
+    out.prims = prims;
+    out.st = st;
     const int nb = (int)prims.size();
     if (nb == 0) return PSKEL_OK;
     const bool f32 = c->precision == PSKEL_C64;
@@ -447,8 +452,8 @@ int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh) 
         off[pi + 1] = off[pi] + 2 * al(16 * m * r) + 3 * al(16 * n * r) + 8 * al(16 * r * r) +
                      2 * al(16 * r) + 4 * al(8 * r) + al(4 * r) + 256;
     }
-    PSKEL_TRY(c->recomp64.reserve(off[nb] + 256));
-    char *base = c->recomp64.as<char>();
+    PSKEL_TRY(buf.reserve(off[nb] + 256));
+    char *base = buf.as<char>();
     std::vector<RecompBlock> jobs(nb);
     std::vector<QrJob> qrs;
     qrs.reserve(2 * nb);
@@ -516,32 +521,40 @@ int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh) 
         sl.ldrp = res.r;
         sl.mirror = -1;
     }
-    PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, c->stream));
-    PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, c->stream));
-    if (f32) recomp_load_kernel<float2><<<nb, 256, 0, c->stream>>>(d_jobs);
-    else recomp_load_kernel<double2><<<nb, 256, 0, c->stream>>>(d_jobs);
+    PSKEL_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), jb, cudaMemcpyHostToDevice, st));
+    PSKEL_CUDA(cudaMemcpyAsync(d_s2, svds.data(), s2, cudaMemcpyHostToDevice, st));
+    if (f32) recomp_load_kernel<float2><<<nb, 256, 0, st>>>(d_jobs);
+    else recomp_load_kernel<double2><<<nb, 256, 0, st>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(batched_qr(qrs, c->stream, c->tmp2));
-    PSKEL_TRY(launch_zgemm(g1, c->stream, c->tmp3));
-    PSKEL_TRY(launch_zgemm(g2, c->stream, c->tmp3));
-    PSKEL_TRY(batched_svd(d_s2, svds, 60, c->stream, c->tmp2));
-    recomp_factors_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
+    PSKEL_TRY(batched_qr(qrs, st, c->tmp2));
+    PSKEL_TRY(launch_zgemm(g1, st, c->tmp3));
+    PSKEL_TRY(launch_zgemm(g2, st, c->tmp3));
+    PSKEL_TRY(batched_svd(d_s2, svds, 60, st, c->tmp2));
+    recomp_factors_kernel<<<nb, 256, 0, st>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    PSKEL_TRY(batched_apply_q(aps, c->stream, c->tmp3));
-    recomp_rp_kernel<<<nb, 256, 0, c->stream>>>(d_jobs);
+    PSKEL_TRY(batched_apply_q(aps, st, c->tmp3));
+    recomp_rp_kernel<<<nb, 256, 0, st>>>(d_jobs);
     PSKEL_LAUNCHED(1);
-    // ranks and SVD statuses back to the host
+    out.d_s2 = d_s2;
+    out.d_k = d_k;
+    return PSKEL_OK;
+}
+
+// Ranks and SVD statuses of an enqueued FP64 recompression back to the host (waits for it).
+int recompress_fp64_finish(pskel_ctx *c, Fp64Recomp &r) {
+    const int nb = (int)r.prims.size();
+    if (nb == 0) return PSKEL_OK;
     std::vector<SvdJob> h2(nb);
     std::vector<int> ks(nb);
-    PSKEL_CUDA(cudaMemcpyAsync(h2.data(), d_s2, s2, cudaMemcpyDeviceToHost, c->stream));
-    PSKEL_CUDA(cudaMemcpyAsync(ks.data(), d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, c->stream));
-    PSKEL_CUDA(cudaStreamSynchronize(c->stream));
+    PSKEL_CUDA(cudaMemcpyAsync(h2.data(), r.d_s2, sizeof(SvdJob) * nb, cudaMemcpyDeviceToHost, r.st));
+    PSKEL_CUDA(cudaMemcpyAsync(ks.data(), r.d_k, sizeof(int) * nb, cudaMemcpyDeviceToHost, r.st));
+    PSKEL_CUDA(cudaStreamSynchronize(r.st));
     for (const SvdJob &j : h2)
         if (j.status != PSKEL_OK) {
             set_error(PSKEL_ERR_NOCONV, "recompress: Jacobi SVD of a core did not converge");
             return PSKEL_ERR_NOCONV;
         }
-    for (int pi = 0; pi < nb; ++pi) c->recomp_slots[prims[pi]].k = ks[pi];
+    for (int pi = 0; pi < nb; ++pi) c->recomp_slots[r.prims[pi]].k = ks[pi];
     return PSKEL_OK;
 }
 
@@ -590,11 +603,24 @@ extern "C" int pskel_recompress(pskel_ctx *c, double thresh, int *ranks) {
         if (recomp_split_eligible(c, b, thresh)) split.push_back(b);
         else fp64.push_back(b);
     PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    // blocks whose pinv kept core values below the split products' accuracy join the FP64 set
+    PSKEL_TRY(recomp_split_precheck(c, thresh, split, fp64));
+    // the FP64 set (usually a few large or full-sample cores, latency-bound) runs on the second
+    // stream beside the split path
+    Fp64Recomp side, rest;
+    cudaStream_t s2 = c->pipe_stream ? c->pipe_stream : c->stream;
+    if (!fp64.empty() && s2 != c->stream) {
+        PSKEL_CUDA(cudaEventRecord(c->pipe_ev[0], c->stream));
+        PSKEL_CUDA(cudaStreamWaitEvent(s2, c->pipe_ev[0], 0));
+    }
+    PSKEL_TRY(recompress_fp64_enqueue(c, fp64, thresh, s2, c->recomp64, side));
     std::vector<int> rejected;
     PSKEL_TRY(recompress_split(c, split, thresh, rejected));
     c->recomp_split_blocks = (int)(split.size() - rejected.size());
-    fp64.insert(fp64.end(), rejected.begin(), rejected.end());
-    PSKEL_TRY(recompress_fp64(c, fp64, thresh));
+    PSKEL_TRY(recompress_fp64_finish(c, side));
+    // blocks the split path handed back (a Cholesky breakdown, an unconverged SVD)
+    PSKEL_TRY(recompress_fp64_enqueue(c, rejected, thresh, c->stream, c->recomp64b, rest));
+    PSKEL_TRY(recompress_fp64_finish(c, rest));
     PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
     PSKEL_CUDA(cudaEventSynchronize(c->ev[4]));
     {

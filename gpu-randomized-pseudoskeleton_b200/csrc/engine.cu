@@ -999,7 +999,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec1.f64.release();
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
-    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->rc_work.release(); c->rc_tab.release(); c->mv_table.release();
+    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->recomp64b.release(); c->rc_work.release(); c->rc_tab.release(); c->rc_idx.release(); c->mv_table.release();
     for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     svd_streams_destroy(c->svd_par);
@@ -1417,7 +1417,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             rounds_used[b] = round + 1;
             const bool ok = hout[i].status == PSKEL_OK && est[i] <= o.tol / safety;
             if (ok || r_cur[b] >= Dmin[b] || round + 1 >= o.max_rounds) continue;
-            r_cur[b] = std::min(2 * r_cur[b], Dmin[b]);
+            r_cur[b] = std::min(std::max(r_cur[b] + 1, (int)std::ceil(c->growth * r_cur[b])), Dmin[b]);
             next.push_back(b);
         }
         active.swap(next);
@@ -1504,6 +1504,15 @@ extern "C" int pskel_set_tri_cols(pskel_ctx *c, int cols) {
         return PSKEL_ERR_ARG;
     }
     c->tri_cols = cols;
+    return PSKEL_OK;
+}
+
+extern "C" int pskel_set_round_growth(pskel_ctx *c, double factor) {
+    if (!c || !(factor > 1.0 && factor <= 4.0)) {
+        set_error(PSKEL_ERR_ARG, "set_round_growth: factor must be in (1, 4]");
+        return PSKEL_ERR_ARG;
+    }
+    c->growth = factor;
     return PSKEL_OK;
 }
 

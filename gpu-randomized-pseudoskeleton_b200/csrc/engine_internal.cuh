@@ -115,6 +115,7 @@ struct pskel_ctx {
     cudaStream_t pipe_stream = nullptr;
     cudaEvent_t pipe_ev[kMaxChunks + 1] = {};
     int pipe_chunks = 2;        // chunks of a round with at least kPipeMinBlocks blocks (1: off)
+    double growth = 2.0;        // sample count factor from one round to the next (2: doubling)
     DevMesh mesh;
     pskel_em_t em{};
     bool have_mesh = false;
@@ -148,8 +149,8 @@ struct pskel_ctx {
     std::vector<int> last_key;  // round-0 key of the previous call (capture on a repeat)
     DevBuf tmp, tmp2, tmp3;
     DevBuf recomp;                          // recompressed factors (split path, loaded store)
-    DevBuf recomp64;                        // FP64 path: recompressed factors and workspace
-    DevBuf rc_work, rc_tab;                 // split path: workspace and job tables
+    DevBuf recomp64, recomp64b;             // FP64 path: recompressed factors and workspace
+    DevBuf rc_work, rc_tab, rc_idx;         // split path: workspace, job tables, SVD order
     int recomp_path = 0;                    // 0 auto, 1 FP64 only, 2 split whenever eligible
     int recomp_split_blocks = 0;            // blocks of the last recompression on the split path
     std::vector<RecompSlot> recomp_slots;   // per block: C', R', S and the rank k
@@ -175,7 +176,18 @@ struct pskel_ctx {
 namespace pskel {
 // Recompression (csrc/blockops.cu, csrc/recomp_tc.cu) of primary blocks: the FP64 path, and the
 // split-precision tensor-core path with the blocks it hands back to the FP64 one.
-int recompress_fp64(pskel_ctx *c, const std::vector<int> &prims, double thresh);
+struct Fp64Recomp {  // one enqueued FP64 recompression
+    std::vector<int> prims;
+    SvdJob *d_s2 = nullptr;
+    int *d_k = nullptr;
+    cudaStream_t st = nullptr;
+};
+int recompress_fp64_enqueue(pskel_ctx *c, const std::vector<int> &prims, double thresh, cudaStream_t st,
+                            DevBuf &buf, Fp64Recomp &out);
+int recompress_fp64_finish(pskel_ctx *c, Fp64Recomp &r);
 bool recomp_split_eligible(const pskel_ctx *c, int b, double thresh);
+// moves the split-eligible blocks whose pinv kept core values below the split products'
+// accuracy (see recomp_tc.cu) from `split` to `fp64` (one device check and read-back)
+int recomp_split_precheck(pskel_ctx *c, double thresh, std::vector<int> &split, std::vector<int> &fp64);
 int recompress_split(pskel_ctx *c, const std::vector<int> &blocks, double thresh, std::vector<int> &rejected);
 }  // namespace pskel

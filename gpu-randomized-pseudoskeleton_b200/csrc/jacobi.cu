@@ -234,22 +234,34 @@ __global__ void __launch_bounds__(kSvdThreads)
         if (j < n && qg == 0) snrm[j] = s2;
     }
     __syncthreads();
+    // truncated form (job.trunc > 0): the QR stops at the first k whose trailing block
+    // R(k:, k:) has Frobenius norm <= trunc (the sum of the remaining column norms), and the
+    // rest works on the leading kp rows of R
+    const double trunc2 = job.trunc > 0 ? job.trunc * job.trunc : -1.0;
+    int kp = n;
     for (int k = 0; k < n; ++k) {
         if (warp == 0) {
             // pivot: the remaining column of largest norm
-            double best = -1.0;
+            double best = -1.0, rest = 0.0;
             int bi = k;
-            for (int j = k + lane; j < n; j += 32)
+            for (int j = k + lane; j < n; j += 32) {
+                rest += snrm[j];
                 if (snrm[j] > best) { best = snrm[j]; bi = j; }
+            }
             for (int o = 16; o > 0; o >>= 1) {
                 const double ob = __shfl_xor_sync(0xffffffffu, best, o);
                 const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                rest += __shfl_xor_sync(0xffffffffu, rest, o);
                 if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
             }
-            if (lane == 0) s_p = bi;
+            if (lane == 0) s_p = (k > 0 && rest <= trunc2) ? -1 : bi;
         }
         __syncthreads();
         const int p = s_p;
+        if (p < 0) {  // uniform: every thread read the same s_p
+            kp = k;
+            break;
+        }
         if (p != k) {
             for (int i = tid; i < m; i += blockDim.x) {
                 const double2 t = sA[i + (size_t)k * m];
@@ -325,7 +337,7 @@ __global__ void __launch_bounds__(kSvdThreads)
         __syncthreads();
     }
     // ---- 2. one-sided Jacobi on X = R^H, rotations accumulated in W
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
+    for (int idx = tid; idx < n * kp; idx += blockDim.x) {
         const int i = idx % n, j = idx / n;
         const double2 r = sA[j + (size_t)i * m];  // R(j, i)
         sX[idx] = j <= i ? make_double2(r.x, -r.y) : make_double2(0.0, 0.0);
@@ -336,19 +348,19 @@ __global__ void __launch_bounds__(kSvdThreads)
         refl = job.V;
         __syncthreads();
     }
-    for (int idx = tid; idx < n * n; idx += blockDim.x) {
-        const int i = idx % n, j = idx / n;
+    for (int idx = tid; idx < kp * kp; idx += blockDim.x) {
+        const int i = idx % kp, j = idx / kp;
         sW[idx] = make_double2(i == j ? 1.0 : 0.0, 0.0);
     }
     __syncthreads();
-    const int team = jacobi_team(n, n, blockDim.x);
+    const int team = jacobi_team(n, kp, blockDim.x);
     const double tol = (double)(n > 1 ? n : 1) * DBL_EPSILON;
-    const double zero2 = zero_column_norm2(sX, (size_t)n * n, n);
+    const double zero2 = zero_column_norm2(sX, (size_t)n * kp, n);
     int sweep = 0, converged = 0;
     for (; sweep < max_sweeps; ++sweep) {
         if (tid == 0) s_rot = 0;
         __syncthreads();
-        inner_sweep(sX, n, sW, n, n, team, tol, zero2, &s_rot);
+        inner_sweep(sX, n, sW, kp, kp, team, tol, zero2, &s_rot);
         __syncthreads();
         const int rot = s_rot;
         __syncthreads();
@@ -357,30 +369,31 @@ __global__ void __launch_bounds__(kSvdThreads)
             break;
         }
     }
-    // ---- 3. sigma, V = P B / sigma, A V = Q W sigma
+    // ---- 3. sigma, V = P B / sigma, A V = Q W sigma (columns kp.. of the truncated form: 0)
     for (int j = tid; j < n; j += blockDim.x) {
         double s2 = 0;
-        for (int i = 0; i < n; ++i) {
-            const double2 b = sX[i + (size_t)j * n];
-            s2 = fma(b.x, b.x, fma(b.y, b.y, s2));
-        }
+        if (j < kp)
+            for (int i = 0; i < n; ++i) {
+                const double2 b = sX[i + (size_t)j * n];
+                s2 = fma(b.x, b.x, fma(b.y, b.y, s2));
+            }
         snrm[j] = sqrt(s2);
     }
     __syncthreads();
-    // A V column j by one team: y = [W(:, j) sigma_j; 0], then y <- H_k y for k = n-1 .. 0;
+    // A V column j by one team: y = [W(:, j) sigma_j; 0], then y <- H_k y for k = kp-1 .. 0;
     // the team's lanes hold rows qg, qg + qteam, ... (at most kQrRowsPerLane each)
     for (int j0 = 0; j0 < n; j0 += qteams) {
         const int j = j0 + qt;
         const bool on = j < n;
-        const double sg = on ? snrm[j] : 0.0;
+        const double sg = (on && j < kp) ? snrm[j] : 0.0;
         double2 y[kQrRowsPerLane];
 #pragma unroll
         for (int e = 0; e < kQrRowsPerLane; ++e) {
             const int i = qg + e * qteam;
-            const double2 w = (on && i < n) ? sW[i + (size_t)j * n] : make_double2(0.0, 0.0);
+            const double2 w = (on && j < kp && i < kp) ? sW[i + (size_t)j * kp] : make_double2(0.0, 0.0);
             y[e] = make_double2(w.x * sg, w.y * sg);
         }
-        for (int k = n - 1; k >= 0; --k) {
+        for (int k = kp - 1; k >= 0; --k) {
             const double coef = scoef[k];
             const double2 v0 = sv0[k];
             double dr = 0, di = 0;
@@ -421,7 +434,7 @@ __global__ void __launch_bounds__(kSvdThreads)
         const int i = idx % n, j = idx / n;
         const double sg = snrm[j];
         const double f = sg > 0 ? 1.0 / sg : 0.0;
-        const double2 b = sX[idx];
+        const double2 b = j < kp ? sX[idx] : make_double2(0.0, 0.0);
         job.V[spiv[i] + (size_t)j * n] = make_double2(b.x * f, b.y * f);
     }
     for (int j = tid; j < n; j += blockDim.x) job.sigma[j] = snrm[j];

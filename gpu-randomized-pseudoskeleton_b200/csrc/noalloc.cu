@@ -76,6 +76,7 @@ __global__ void noalloc_setup_kernel(unsigned char *base, const double2 *A, int 
         sj->n = n;
         sj->status = PSKEL_ERR_NOCONV;  // overwritten by the SVD kernel
         sj->sweeps = 0;
+        sj->trunc = 0.0;
         *reinterpret_cast<int *>(base + NoAllocLayout::idx) = 0;
         *reinterpret_cast<int *>(base + NoAllocLayout::rank) = 0;
         PinvJob *pj = reinterpret_cast<PinvJob *>(base + NoAllocLayout::pinv);

@@ -204,6 +204,11 @@ struct SvdJob {
     int m, n;
     int status;      // written by the kernel: 0 converged, PSKEL_ERR_NOCONV otherwise
     int sweeps;
+    // > 0 (resident kernel only): truncated SVD. The pivoted QR stops at the first k whose
+    // trailing block has Frobenius norm <= trunc; the k singular triplets of the leading rows
+    // are returned and the other columns of A V, V and sigma are zero. Every singular value
+    // moves by at most trunc.
+    double trunc;
 };
 
 // Run the SVD of every job to convergence (max_sweeps cap). jobs is a DEVICE array; the host

@@ -84,6 +84,7 @@ SIGNATURES = {
     "pskel_set_fill_split": (ci, [VP, ci, ci]),
     "pskel_set_tri_cols": (ci, [VP, ci]),
     "pskel_set_pipeline": (ci, [VP, ci]),
+    "pskel_set_round_growth": (ci, [VP, cd]),
     "pskel_set_fill_geometry": (ci, [VP, ci]),
     "pskel_set_symmetric": (ci, [VP, ci]),
     "pskel_fill_near_device": (ci, [VP, VP, ci, VP, ci, VP, ci, cd, cd, cd, ci]),

@@ -371,6 +371,10 @@ class Engine:
         """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
+    def set_round_growth(self, factor: float):
+        """Sample count factor from one round to the next (default 2, the reference's doubling)."""
+        _lib.check(self._lib.pskel_set_round_growth(self._h, float(factor)))
+
     def set_pipeline(self, chunks: int):
         """Chunks of a pipelined compression round (1 = off; default 2): the fill of one chunk
         overlaps the SVD, pinv and estimate of the previous one."""

@@ -271,6 +271,11 @@ int pskel_last_timing(pskel_ctx *ctx, double *out, int n);
    pinv phase the last chunk's pinv and estimate. */
 int pskel_set_pipeline(pskel_ctx *ctx, int chunks);
 
+/* Sample count of a block's next round: max(r + 1, ceil(factor * r)), capped by the block's
+   smaller side (1 < factor <= 4; default 2, the reference's doubling,
+   compres_single_block_spheres_for_sweep2.jl:878-973). */
+int pskel_set_round_growth(pskel_ctx *ctx, double factor);
+
 /* Copy block b's factors to host buffers (complex128): C m x r, U r x r, R r x n, 0-based
    local samples I (r) and J (r). Any pointer may be NULL. */
 int pskel_get_block(pskel_ctx *ctx, int b, pskel_c128 *C, pskel_c128 *U, pskel_c128 *R,
