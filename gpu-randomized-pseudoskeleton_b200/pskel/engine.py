@@ -142,7 +142,8 @@ class Engine:
                  max_rounds: int = 12,
                  seed: int = 0,
                  use_graph: bool = False, recompress: bool = False,
-                 recompress_tol: float = 0.0, per_block: bool = False) -> np.ndarray:
+                 recompress_tol: float = 0.0, per_block: bool = False,
+                 round_growth: float = 2.0) -> np.ndarray:
         """Compress every block; returns a structured array of per-block stats
         (m, n, r, rank, rank_recompressed, rounds, status, est).
 
@@ -150,7 +151,10 @@ class Engine:
         passes with est above tol / (est_safety * est_verify) is re-checked on a second set of
         extra rows and columns and passes on the pooled estimate (est_verify <= 1: no
         re-check). A block sampled on its whole smaller side (r = min(m, n)) uses the pinv
-        threshold min(tau, full_tau) (relative; full_tau = 0: tau)."""
+        threshold min(tau, full_tau) (relative; full_tau = 0: tau). A block that fails is
+        compressed again with max(r + 1, ceil(round_growth * r)) samples (2: the reference's
+        doubling)."""
+        self.set_round_growth(round_growth)
         o = _lib.Opts(tol=tol, tau=tau, tau_relative=int(bool(tau_relative)),
                       precision=_prec(precision),
                       start=START_GIVEN if r0 is not None else START_REFERENCE,
