@@ -376,11 +376,14 @@ def run_ours(args, rank, world, dev):
             eng.set_symmetric(True)
             return eng.compress(TOL, r0=predict_r0(), use_graph=True, **dict(PRODUCT, precision="c128"))
         lsym128_ms, _, _, _ = timed(learned_sym_c128, 1, 2)
-    # per-phase timing of the product without the graph (roofline of the fill)
+    # per-phase timing of the product without the graph and without the pipelined round (the
+    # fill launches alone on the GPU: the roofline of the fill kernel)
     eng.set_symmetric(True)
     r0 = predict_r0()
+    eng.set_pipeline(1)
     st_np = eng.compress(TOL, r0=r0, use_graph=False, **PRODUCT)
     tph = eng.timing()
+    eng.set_pipeline(2)
     fp32_peak = ctypes.c_double()
     fp64_peak = ctypes.c_double()
     _lib.check(L.pskel_fma_peak(ctypes.byref(fp32_peak), ctypes.byref(fp64_peak)))
@@ -815,7 +818,7 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
 #   python bench.py --profile-case fill --precision c64 --calls 2 --split 8 --geom32 1
 #   python bench.py --profile-case store --calls 5
 #   python bench.py --profile-case extras
-#   python bench.py --profile-case recompress --calls 2
+#   python bench.py --profile-case recompress --calls 2 [--subdiv 5]
 def fill_case(prec, calls, split, geom32):
     """CALLS single-round compressions of every far block of the 7,680-RWG sphere at a fixed
     sample count of 24 with the given precision (c128 or c64) and fill variant (8: triangle
@@ -872,22 +875,29 @@ def store_case(calls):
                   f"status {eng.store_status()}", flush=True)
 
 
-def recompress_case(calls):
-    """Compress the same sphere at tol 1e-4 (c64, symmetric mode) and recompress it CALLS times
-    at thresh 1e-5 on the default (split tensor-core) path, then once on the FP64 path, printing
-    the device time of each call. Under a profiler the split path's launches per call are
-    rc_prep_kernel, rc_tc_kernel (X, Yh), rc_gram_kernel, the SVD classes, rc_factor_kernel and
-    rc_tc_kernel (C', R')."""
+def recompress_case(calls, subdiv=4):
+    """Compress the sphere (icosphere R = 2 lambda, SUBDIV subdivisions: 4 -> 7,680 RWG with
+    0.5-lambda leaves merged to >= 30, 5 -> 30,720 RWG merged to >= 40 with the learned first
+    sample counts, the bench workload) at tol 1e-4 (c64, symmetric mode) and recompress it CALLS
+    times at thresh 1e-5 on the default (split tensor-core) path, then once on the FP64 path,
+    printing the device time of each call. Under a profiler the split path's launches per call
+    are rc_check_kernel, the FP64 set beside it, rc_prep_kernel, rc_tc_kernel (X, Yh),
+    rc_gram_kernel, the SVD classes, rc_factor_kernel and rc_tc_kernel (C', R')."""
     from pskel import mesh as pmesh
     from pskel import octree
     from pskel.engine import Engine
-    m = pmesh.icosphere(2.0, 4)
-    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    from pskel.predictor import Predictor
+    m = pmesh.icosphere(2.0, subdiv)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30 if subdiv <= 4 else 40)
+    r0 = Predictor.load().sample_counts(part, 2 * np.pi, 1e-4) if subdiv >= 5 else None
     with Engine() as eng:
         eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
         eng.set_blocks(part)
         eng.set_symmetric(True)
-        eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        if r0 is None:
+            eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        else:
+            eng.compress(1e-4, precision="c64", tau=1e-7, r0=r0, oversample=0, seed=0)
         for i in range(calls + 1):
             path = "auto" if i < calls else "fp64"
             ks = eng.recompress(1e-5, path=path)
@@ -970,6 +980,8 @@ def main():
     ap.add_argument("--calls", type=int, default=3, help="profiling cases: calls of the kernel")
     ap.add_argument("--split", type=int, default=8, help="profiling case fill: fill variant")
     ap.add_argument("--geom32", type=int, default=0, help="profiling case fill: FP32 pair geometry")
+    ap.add_argument("--subdiv", type=int, default=4,
+                    help="profiling case recompress: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
     args = ap.parse_args()
     if args.profile_case:
         if args.profile_case == "fill":
@@ -977,7 +989,7 @@ def main():
         elif args.profile_case == "store":
             store_case(args.calls)
         elif args.profile_case == "recompress":
-            recompress_case(args.calls)
+            recompress_case(args.calls, args.subdiv)
         else:
             extras_case()
         return

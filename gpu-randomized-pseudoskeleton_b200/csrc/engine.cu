@@ -227,8 +227,12 @@ struct EstJob {
     double *out;      // est, then the four sums (rows num, den, cols num, den)
 };
 
-template <typename S>
+// SM: U and the scratch Tr, Sc live in shared memory (est_smem_bytes of the launch's largest
+// r, pe, pc); otherwise U is read from global memory and Tr, Sc use the job's scratch. The
+// arithmetic and its order are the same in both.
+template <typename S, bool SM>
 __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict__ jobs) {
+    extern __shared__ __align__(16) unsigned char est_smem[];
     __shared__ double s_red[4][256];
     const EstJob w = jobs[blockIdx.x];
     const int r = w.r, pe = w.pe, pc = w.pc, n = w.n, m = w.m, ldr = w.ldr, ldxr = w.ldxr;
@@ -236,8 +240,27 @@ __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict_
     const S *Rm = reinterpret_cast<const S *>(w.R);
     const S *Xr = reinterpret_cast<const S *>(w.Xr);
     const S *Xc = reinterpret_cast<const S *>(w.Xc);
+    const double2 *Uc = w.U;
     double2 *Tr = w.T;             // pe x r
     double2 *Sc = w.T + pe * r;    // r x pc
+    if (SM) {
+        double2 *sU = reinterpret_cast<double2 *>(est_smem);
+        for (int e0 = threadIdx.x; e0 < r * r; e0 += 8 * blockDim.x) {
+            double2 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {  // loads first, then the stores
+                const int e = e0 + u * blockDim.x;
+                if (e < r * r) v[u] = w.U[e];
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (e0 + u * blockDim.x < r * r) sU[e0 + u * blockDim.x] = v[u];
+        }
+        Uc = sU;
+        Tr = sU + r * r;
+        Sc = Tr + pe * r;
+        __syncthreads();
+    }
     // Tr = C(Ix, :) U ; Sc = U R(:, Jx)
     for (int idx = threadIdx.x; idx < pe * r + r * pc; idx += blockDim.x) {
         double sx = 0, sy = 0;
@@ -246,7 +269,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict_
             const int row = w.Ix[e];
             for (int l = 0; l < r; ++l) {
                 const double2 c = promote(C[row + (size_t)l * m]);
-                const double2 u = w.U[l + (size_t)k * r];
+                const double2 u = Uc[l + (size_t)k * r];
                 sx = fma(c.x, u.x, fma(-c.y, u.y, sx));
                 sy = fma(c.x, u.y, fma(c.y, u.x, sy));
             }
@@ -256,7 +279,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict_
             const int k = q % r, cc = q / r;
             const int col = w.Jx[cc];
             for (int l = 0; l < r; ++l) {
-                const double2 u = w.U[k + (size_t)l * r];
+                const double2 u = Uc[k + (size_t)l * r];
                 const double2 rv = promote(Rm[l + (size_t)col * ldr]);
                 sx = fma(u.x, rv.x, fma(-u.y, rv.y, sx));
                 sy = fma(u.x, rv.y, fma(u.y, rv.x, sy));
@@ -342,6 +365,34 @@ __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict_
         w.out[0] = fmax(er, ec);
         for (int q = 0; q < 4; ++q) w.out[1 + q] = s_red[q][0];
     }
+}
+
+// Shared memory of the estimate for cores up to r, pe extra rows, pc extra columns.
+inline size_t est_smem_bytes(int r, int pe, int pc) {
+    return sizeof(double2) * ((size_t)r * r + (size_t)(pe + pc) * r);
+}
+constexpr size_t kEstSmemMax = 96 * 1024;
+
+// One estimate launch of cnt jobs whose largest r, pe, pc are given.
+int launch_estimate(const EstJob *d_jobs, int cnt, int precision, int rmax, int pemax, int pcmax,
+                    cudaStream_t st) {
+    if (cnt <= 0) return PSKEL_OK;
+    const size_t sm = est_smem_bytes(rmax, pemax, pcmax);
+    if (sm <= kEstSmemMax) {
+        if (precision == PSKEL_C64) {
+            PSKEL_TRY(ensure_smem_attr(estimate_kernel<float2, true>, kEstSmemMax));
+            estimate_kernel<float2, true><<<cnt, 256, sm, st>>>(d_jobs);
+        } else {
+            PSKEL_TRY(ensure_smem_attr(estimate_kernel<double2, true>, kEstSmemMax));
+            estimate_kernel<double2, true><<<cnt, 256, sm, st>>>(d_jobs);
+        }
+    } else if (precision == PSKEL_C64) {
+        estimate_kernel<float2, false><<<cnt, 256, 0, st>>>(d_jobs);
+    } else {
+        estimate_kernel<double2, false><<<cnt, 256, 0, st>>>(d_jobs);
+    }
+    PSKEL_LAUNCHED(1);
+    return PSKEL_OK;
 }
 
 // per-block outcome gather: est, rank, svd status into one compact array for a single D2H
@@ -749,12 +800,13 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
         PSKEL_TRY(svd_launch(p.d_svd, idx, plan, 60, st, &c->svd_par));
         PSKEL_TRY(batched_pinv(p.d_pinv + b0, cnt, ptiles, st));
         if (between) PSKEL_CUDA(cudaEventRecord(between, st));
-        if (o.precision == PSKEL_C64)
-            estimate_kernel<float2><<<cnt, 256, 0, st>>>(p.d_est + b0);
-        else
-            estimate_kernel<double2><<<cnt, 256, 0, st>>>(p.d_est + b0);
-        PSKEL_LAUNCHED(1);
-        return PSKEL_OK;
+        int rmax = 0, pemax = 0, pcmax = 0;
+        for (int i = b0; i < b0 + cnt; ++i) {
+            rmax = std::max(rmax, p.r[i]);
+            pemax = std::max(pemax, p.pe[i]);
+            pcmax = std::max(pcmax, p.pc[i]);
+        }
+        return launch_estimate(p.d_est + b0, cnt, o.precision, rmax, pemax, pcmax, st);
     };
     if (nch <= 1) {
         PSKEL_TRY(fill(0, p.d_fill_prefix, p.fill_jobs, p.fill_tiles, s));
@@ -922,11 +974,15 @@ int run_verify(pskel_ctx *c, const RoundPlan &p, const std::vector<int> &sel,
                                   reinterpret_cast<int *>(d + o_p), (int)nf, prefix.back(),
                                   c->flags.as<int>(), s));
     }
-    if (o.precision == PSKEL_C64)
-        estimate_kernel<float2><<<nv, 256, 0, s>>>(reinterpret_cast<EstJob *>(d + o_e));
-    else
-        estimate_kernel<double2><<<nv, 256, 0, s>>>(reinterpret_cast<EstJob *>(d + o_e));
-    PSKEL_LAUNCHED(1);
+    {
+        int rmax = 0, pemax = 0, pcmax = 0;
+        for (int v = 0; v < nv; ++v) {
+            rmax = std::max(rmax, w1[sel[v]].r);
+            pemax = std::max(pemax, pe2[v]);
+            pcmax = std::max(pcmax, pc2[v]);
+        }
+        PSKEL_TRY(launch_estimate(reinterpret_cast<EstJob *>(d + o_e), nv, o.precision, rmax, pemax, pcmax, s));
+    }
     std::vector<double> h_outs(8 * (size_t)nv);
     PSKEL_CUDA(cudaMemcpyAsync(h_outs.data(), outs, sizeof(double) * 8 * nv, cudaMemcpyDeviceToHost, s));
     PSKEL_CUDA(cudaStreamSynchronize(s));
