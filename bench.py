@@ -411,7 +411,11 @@ def run_ours(args, rank, world, dev):
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     octree_t = run_octree(args, m, part, dev) if rank == 0 else None
     aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only and not large) else None
-    # e2e: the public call path from host buffers: mesh + groups + features up, stats down
+    # e2e: the public call path from host buffers: mesh + groups + features up, stats down (its
+    # own engine; this one's device memory is released first, which the 122,880-RWG workload
+    # needs)
+    mirror = eng.mirror_of()
+    eng.close()
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
                                    fill_choice=tune["choice"])
     if args.save and rank == 0:
@@ -450,8 +454,8 @@ def run_ours(args, rank, world, dev):
         step_times_ms=[round(t, 3) for t in times],
         phases_ms={k: round(v, 3) for k, v in tinfo.items() if k in ("fill", "total")},
         product=dict(r_mean=float(st["r"].mean()), rounds_mean=float(st["rounds"].mean()),
-                     blocks_compressed=int(sum(1 for b, p in enumerate(eng.mirror_of()) if p < 0 or b < p)),
-                     blocks_mirrored=int(sum(1 for b, p in enumerate(eng.mirror_of()) if 0 <= p < b)),
+                     blocks_compressed=int(sum(1 for b, p in enumerate(mirror) if p < 0 or b < p)),
+                     blocks_mirrored=int(sum(1 for b, p in enumerate(mirror) if 0 <= p < b)),
                      first_round_accepted=float(np.mean(st["rounds"] == 1)),
                      err_max=float(err.max()), err_median=float(np.median(err)),
                      blocks_over_tol=int((err > TOL).sum()),

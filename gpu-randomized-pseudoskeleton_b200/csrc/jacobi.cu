@@ -197,7 +197,11 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 //      product of A and V would carry eps |A| in every column, which the inverse of a small
 //      singular value amplifies).
 // Columns of B whose norm is zero give zero columns of V.
-__global__ void __launch_bounds__(kSvdThreads)
+// Two instantiations: up to 512 threads (large cores), and up to 256 threads with five CTAs
+// per SM (at most 48 registers) for the classes of small cores, where more resident cores per
+// SM hide the latency of the rotation rounds.
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
     // blockDim.x is a multiple of 32 chosen by the launcher (enough lane teams for one round)
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -597,7 +601,8 @@ int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
 }
 
 int svd_resident_attr() {
-    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel, kSmemBudget));
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<kSvdThreads, 1>, kSmemBudget));
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<256, 5>, kSmemBudget));
     return ensure_smem_attr(svd_blocked_kernel, kSmemBudget);
 }
 
@@ -646,7 +651,10 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
     for (int ci : order) {
         const SvdPlan::Cls &c = plan.res[ci];
         cudaStream_t s = lane(l++);
-        svd_resident_kernel<<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
+        if (c.threads <= 256)
+            svd_resident_kernel<256, 5><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
+        else
+            svd_resident_kernel<kSvdThreads, 1><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
     if (plan.blk_count > 0) {
