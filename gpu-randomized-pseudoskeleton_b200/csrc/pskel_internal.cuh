@@ -60,6 +60,31 @@ struct DevBuf {
     template <typename T> T *as() const { return static_cast<T *>(ptr); }
 };
 
+// Page-locked host buffer: job tables are packed here and uploaded with one asynchronous copy
+// (a pageable source is staged by the driver and blocks the host for the transfer). The owner
+// must not repack it before the stream has consumed the previous upload.
+struct PinnedBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int reserve(size_t want) {
+        if (want <= bytes) return PSKEL_OK;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        size_t sz = want < 4096 ? 4096 : want;
+        sz = (sz + 4095) & ~size_t(4095);
+        PSKEL_CUDA(cudaHostAlloc(&ptr, sz, cudaHostAllocDefault));
+        bytes = sz;
+        return PSKEL_OK;
+    }
+    void release() {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T *as() const { return static_cast<T *>(ptr); }
+};
+
 // ------------------------------------------------------------------ mesh records
 // Per-RWG quadrature record: for the 2Q points of the basis (Q on T+, then Q on T-), seven
 // fields stored field-major: x[2Q] y[2Q] z[2Q] ux[2Q] uy[2Q] uz[2Q] d[2Q], where
@@ -215,7 +240,7 @@ struct SvdJob {
 // copy is used for sizes. Returns PSKEL_OK even if some job failed to converge (their status
 // field says so).
 int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
-                cudaStream_t stream, DevBuf &scratch);
+                cudaStream_t stream, DevBuf &scratch, bool dense = false);
 
 // The same work as a host plan (job order: resident jobs by size class, then blocked ones) and
 // launches from device tables, so the launches can be captured in a CUDA graph.
@@ -240,8 +265,9 @@ struct SvdStreams {
 };
 int svd_streams_create(SvdStreams &p);
 void svd_streams_destroy(SvdStreams &p);
+// dense: the classes of up to 256 threads run five CTAs per SM
 int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
-               cudaStream_t stream, const SvdStreams *par = nullptr);
+               cudaStream_t stream, const SvdStreams *par = nullptr, bool dense = false);
 // One resident job (m x n fits in shared memory) whose index map entry is d_idx0[0].
 int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
                                cudaStream_t stream);
