@@ -197,9 +197,11 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 //      product of A and V would carry eps |A| in every column, which the inverse of a small
 //      singular value amplifies).
 // Columns of B whose norm is zero give zero columns of V.
-// Two instantiations: up to 512 threads, and up to 256 threads with five CTAs per SM (at most
-// 48 registers, a few spilled) for the classes of small cores of callers that ask for it (the
-// recompression's truncated cores: 8 % faster; the pinv's cores: 2 % slower).
+// Two instantiations: up to 512 threads with at most 64 registers (two 512-thread CTAs or four
+// 256-thread CTAs per SM), and up to 256 threads with five CTAs per SM (at most 48 registers, a
+// few spilled) for the classes of small cores of callers that ask for it (the recompression's
+// truncated cores: 8 % faster; the pinv's cores: 2 % slower). Without the register cap the
+// compiler takes 104 registers and the 256-thread classes drop to two CTAs per SM (50 % slower).
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
@@ -601,7 +603,7 @@ int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
 }
 
 int svd_resident_attr() {
-    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<kSvdThreads, 1>, kSmemBudget));
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<kSvdThreads, 2>, kSmemBudget));
     PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<256, 5>, kSmemBudget));
     return ensure_smem_attr(svd_blocked_kernel, kSmemBudget);
 }
@@ -654,7 +656,7 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
         if (dense && c.threads <= 256)
             svd_resident_kernel<256, 5><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         else
-            svd_resident_kernel<kSvdThreads, 1><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
+            svd_resident_kernel<kSvdThreads, 2><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
     if (plan.blk_count > 0) {
