@@ -152,6 +152,7 @@ struct pskel_ctx {
     DevBuf recomp64, recomp64b;             // FP64 path: recompressed factors and workspace
     DevBuf rc_work, rc_tab, rc_idx;         // split path: workspace, job tables, SVD order
     pskel::PinnedBuf rc_host;               // split path: host copy of the job tables
+    std::vector<pskel::SvdJob> rc_hs;       // split path: host SVD jobs (kept: no per-call allocation)
     int recomp_path = 0;                    // 0 auto, 1 FP64 only, 2 split whenever eligible
     int recomp_split_blocks = 0;            // blocks of the last recompression on the split path
     std::vector<RecompSlot> recomp_slots;   // per block: C', R', S and the rank k

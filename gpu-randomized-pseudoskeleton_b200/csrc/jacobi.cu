@@ -197,11 +197,12 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 //      product of A and V would carry eps |A| in every column, which the inverse of a small
 //      singular value amplifies).
 // Columns of B whose norm is zero give zero columns of V.
-// Two instantiations: up to 512 threads with at most 64 registers (two 512-thread CTAs or four
-// 256-thread CTAs per SM), and up to 256 threads with five CTAs per SM (at most 48 registers, a
-// few spilled) for the classes of small cores of callers that ask for it (the recompression's
-// truncated cores: 8 % faster; the pinv's cores: 2 % slower). Without the register cap the
-// compiler takes 104 registers and the 256-thread classes drop to two CTAs per SM (50 % slower).
+// Two instantiations: up to 512 threads with at most 64 registers (one 512-thread CTA per 32 k
+// registers), and up to 256 threads with five CTAs per SM (at most 48 registers, a few spilled)
+// for the classes of small cores: more resident cores per SM hide the latency of the rotation
+// rounds (pinv of the 30,720-RWG round 13.4 -> 12.8 ms, recompression cores 6.2 -> 5.7 ms).
+// Without the register cap the compiler takes 104 registers and the 512-thread classes drop to
+// one CTA per SM.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
@@ -634,7 +635,7 @@ void svd_streams_destroy(SvdStreams &p) {
 }
 
 int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
-               cudaStream_t stream, const SvdStreams *par, bool dense) {
+               cudaStream_t stream, const SvdStreams *par) {
     PSKEL_TRY(svd_resident_attr());
     const int nl = (int)plan.res.size() + (plan.blk_count > 0 ? 1 : 0);
     // launch l on the main stream (l = 0) or on side stream l - 1 (the classes are independent)
@@ -653,7 +654,7 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
     for (int ci : order) {
         const SvdPlan::Cls &c = plan.res[ci];
         cudaStream_t s = lane(l++);
-        if (dense && c.threads <= 256)
+        if (c.threads <= 256)
             svd_resident_kernel<256, 5><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         else
             svd_resident_kernel<kSvdThreads, 2><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
@@ -682,7 +683,7 @@ int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, i
 }
 
 int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
-                cudaStream_t stream, DevBuf &scratch, bool dense) {
+                cudaStream_t stream, DevBuf &scratch) {
     if (h_jobs.empty()) return PSKEL_OK;
     SvdPlan plan;
     PSKEL_TRY(svd_plan(h_jobs, plan));
@@ -690,7 +691,7 @@ int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweep
     int *d_idx = scratch.as<int>();
     PSKEL_CUDA(cudaMemcpyAsync(d_idx, plan.idx.data(), sizeof(int) * plan.idx.size(),
                                cudaMemcpyHostToDevice, stream));
-    return svd_launch(d_jobs, d_idx, plan, max_sweeps, stream, nullptr, dense);
+    return svd_launch(d_jobs, d_idx, plan, max_sweeps, stream);
 }
 
 // ------------------------------------------------------------------ pseudo-inverse

@@ -240,7 +240,7 @@ struct SvdJob {
 // copy is used for sizes. Returns PSKEL_OK even if some job failed to converge (their status
 // field says so).
 int batched_svd(SvdJob *d_jobs, const std::vector<SvdJob> &h_jobs, int max_sweeps,
-                cudaStream_t stream, DevBuf &scratch, bool dense = false);
+                cudaStream_t stream, DevBuf &scratch);
 
 // The same work as a host plan (job order: resident jobs by size class, then blocked ones) and
 // launches from device tables, so the launches can be captured in a CUDA graph.
@@ -265,9 +265,8 @@ struct SvdStreams {
 };
 int svd_streams_create(SvdStreams &p);
 void svd_streams_destroy(SvdStreams &p);
-// dense: the classes of up to 256 threads run five CTAs per SM
 int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sweeps,
-               cudaStream_t stream, const SvdStreams *par = nullptr, bool dense = false);
+               cudaStream_t stream, const SvdStreams *par = nullptr);
 // One resident job (m x n fits in shared memory) whose index map entry is d_idx0[0].
 int svd_launch_single_resident(SvdJob *d_job, const int *d_idx0, int m, int n, int max_sweeps,
                                cudaStream_t stream);
