@@ -278,6 +278,14 @@ def run_ours(args, rank, world, dev):
         r0 = predict_r0()
         return eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
 
+    # chunks of the pipelined first round, picked by timing the product step (outside the timed
+    # region; 2 unless --pipeline is given)
+    if args.pipeline:
+        pipe = {"choice": args.pipeline, "ms": "given"}
+        eng.set_pipeline(args.pipeline)
+    else:
+        pipe = autotune.autotune_pipeline(eng, step, repeats=2, flush=flush)
+
     def without_symmetry(fn):
         def run():
             eng.set_symmetric(False)
@@ -383,7 +391,7 @@ def run_ours(args, rank, world, dev):
     eng.set_pipeline(1)
     st_np = eng.compress(TOL, r0=r0, use_graph=False, **PRODUCT)
     tph = eng.timing()
-    eng.set_pipeline(2)
+    eng.set_pipeline(pipe["choice"])
     fp32_peak = ctypes.c_double()
     fp64_peak = ctypes.c_double()
     _lib.check(L.pskel_fma_peak(ctypes.byref(fp32_peak), ctypes.byref(fp64_peak)))
@@ -417,7 +425,7 @@ def run_ours(args, rank, world, dev):
     mirror = eng.mirror_of()
     eng.close()
     e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
-                                   fill_choice=tune["choice"])
+                                   fill_choice=tune["choice"], pipeline=pipe["choice"])
     if args.save and rank == 0:
         np.savez(args.save, m=st["m"], n=st["n"], r=st["r"], rounds=st["rounds"], est=st["est"],
                  err=err, r_plain=st_plain["r"], rounds_plain=st_plain["rounds"],
@@ -435,6 +443,7 @@ def run_ours(args, rank, world, dev):
                     pinv_tau_relative=PRODUCT["tau"], estimator="16 extra rows + 16 extra columns, safety 2",
                     l2="512 MB write before every timed step (inputs also exceed L2)",
                     fill_variant=f"{tune['choice'][0]}{tune['choice'][1]} (autotuned: {tune['ms']} ms)",
+                    pipeline_chunks=f"{pipe['choice']} (autotuned step ms: {pipe['ms']})",
                     symmetry="one block of each (t,s)/(s,t) pair compressed, the other taken as its "
                              "transpose (Galerkin Z = Z^T); every block's error measured against its "
                              "own dense FP64 fill"),
@@ -758,7 +767,7 @@ def run_aca(m, part, dev, reps=3):
                      "one CTA per block, symmetric mode; wall time of the call")
 
 
-def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None):
+def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None, pipeline=None):
     """Host data in, compressed blocks resident on the GPU, per-block stats out."""
     import torch
 
@@ -774,6 +783,8 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
     eng = Engine(dev)
     if fill_choice is not None:  # the fill variant the autotuner picked for this GPU and workload
         autotune.apply(eng, PRODUCT["precision"], fill_choice)
+    if pipeline is not None:  # and the chunks of the pipelined round
+        eng.set_pipeline(pipeline)
     eng.set_symmetric(True)
     L = _lib.lib()
     feats_host = features(sp, K_WAVE, TOL)
@@ -974,6 +985,8 @@ def main():
     ap.add_argument("--fill-variant", default=None,
                     help="fill variant instead of the autotuner's choice: tri<w> or tri32_<w> "
                          "(w = 0 balanced, 4, 8, 16) or entry<s>")
+    ap.add_argument("--pipeline", type=int, default=0,
+                    help="chunks of the pipelined first round (1: off) instead of the autotuner's choice")
     ap.add_argument("--product-only", action="store_true",
                     help="time the product steps only (no baselines, ablations, checks): the "
                          "command the kernel launch list is captured from")

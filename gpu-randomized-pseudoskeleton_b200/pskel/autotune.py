@@ -1,5 +1,5 @@
-"""Autotuner of the fill launch: times the fill variants on the engine's own block list and
-keeps the fastest.
+"""Autotuners: the fill launch (times the fill variants on the engine's own block list and
+keeps the fastest) and the pipelined first round (times the product step per chunk count).
 
 The variants are the triangle-moment kernel with 4, 8 or 16 columns per CTA tile (usable while
 every group has at most 512 RWG; in complex FP32 also with the FP32 pair geometry) and the
@@ -88,3 +88,36 @@ def autotune_fill(eng, precision: str = "c64", samples: int = 24, repeats: int =
         with open(cache, "w") as f:
             json.dump(table, f, indent=1)
     return {"choice": choice, "ms": timings, "cached": False}
+
+
+PIPELINE_CHUNKS = (1, 2, 3, 4)
+
+
+def autotune_pipeline(eng, step, chunks=PIPELINE_CHUNKS, repeats: int = 3, flush=None) -> dict:
+    """Time the product step `step()` (a callable running one compression on eng) with the first
+    round split into each chunk count of `chunks` (1: not pipelined; pskel_set_pipeline) and
+    apply the fastest; returns {"choice": chunks, "ms": {chunks: best step ms}}. Device time of
+    the whole call (CUDA events), after one untimed run per setting; flush, if given, is a
+    tensor larger than L2 written before every timed run."""
+    import torch
+    timings = {}
+    for k in chunks:
+        eng.set_pipeline(k)
+        step()  # warm: tables, graph capture for this setting
+        step()
+        best = float("inf")
+        for _ in range(repeats):
+            if flush is not None:
+                flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            step()
+            e1.record()
+            torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        timings[k] = round(best, 3)
+    choice = min(timings, key=timings.get)
+    eng.set_pipeline(choice)
+    return {"choice": choice, "ms": timings}
