@@ -86,3 +86,26 @@ def test_fp32_geometry_matches_fp64_geometry(sphere):
         st = eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
         err = eng.true_errors()
         assert np.median(err) < 2e-5 and err.max() <= 1e-4
+
+
+def test_pipeline_autotuner_applies_a_timed_setting():
+    """The pipelined-round autotuner times the product step per chunk count and applies the
+    fastest; the compression it leaves behind is unchanged (pipelining does not change results).
+    The 7,680-RWG sphere has more than 2,048 blocks, so its first round is pipelined."""
+    m = pmesh.icosphere(2.0, 4)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        r0 = np.full(eng.n_blocks, 20, dtype=np.int32)
+        step = lambda: eng.compress(1e-4, precision="c64", tau=1e-7, r0=r0, oversample=0,
+                                    use_graph=True, seed=4)
+        eng.set_pipeline(1)
+        ref = step()
+        out = autotune.autotune_pipeline(eng, step, chunks=(1, 2, 3), repeats=1)
+        assert out["choice"] in (1, 2, 3) and set(out["ms"]) == {1, 2, 3}
+        assert out["ms"][out["choice"]] == min(out["ms"].values())
+        st = step()
+        for f in ("r", "rank", "rounds", "est"):
+            assert np.array_equal(st[f], ref[f]), f
