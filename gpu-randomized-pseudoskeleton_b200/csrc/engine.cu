@@ -145,7 +145,9 @@ static size_t sample_smem() {
 
 // Re-check of a block accepted with little margin: pe2 fresh extra rows and pc2 fresh extra
 // columns, drawn outside every row / column the block's round already used (I and Ix, J and
-// Jx), from Philox streams 4 (rows) and 5 (columns) of that round.
+// Jx), from Philox streams 4 (rows) and 5 (columns) of that round. Every block that may need one
+// is planned with its round; *gate, set on the device once the round's estimate is known,
+// says whether it runs.
 struct VerifyWork {
     const int *rows_g, *cols_g;
     const int *I, *J, *Ix, *Jx;  // the round's local samples
@@ -153,6 +155,7 @@ struct VerifyWork {
     int *Ig2, *Jg2;              // their global ids
     int m, n, r, pe, pc, pe2, pc2;
     int block_id, round;
+    const int *gate;
 };
 
 __global__ void __launch_bounds__(128) verify_sample_kernel(const VerifyWork *__restrict__ works,
@@ -163,6 +166,7 @@ __global__ void __launch_bounds__(128) verify_sample_kernel(const VerifyWork *__
     __shared__ int scan[kMaxGroup / 32];
     __shared__ int pick[kMaxExtra];
     const VerifyWork w = works[blockIdx.x];
+    if (*w.gate == 0) return;
     for (int side = 0; side < 2; ++side) {
         const int D = side == 0 ? w.m : w.n;
         const int *S0 = side == 0 ? w.I : w.J;
@@ -225,6 +229,7 @@ struct EstJob {
     int m, n, r, ldr, ldxr, pe, pc;
     double2 *T;       // scratch: C(Ix, :) U (pe x r), then U R(:, Jx) (r x pc)
     double *out;      // est, then the four sums (rows num, den, cols num, den)
+    const int *gate = nullptr;  // non-null: nothing is done while *gate is 0 (a re-check)
 };
 
 // SM: U and the scratch Tr, Sc live in shared memory (est_smem_bytes of the launch's largest
@@ -235,6 +240,7 @@ __global__ void __launch_bounds__(256) estimate_kernel(const EstJob *__restrict_
     extern __shared__ __align__(16) unsigned char est_smem[];
     __shared__ double s_red[4][256];
     const EstJob w = jobs[blockIdx.x];
+    if (w.gate && *w.gate == 0) return;
     const int r = w.r, pe = w.pe, pc = w.pc, n = w.n, m = w.m, ldr = w.ldr, ldxr = w.ldxr;
     const S *C = reinterpret_cast<const S *>(w.C);
     const S *Rm = reinterpret_cast<const S *>(w.R);
@@ -415,6 +421,30 @@ __global__ void collect_kernel(const BlockWork *__restrict__ works, const SvdJob
     out[b].sweeps = svd[b].sweeps;
 }
 
+// Which of the round's re-check candidates run: candidate v (the round's block idx[v]) passed
+// with little margin (status OK, est <= hi, not est <= lo).
+__global__ void verify_select_kernel(const int *__restrict__ idx, int nv, const RoundOut *__restrict__ outs,
+                                     double hi, double lo, int *gate) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= nv) return;
+    const RoundOut q = outs[idx[v]];
+    gate[v] = (q.status == PSKEL_OK && q.est <= hi && !(q.est <= lo)) ? 1 : 0;
+}
+
+// Extra rows and columns of a re-check: as many as are left outside the round's samples, up to
+// the option's counts.
+void verify_extent(int m, int n, int r, int pe, int pc, const pskel_opts_t &o, int *pe2, int *pc2) {
+    *pe2 = std::max(0, std::min(o.extra_rows, m - r - pe));
+    *pc2 = std::max(0, std::min(o.extra_cols, n - r - pc));
+}
+
+// The round's outcome buffer: RoundOut per block, then 8 doubles per re-check candidate (est on
+// the new samples alone, the four residual sums), then each candidate's gate.
+size_t al256(size_t x) { return (x + 255) & ~size_t(255); }
+size_t outs_vouts_offset(int nb) { return al256(sizeof(RoundOut) * (size_t)nb); }
+size_t outs_gates_offset(int nb, int nv) { return outs_vouts_offset(nb) + al256(sizeof(double) * 8 * (size_t)nv); }
+size_t outs_bytes(int nb, int nv) { return outs_gates_offset(nb, nv) + al256(sizeof(int) * (size_t)nv); }
+
 // ------------------------------------------------------------------ true errors
 __global__ void block_norm_kernel(const double2 *const *mats, const long long *sizes, double *out) {
     __shared__ double s[256];
@@ -530,6 +560,22 @@ struct RoundPlan {
     std::vector<int> ch_tiles, ch_pinv_tiles;
     std::vector<int *> ch_prefix, ch_idx;
     std::vector<SvdPlan> ch_svd;
+    // re-check candidates (round indices; set before planning) and the selection thresholds
+    std::vector<int> vcand;
+    double v_hi = 0, v_lo = 0;
+    // their tables (inside arena.tables), gated by the selection after the round's estimate
+    int nv = 0;
+    VerifyWork *d_vworks = nullptr;
+    FillJob *d_vfill = nullptr;
+    GroupFillJob *d_vgfill = nullptr;
+    int *d_vidx = nullptr, *d_gates = nullptr;
+    const int *const *d_vjgate = nullptr;  // per re-check fill job: its candidate's gate
+    // per pipeline chunk: its candidates [vc[k], vc[k+1]), fill jobs [vj[k], vj[k+1]) with their
+    // own tile prefix (from 0) and tile count
+    std::vector<int> vc, vj, vch_tiles;
+    std::vector<int *> vch_prefix;
+    EstJob *d_vest = nullptr;
+    int vtri_rows = 0, vrmax = 0, vpemax = 0, vpcmax = 0;
 };
 
 constexpr int kPipeMinBlocks = 2048;  // smaller rounds run as one chunk
@@ -541,6 +587,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     if ((int)c->arenas.size() <= p.round) c->arenas.resize(p.round + 1);
     RoundArena &ar = c->arenas[p.round];
     const size_t es = o.precision == PSKEL_C64 ? sizeof(float2) : sizeof(double2);
+    const int nv = (int)p.vcand.size();
+    p.nv = nv;
     // ---- keep arena
     std::vector<size_t> off(nb + 1, 0);
     size_t scratch_total = 0;
@@ -564,9 +612,24 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         off[i + 1] = off[i] + ((s + 255) & ~size_t(255));
         scratch_total += 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
     }
+    // re-check storage of every candidate after the blocks' scratch: the fresh extra columns
+    // (m x pc2) and rows (pe2 x n), their local and global ids, the estimate's scratch
+    std::vector<int> vpe2(nv), vpc2(nv);
+    std::vector<size_t> voff(nv + 1, 0);
+    for (int v = 0; v < nv; ++v) {
+        const int i = p.vcand[v], b = p.blocks[i];
+        const int m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
+        const int n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
+        verify_extent(m, n, p.r[i], p.pe[i], p.pc[i], o, &vpe2[v], &vpc2[v]);
+        size_t q = al16((size_t)m * vpc2[v] * es) + al16((size_t)vpe2[v] * n * es);
+        q += 4 * al16(sizeof(int) * (kMaxExtra + 1));
+        q += al16(sizeof(double2) * (size_t)(vpe2[v] + vpc2[v]) * p.r[i]);
+        voff[v + 1] = voff[v] + al256(q);
+    }
+    scratch_total = al256(scratch_total);
     PSKEL_TRY(ar.keep.reserve(off[nb] + 256));
-    PSKEL_TRY(ar.work.reserve(scratch_total + 256));
-    PSKEL_TRY(ar.outs.reserve(sizeof(RoundOut) * nb + 256));
+    PSKEL_TRY(ar.work.reserve(scratch_total + voff[nv] + 256));
+    PSKEL_TRY(ar.outs.reserve(outs_bytes(nb, nv) + 256));
     std::vector<BlockWork> works(nb);
     std::vector<FillJob> fills;
     fills.reserve(2 * nb);
@@ -712,6 +775,109 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         for (int i = b0; i < b1; ++i)
             p.ch_pinv_tiles[k] = std::max(p.ch_pinv_tiles[k], ((p.r[i] + 31) / 32) * ((p.r[i] + 31) / 32));
     }
+    // re-check tables of every candidate; the gates and outputs live in the outcome buffer
+    std::vector<VerifyWork> vws(nv);
+    std::vector<EstJob> vests(nv);
+    std::vector<FillJob> vfills;
+    std::vector<GroupFillJob> vgfills;
+    std::vector<const int *> vjgate;  // each re-check fill job's gate
+    std::vector<int> vjob0(nv + 1, 0);  // each candidate's first fill job
+    {
+        char *vb = sb + scratch_total;
+        char *ob = ar.outs.as<char>();
+        double *vouts = reinterpret_cast<double *>(ob + outs_vouts_offset(nb));
+        int *gates = reinterpret_cast<int *>(ob + outs_gates_offset(nb, nv));
+        p.d_gates = gates;
+        p.vrmax = p.vpemax = p.vpcmax = p.vtri_rows = 0;
+        for (int v = 0; v < nv; ++v) {
+            const int i = p.vcand[v];
+            const BlockWork &w = works[i];
+            const int b = w.block_id, pe2 = vpe2[v], pc2 = vpc2[v];
+            vjob0[v] = (int)vjgate.size();
+            char *q = vb + voff[v];
+            auto take = [&](size_t bytes) { char *x = q; q += al16(bytes); return x; };
+            VerifyWork &x = vws[v];
+            x.rows_g = w.rows_g;
+            x.cols_g = w.cols_g;
+            x.I = w.I;
+            x.J = w.J;
+            x.Ix = w.Ix;
+            x.Jx = w.Jx;
+            x.m = w.m;
+            x.n = w.n;
+            x.r = w.r;
+            x.pe = w.pe;
+            x.pc = w.pc;
+            x.pe2 = pe2;
+            x.pc2 = pc2;
+            x.block_id = b;
+            x.round = w.round;
+            x.gate = gates + v;
+            void *Xc = take((size_t)w.m * pc2 * es);
+            void *Xr = take((size_t)pe2 * w.n * es);
+            x.Ix2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+            x.Jx2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+            x.Ig2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+            x.Jg2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
+            double2 *T = reinterpret_cast<double2 *>(take(sizeof(double2) * (size_t)(pe2 + pc2) * w.r));
+            vests[v] = EstJob{w.C, w.Rx, w.U, Xr, Xc, x.Ix2, x.Jx2, w.m, w.n, w.r, w.r + w.pe,
+                              std::max(pe2, 1), pe2, pc2, T, vouts + 8 * (size_t)v, gates + v};
+            p.vrmax = std::max(p.vrmax, w.r);
+            p.vpemax = std::max(p.vpemax, pe2);
+            p.vpcmax = std::max(p.vpcmax, pc2);
+            const int gt = c->gt[b], gs = c->gs[b];
+            if (p.tri) {
+                const int *tr = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
+                const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
+                if (pc2 > 0) {
+                    vgfills.push_back(GroupFillJob{w.rows_g, tr + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
+                                                   x.Jg2, Xc, w.m, ntt, pc2, w.m, 0, tri_cols_for(c, ntt),
+                                                   guse_of(c, gt)});
+                    vjgate.push_back(gates + v);
+                    p.vtri_rows = std::max(p.vtri_rows, w.m);
+                }
+                if (pe2 > 0) {
+                    vgfills.push_back(GroupFillJob{w.cols_g, tr + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
+                                                   x.Ig2, Xr, w.n, nts, pe2, pe2, 1, tri_cols_for(c, nts),
+                                                   guse_of(c, gs)});
+                    vjgate.push_back(gates + v);
+                    p.vtri_rows = std::max(p.vtri_rows, w.n);
+                }
+            } else {
+                if (pc2 > 0) {
+                    vfills.push_back(FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2, w.m, 0});
+                    vjgate.push_back(gates + v);
+                }
+                if (pe2 > 0) {
+                    vfills.push_back(FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2, pe2, 1});
+                    vjgate.push_back(gates + v);
+                }
+            }
+        }
+    }
+    const size_t nvf = p.tri ? vgfills.size() : vfills.size();
+    std::vector<int> vprefix(nvf + 1, 0);
+    for (size_t f = 0; f < nvf; ++f)
+        vprefix[f + 1] = vprefix[f] + (p.tri ? (vgfills[f].nc + vgfills[f].tc - 1) / vgfills[f].tc
+                                             : ((vfills[f].nr + tm - 1) / tm) * ((vfills[f].nc + tn - 1) / tn));
+    // the re-checks by pipeline chunk (candidates are in round order, so each chunk's candidates
+    // and their fill jobs are contiguous)
+    vjob0[nv] = (int)nvf;
+    const int nchv = (int)p.cb.size() - 1;
+    p.vc.assign(nchv + 1, nv);
+    p.vj.assign(nchv + 1, (int)nvf);
+    p.vch_tiles.assign(nchv, 0);
+    std::vector<int> vch_prefix_all;
+    std::vector<size_t> vch_off(nchv);
+    for (int k = 0; k < nchv; ++k) {
+        p.vc[k] = (int)(std::lower_bound(p.vcand.begin(), p.vcand.end(), p.cb[k]) - p.vcand.begin());
+        p.vj[k] = vjob0[p.vc[k]];
+    }
+    for (int k = 0; k < nchv; ++k) {
+        vch_off[k] = vch_prefix_all.size();
+        for (int j = p.vj[k]; j <= p.vj[k + 1]; ++j) vch_prefix_all.push_back(vprefix[j] - vprefix[p.vj[k]]);
+        p.vch_tiles[k] = vprefix[p.vj[k + 1]] - vprefix[p.vj[k]];
+    }
     // pack tables
     size_t t = 0;
     auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
@@ -725,6 +891,12 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     const size_t o_est = slot(sizeof(EstJob) * nb);
     const size_t o_cpref = slot(sizeof(int) * ch_prefix_all.size());
     const size_t o_cidx = slot(sizeof(int) * (ch_idx_all.size() + 1));
+    const size_t o_vw = slot(sizeof(VerifyWork) * nv);
+    const size_t o_vf = p.tri ? slot(sizeof(GroupFillJob) * (nvf + 1)) : slot(sizeof(FillJob) * (nvf + 1));
+    const size_t o_vp = slot(sizeof(int) * vch_prefix_all.size());
+    const size_t o_ve = slot(sizeof(EstJob) * nv);
+    const size_t o_vi = slot(sizeof(int) * (nv + 1));
+    const size_t o_vg = slot(sizeof(const int *) * (nvf + 1));
     ar.h_tables.assign(t, 0);
     std::memcpy(ar.h_tables.data() + o_works, works.data(), sizeof(BlockWork) * nb);
     if (p.tri)
@@ -738,6 +910,13 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     std::memcpy(ar.h_tables.data() + o_est, ests.data(), sizeof(EstJob) * nb);
     std::memcpy(ar.h_tables.data() + o_cpref, ch_prefix_all.data(), sizeof(int) * ch_prefix_all.size());
     std::memcpy(ar.h_tables.data() + o_cidx, ch_idx_all.data(), sizeof(int) * ch_idx_all.size());
+    std::memcpy(ar.h_tables.data() + o_vw, vws.data(), sizeof(VerifyWork) * nv);
+    if (p.tri) std::memcpy(ar.h_tables.data() + o_vf, vgfills.data(), sizeof(GroupFillJob) * nvf);
+    else std::memcpy(ar.h_tables.data() + o_vf, vfills.data(), sizeof(FillJob) * nvf);
+    std::memcpy(ar.h_tables.data() + o_vp, vch_prefix_all.data(), sizeof(int) * vch_prefix_all.size());
+    std::memcpy(ar.h_tables.data() + o_ve, vests.data(), sizeof(EstJob) * nv);
+    std::memcpy(ar.h_tables.data() + o_vi, p.vcand.data(), sizeof(int) * nv);
+    std::memcpy(ar.h_tables.data() + o_vg, vjgate.data(), sizeof(const int *) * nvf);
     PSKEL_TRY(ar.tables.reserve(t + 256));
     PSKEL_CUDA(cudaMemcpyAsync(ar.tables.ptr, ar.h_tables.data(), t, cudaMemcpyHostToDevice,
                                c->stream));
@@ -752,6 +931,14 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.d_svd_idx = reinterpret_cast<int *>(d + o_idx);
     p.d_pinv = reinterpret_cast<PinvJob *>(d + o_pinv);
     p.d_est = reinterpret_cast<EstJob *>(d + o_est);
+    p.d_vworks = reinterpret_cast<VerifyWork *>(d + o_vw);
+    p.d_vfill = reinterpret_cast<FillJob *>(d + o_vf);
+    p.d_vgfill = reinterpret_cast<GroupFillJob *>(d + o_vf);
+    p.vch_prefix.assign(nchv, nullptr);
+    for (int k = 0; k < nchv; ++k) p.vch_prefix[k] = reinterpret_cast<int *>(d + o_vp) + vch_off[k];
+    p.d_vest = reinterpret_cast<EstJob *>(d + o_ve);
+    p.d_vidx = reinterpret_cast<int *>(d + o_vi);
+    p.d_vjgate = reinterpret_cast<const int *const *>(d + o_vg);
     p.ch_prefix.assign(nch, nullptr);
     p.ch_idx.assign(nch, nullptr);
     for (int k = 0; k < nch; ++k) {
@@ -808,10 +995,42 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
         }
         return launch_estimate(p.d_est + b0, cnt, o.precision, rmax, pemax, pcmax, st);
     };
+    const RoundOut *outs = c->arenas[p.round].outs.as<RoundOut>();
+    auto collect = [&](int b0, int cnt, cudaStream_t st) {
+        collect_kernel<<<(cnt + 255) / 256, 256, 0, st>>>(p.d_works + b0, p.d_svd + b0, cnt,
+                                                          c->arenas[p.round].outs.as<RoundOut>() + b0);
+        PSKEL_LAUNCHED(1);
+    };
+    // the re-check of chunk k's blocks accepted with little margin, selected on the device from
+    // their estimates: every candidate's launches are planned, the unselected return at once
+    auto verify = [&](int k, cudaStream_t st) -> int {
+        const int v0 = p.vc[k], cnt = p.vc[k + 1] - v0;
+        if (cnt <= 0) return PSKEL_OK;
+        verify_select_kernel<<<(cnt + 255) / 256, 256, 0, st>>>(p.d_vidx + v0, cnt, outs, p.v_hi, p.v_lo,
+                                                                p.d_gates + v0);
+        PSKEL_LAUNCHED(1);
+        verify_sample_kernel<<<cnt, 128, 0, st>>>(p.d_vworks + v0, o.seed);
+        PSKEL_LAUNCHED(1);
+        const int j0 = p.vj[k], nj = p.vj[k + 1] - j0;
+        if (p.vch_tiles[k] > 0) {
+            FillParams vf = fp;
+            vf.persistent = false;  // one CTA per tile: the tiles of unselected blocks retire at once
+            vf.max_rows = p.vtri_rows;
+            vf.gates = p.d_vjgate + j0;
+            if (p.tri)
+                PSKEL_TRY(launch_tri_fill(c->mesh, vf, p.d_vgfill + j0, p.vch_prefix[k], nj, p.vch_tiles[k], st));
+            else
+                PSKEL_TRY(launch_fill(c->mesh, vf, p.d_vfill + j0, p.vch_prefix[k], nj, p.vch_tiles[k],
+                                      c->flags.as<int>(), st));
+        }
+        return launch_estimate(p.d_vest + v0, cnt, o.precision, p.vrmax, p.vpemax, p.vpcmax, st);
+    };
     if (nch <= 1) {
         PSKEL_TRY(fill(0, p.d_fill_prefix, p.fill_jobs, p.fill_tiles, s));
         if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
         PSKEL_TRY(pinv_est(0, p.nb, p.svd, p.d_svd_idx, p.pinv_tiles, s, events ? c->ev[3] : nullptr));
+        collect(0, p.nb, s);
+        if (p.nv > 0) PSKEL_TRY(verify(0, s));
     } else {
         cudaStream_t s2 = c->pipe_stream;
         fp.persistent = false;
@@ -821,175 +1040,28 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
             PSKEL_CUDA(cudaEventRecord(c->pipe_ev[k], s));
             PSKEL_CUDA(cudaStreamWaitEvent(s2, c->pipe_ev[k], 0));
             PSKEL_TRY(pinv_est(b0, cnt, p.ch_svd[k], p.ch_idx[k], p.ch_pinv_tiles[k], s2, nullptr));
+            collect(b0, cnt, s2);
+            PSKEL_CUDA(cudaEventRecord(c->chunk_ev[k], s2));
         }
         if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));  // the last fill
+        // chunk k's re-check on the context's stream, beside the later chunks' SVD, pinv and
+        // estimate on the pipeline stream
+        if (p.nv > 0)
+            for (int k = 0; k < nch; ++k) {
+                PSKEL_CUDA(cudaStreamWaitEvent(s, c->chunk_ev[k], 0));
+                PSKEL_TRY(verify(k, s));
+            }
         PSKEL_CUDA(cudaEventRecord(c->pipe_ev[pskel_ctx::kMaxChunks], s2));
         PSKEL_CUDA(cudaStreamWaitEvent(s, c->pipe_ev[pskel_ctx::kMaxChunks], 0));
         if (events) PSKEL_CUDA(cudaEventRecord(c->ev[3], s));  // the last chunk's pinv and estimate
     }
     // (pipelined: ev[1..2] = the fills with the earlier chunks' pinv and estimate beside them,
-    // ev[2..3] = the last chunk's pinv and estimate, ev[3..4] = the collect)
-    collect_kernel<<<(p.nb + 255) / 256, 256, 0, s>>>(p.d_works, p.d_svd, p.nb,
-                                                     c->arenas[p.round].outs.as<RoundOut>());
-    PSKEL_LAUNCHED(1);
+    // ev[2..3] = the last chunk's pinv, estimate and the re-checks, ev[3..4] = nothing)
     if (events) PSKEL_CUDA(cudaEventRecord(c->ev[4], s));
     return PSKEL_OK;
 }
 
 int set_kernel_attrs() { return ensure_smem_attr(sample_kernel, sample_smem()); }
-
-// Re-check of the blocks `sel` (indices into the round plan p) on fresh extra rows and
-// columns: sample, fill and estimate launches on the context's stream; out receives 5 doubles
-// per re-checked block (est on the new samples alone, then the four residual sums).
-int run_verify(pskel_ctx *c, const RoundPlan &p, const std::vector<int> &sel,
-               const pskel_opts_t &o, std::vector<double> &out, double *entries) {
-    const int nv = (int)sel.size();
-    out.assign(5 * (size_t)nv, 0.0);
-    if (nv == 0) return PSKEL_OK;
-    const size_t es = o.precision == PSKEL_C64 ? sizeof(float2) : sizeof(double2);
-    const std::vector<char> &h1 = c->arenas[p.round].h_tables;
-    const BlockWork *w1 = reinterpret_cast<const BlockWork *>(h1.data());  // the round's works
-    const size_t outs_bytes = (sizeof(double) * 8 * (size_t)nv + 255) & ~size_t(255);
-    std::vector<size_t> off(nv + 1, outs_bytes);
-    std::vector<int> pe2(nv), pc2(nv);
-    for (int v = 0; v < nv; ++v) {
-        const BlockWork &w = w1[sel[v]];
-        pe2[v] = std::max(0, std::min(o.extra_rows, w.m - w.r - w.pe));
-        pc2[v] = std::max(0, std::min(o.extra_cols, w.n - w.r - w.pc));
-        const size_t m = w.m, n = w.n, r = w.r;
-        size_t b = al16(m * pc2[v] * es) + al16((size_t)pe2[v] * n * es);
-        b += 4 * al16(sizeof(int) * (kMaxExtra + 1));
-        b += al16(sizeof(double2) * (pe2[v] + pc2[v]) * r);
-        off[v + 1] = off[v] + ((b + 255) & ~size_t(255));
-    }
-    PSKEL_TRY(c->verify_keep.reserve(off[nv] + 256));
-    std::vector<VerifyWork> vw(nv);
-    std::vector<EstJob> ej(nv);
-    std::vector<FillJob> fills;
-    std::vector<GroupFillJob> gfills;
-    const bool tri = tri_for(c, o.precision);
-    char *base = c->verify_keep.as<char>();
-    double *outs = reinterpret_cast<double *>(base);  // 8 doubles per re-checked block
-    double ent = 0;
-    for (int v = 0; v < nv; ++v) {
-        const int i = sel[v];
-        const BlockWork &w = w1[i];
-        const int b = w.block_id;
-        char *q = base + off[v];
-        auto take = [&](size_t bytes) { char *x = q; q += al16(bytes); return x; };
-        VerifyWork &x = vw[v];
-        x.rows_g = w.rows_g;
-        x.cols_g = w.cols_g;
-        x.I = w.I;
-        x.J = w.J;
-        x.Ix = w.Ix;
-        x.Jx = w.Jx;
-        x.m = w.m;
-        x.n = w.n;
-        x.r = w.r;
-        x.pe = w.pe;
-        x.pc = w.pc;
-        x.pe2 = pe2[v];
-        x.pc2 = pc2[v];
-        x.block_id = b;
-        x.round = w.round;
-        void *Xc = take((size_t)w.m * pc2[v] * es);
-        void *Xr = take((size_t)pe2[v] * w.n * es);
-        x.Ix2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
-        x.Jx2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
-        x.Ig2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
-        x.Jg2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
-        double2 *T = reinterpret_cast<double2 *>(take(sizeof(double2) * (pe2[v] + pc2[v]) * (size_t)w.r));
-        double *res = outs + 8 * (size_t)v;
-        ej[v] = EstJob{w.C, w.Rx, w.U, Xr, Xc, x.Ix2, x.Jx2, w.m, w.n, w.r, w.r + w.pe,
-                       std::max(pe2[v], 1), pe2[v], pc2[v], T, res};
-        ent += (double)w.m * pc2[v] + (double)pe2[v] * w.n;
-        const int gt = c->gt[b], gs = c->gs[b];
-        if (tri) {
-            const int *tr = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
-            const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
-            if (pc2[v] > 0)
-                gfills.push_back(GroupFillJob{w.rows_g, tr + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                              x.Jg2, Xc, w.m, ntt, pc2[v], w.m, 0, tri_cols_for(c, ntt),
-                                              guse_of(c, gt)});
-            if (pe2[v] > 0)
-                gfills.push_back(GroupFillJob{w.cols_g, tr + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                              x.Ig2, Xr, w.n, nts, pe2[v], pe2[v], 1, tri_cols_for(c, nts),
-                                              guse_of(c, gs)});
-        } else {
-            if (pc2[v] > 0) fills.push_back(FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2[v], w.m, 0});
-            if (pe2[v] > 0) fills.push_back(FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2[v], pe2[v], 1});
-        }
-    }
-    *entries = ent;
-    int tm, tn;
-    fill_tile_shape(o.precision, c->em.q_test, entry_split_for(c, o.precision), &tm, &tn);
-    const size_t nf = tri ? gfills.size() : fills.size();
-    std::vector<int> prefix(nf + 1, 0);
-    int max_rows = 0;
-    for (size_t f = 0; f < nf; ++f) {
-        if (tri) {
-            prefix[f + 1] = prefix[f] + (gfills[f].nc + gfills[f].tc - 1) / gfills[f].tc;
-            max_rows = std::max(max_rows, gfills[f].m);
-        } else {
-            prefix[f + 1] = prefix[f] + ((fills[f].nr + tm - 1) / tm) * ((fills[f].nc + tn - 1) / tn);
-        }
-    }
-    size_t t = 0;
-    auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
-    const size_t o_w = slot(sizeof(VerifyWork) * nv);
-    const size_t o_f = tri ? slot(sizeof(GroupFillJob) * (nf + 1)) : slot(sizeof(FillJob) * (nf + 1));
-    const size_t o_p = slot(sizeof(int) * prefix.size());
-    const size_t o_e = slot(sizeof(EstJob) * nv);
-    std::vector<char> &h = c->verify_h_tables;
-    h.assign(t, 0);
-    std::memcpy(h.data() + o_w, vw.data(), sizeof(VerifyWork) * nv);
-    if (tri) std::memcpy(h.data() + o_f, gfills.data(), sizeof(GroupFillJob) * nf);
-    else std::memcpy(h.data() + o_f, fills.data(), sizeof(FillJob) * nf);
-    std::memcpy(h.data() + o_p, prefix.data(), sizeof(int) * prefix.size());
-    std::memcpy(h.data() + o_e, ej.data(), sizeof(EstJob) * nv);
-    PSKEL_TRY(c->verify_tables.reserve(t + 256));
-    cudaStream_t s = c->stream;
-    PSKEL_CUDA(cudaMemcpyAsync(c->verify_tables.ptr, h.data(), t, cudaMemcpyHostToDevice, s));
-    char *d = c->verify_tables.as<char>();
-    verify_sample_kernel<<<nv, 128, 0, s>>>(reinterpret_cast<VerifyWork *>(d + o_w), o.seed);
-    PSKEL_LAUNCHED(1);
-    if (prefix.back() > 0) {
-        FillParams fp;
-        fp.k = c->em.k;
-        fp.eta = c->em.eta;
-        fp.r_near = 0.0;
-        fp.q_test = c->em.q_test;
-        fp.q_src = c->em.q_src;
-        fp.precision = o.precision;
-        fp.split = entry_split_for(c, o.precision);
-        fp.tri_cols = c->tri_cols;
-            fp.geom32 = c->geom32;
-        fp.max_rows = max_rows;
-        if (tri)
-            PSKEL_TRY(launch_tri_fill(c->mesh, fp, reinterpret_cast<GroupFillJob *>(d + o_f),
-                                      reinterpret_cast<int *>(d + o_p), (int)nf, prefix.back(), s));
-        else
-            PSKEL_TRY(launch_fill(c->mesh, fp, reinterpret_cast<FillJob *>(d + o_f),
-                                  reinterpret_cast<int *>(d + o_p), (int)nf, prefix.back(),
-                                  c->flags.as<int>(), s));
-    }
-    {
-        int rmax = 0, pemax = 0, pcmax = 0;
-        for (int v = 0; v < nv; ++v) {
-            rmax = std::max(rmax, w1[sel[v]].r);
-            pemax = std::max(pemax, pe2[v]);
-            pcmax = std::max(pcmax, pc2[v]);
-        }
-        PSKEL_TRY(launch_estimate(reinterpret_cast<EstJob *>(d + o_e), nv, o.precision, rmax, pemax, pcmax, s));
-    }
-    std::vector<double> h_outs(8 * (size_t)nv);
-    PSKEL_CUDA(cudaMemcpyAsync(h_outs.data(), outs, sizeof(double) * 8 * nv, cudaMemcpyDeviceToHost, s));
-    PSKEL_CUDA(cudaStreamSynchronize(s));
-    for (int v = 0; v < nv; ++v)
-        for (int q = 0; q < 5; ++q) out[5 * (size_t)v + q] = h_outs[8 * (size_t)v + q];
-    return PSKEL_OK;
-}
 
 // Relative error from pooled residual sums (rows num, den, cols num, den): the larger side.
 double pooled_est(const double *a, const double *b) {
@@ -1028,6 +1100,11 @@ extern "C" int pskel_create(pskel_ctx **out, int device) {
         set_error(PSKEL_ERR_CUDA, "stream creation failed");
         return fail(PSKEL_ERR_CUDA);
     }
+    for (auto &e : c->chunk_ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            set_error(PSKEL_ERR_CUDA, "event creation failed");
+            return fail(PSKEL_ERR_CUDA);
+        }
     for (auto &e : c->pipe_ev)
         if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
             set_error(PSKEL_ERR_CUDA, "event creation failed");
@@ -1063,6 +1140,8 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->near_jobs.release(); c->near_mom.release(); c->near_data.release(); c->near_tab.release();
     c->aca_buf.release(); c->aca_tab.release();
     for (auto &e : c->pipe_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : c->chunk_ev)
         if (e) cudaEventDestroy(e);
     if (c->pipe_stream) cudaStreamDestroy(c->pipe_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1319,6 +1398,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
     PSKEL_CUDA(cudaEventCreate(&t1));
     PSKEL_CUDA(cudaEventRecord(t0, c->stream));
     std::vector<RoundOut> hout;
+    std::vector<char> hbuf;
     // rounds of an active set until every block of it is done
     auto run_rounds = [&](std::vector<int> active, bool allow_graph) -> int {
     int round = 0;
@@ -1335,6 +1415,19 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             p.pe[i] = std::min(o.extra_rows, mrows[b] - r_cur[b]);
             p.pc[i] = std::min(o.extra_cols, ncols[b] - r_cur[b]);
         }
+        // blocks whose estimate may pass with little margin (est within a factor est_verify of
+        // the acceptance threshold) are re-checked on fresh extra rows and columns, inside the
+        // round; candidates are the blocks that could still go on to another round
+        if (o.est_verify > 1.0) {
+            p.v_hi = o.tol / safety;
+            p.v_lo = o.tol / (safety * o.est_verify);
+            for (size_t i = 0; i < active.size(); ++i) {
+                const int b = active[i];
+                const bool more = mrows[b] - p.r[i] - p.pe[i] > 0 || ncols[b] - p.r[i] - p.pc[i] > 0;
+                if (more && r_cur[b] < Dmin[b] && round + 1 < o.max_rounds) p.vcand.push_back((int)i);
+            }
+        }
+        const int nv = (int)p.vcand.size();
         {
             double ent = 0;
             for (size_t i = 0; i < active.size(); ++i) {
@@ -1361,6 +1454,13 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             key.push_back(c->split[0] * 8 + c->split[1] + (c->use_tri ? 1000 : 0));
             key.push_back(c->tri_cols + 100 * c->geom32);
             key.push_back(c->pipe_chunks);
+            key.push_back(o.max_rounds);
+            for (double x : {p.v_hi, p.v_lo}) {  // the re-check's thresholds, bit for bit
+                int h[2];
+                std::memcpy(h, &x, sizeof(h));
+                key.push_back(h[0]);
+                key.push_back(h[1]);
+            }
             // capture only when the same first round ran eagerly before (warm, attributes set)
             const bool seen = key == c->last_key || (c->graph && key == c->graph_key);
             c->last_key = key;
@@ -1411,10 +1511,16 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
                 PSKEL_TRY(launch_round(c, p, o, true));
             }
         }
-        hout.resize(active.size());
-        PSKEL_CUDA(cudaMemcpyAsync(hout.data(), c->arenas[round].outs.ptr, sizeof(RoundOut) * active.size(),
-                                   cudaMemcpyDeviceToHost, c->stream));
+        // the round's outcome, the re-checks' sums and gates in one read-back
+        const int na = (int)active.size();
+        hbuf.resize(outs_bytes(na, nv));
+        PSKEL_CUDA(cudaMemcpyAsync(hbuf.data(), c->arenas[round].outs.ptr, hbuf.size(), cudaMemcpyDeviceToHost,
+                                   c->stream));
         PSKEL_CUDA(cudaStreamSynchronize(c->stream));
+        hout.resize(na);
+        std::memcpy(hout.data(), hbuf.data(), sizeof(RoundOut) * na);
+        const double *vouts = reinterpret_cast<const double *>(hbuf.data() + outs_vouts_offset(na));
+        const int *gates = reinterpret_cast<const int *>(hbuf.data() + outs_gates_offset(na, nv));
         {
             float ms = 0;
             const bool per_phase = !(try_graph);
@@ -1428,36 +1534,23 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
                 c->timing[1] += ms;  // graph replays are not split by phase
             }
         }
-        // re-check the blocks accepted with little margin (est within a factor est_verify of
-        // the acceptance threshold) on fresh extra rows and columns; they pass on the estimate
-        // pooled over both sample sets
-        std::vector<double> est(active.size());
-        for (size_t i = 0; i < active.size(); ++i) est[i] = hout[i].est;
-        if (o.est_verify > 1.0) {
-            std::vector<int> sel;
-            for (size_t i = 0; i < active.size(); ++i) {
-                const int b = active[i];
-                const bool pass = hout[i].status == PSKEL_OK && hout[i].est <= o.tol / safety;
-                const bool margin = hout[i].est <= o.tol / (safety * o.est_verify);
-                const bool more = mrows[b] - p.r[i] - p.pe[i] > 0 || ncols[b] - p.r[i] - p.pc[i] > 0;
-                if (pass && !margin && more && r_cur[b] < Dmin[b] && round + 1 < o.max_rounds)
-                    sel.push_back((int)i);
+        // the re-checked blocks pass on the estimate pooled over both sample sets
+        std::vector<double> est(na);
+        for (int i = 0; i < na; ++i) est[i] = hout[i].est;
+        {
+            double ent = 0;
+            for (int v = 0; v < nv; ++v) {
+                if (!gates[v]) continue;
+                const int i = p.vcand[v], b = active[i];
+                int pe2, pc2;
+                verify_extent(mrows[b], ncols[b], p.r[i], p.pe[i], p.pc[i], o, &pe2, &pc2);
+                ent += (double)mrows[b] * pc2 + (double)pe2 * ncols[b];
+                est[i] = pooled_est(hout[i].sums, vouts + 8 * (size_t)v + 1);
             }
-            if (!sel.empty()) {
-                std::vector<double> vout;
-                double ent = 0;
-                PSKEL_CUDA(cudaEventRecord(c->ev[0], c->stream));
-                PSKEL_TRY(run_verify(c, p, sel, o, vout, &ent));
-                PSKEL_CUDA(cudaEventRecord(c->ev[4], c->stream));
-                PSKEL_CUDA(cudaEventSynchronize(c->ev[4]));
-                float vms = 0;
-                cudaEventElapsedTime(&vms, c->ev[0], c->ev[4]);
-                c->timing[3] += vms;
+            if (ent > 0) {
                 c->timing[6] += ent;
                 c->timing[7] += ent * 4.0 * c->em.q_test * c->em.q_src;
                 c->timing[8] += 1;
-                for (size_t v = 0; v < sel.size(); ++v)
-                    est[sel[v]] = pooled_est(hout[sel[v]].sums, vout.data() + 5 * v + 1);
             }
         }
         std::vector<int> next;

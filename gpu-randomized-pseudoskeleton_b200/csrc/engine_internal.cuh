@@ -63,10 +63,11 @@ struct BlockResult {
 
 struct RoundArena {
     DevBuf keep;     // C, Rx, U, samples, sigma, est ... of the blocks of the round
-    DevBuf work;     // AV, V of the round (scratch, but owned per round so that a captured
-                     // round keeps valid pointers while later rounds grow their own)
+    DevBuf work;     // AV, V of the round and the storage of its re-checks (scratch, but owned
+                     // per round so that a captured round keeps valid pointers while later
+                     // rounds grow their own)
     DevBuf tables;   // device copies of the job tables
-    DevBuf outs;     // RoundOut per block of the round
+    DevBuf outs;     // RoundOut per block of the round, then its re-checks' sums and gates
     std::vector<char> h_tables;
 };
 
@@ -114,6 +115,7 @@ struct pskel_ctx {
     static constexpr int kMaxChunks = 8;
     cudaStream_t pipe_stream = nullptr;
     cudaEvent_t pipe_ev[kMaxChunks + 1] = {};
+    cudaEvent_t chunk_ev[kMaxChunks] = {};  // a chunk's outcome collected (its re-check may start)
     int pipe_chunks = 2;        // chunks of a round with at least kPipeMinBlocks blocks (1: off)
     double growth = 2.0;        // sample count factor from one round to the next (2: doubling)
     DevMesh mesh;
@@ -131,8 +133,6 @@ struct pskel_ctx {
     std::vector<double> h_vertex, h_ln, h_cent;  // host copies of the mesh arrays it is built from
     bool use_tri = false;
     std::vector<RoundArena> arenas;
-    DevBuf verify_keep, verify_tables;  // re-check of blocks accepted with little margin
-    std::vector<char> verify_h_tables;
     std::vector<BlockResult> graph_results;  // round-0 result slots of the captured graph
     std::vector<BlockResult> results;
     int precision = PSKEL_C128;

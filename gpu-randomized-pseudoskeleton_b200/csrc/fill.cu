@@ -59,11 +59,12 @@ template <typename T> struct FillOcc { static constexpr int value = sizeof(T) ==
 
 // Records are read from the FP64 record array; positions are staged in shared memory as G
 // (double) and the weighted RWG vectors/charges as T.
-template <typename T, int Q, int TM, int TN, int SPLIT>
+template <typename T, int Q, int TM, int TN, int SPLIT, bool GATED = false>
 __global__ void __launch_bounds__(TM *TN *SPLIT, FillOcc<T>::value)
     fill_kernel(const double *__restrict__ rec_t, const double *__restrict__ rec_s,
                 const FillJob *__restrict__ jobs, const int *__restrict__ tile_prefix, int njobs,
-                int total_tiles, T k, T kinv, double kphase, T scale, double r_near2, int *flags) {
+                int total_tiles, T k, T kinv, double kphase, T scale, double r_near2, int *flags,
+                const int *const *__restrict__ gates) {
     constexpr int NP = 2 * Q;
     constexpr int RS = (7 * NP) | 1;
     constexpr int PS = (3 * NP) | 1;  // staged position stride (doubles)
@@ -84,6 +85,9 @@ __global__ void __launch_bounds__(TM *TN *SPLIT, FillOcc<T>::value)
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const int jb = find_job(tile_prefix, njobs, tile);
+        if constexpr (GATED) {
+            if (*gates[jb] == 0) continue;  // uniform over the CTA
+        }
         const FillJob job = jobs[jb];
         const int local = tile - tile_prefix[jb];
         const int tiles_r = (job.nr + TM - 1) / TM;
@@ -274,12 +278,12 @@ template <typename T> struct Fill2Occ { static constexpr int value = sizeof(T) =
 // so every source point read from shared memory serves two entries. Source points are staged
 // as {x, y} (double2), z (double), {ux, uy, uz, e} (T4); test points field-major per row with
 // odd strides. Persistent grid over the tile list of all jobs, like fill_kernel.
-template <typename T, int Q, int TM, int TN>
+template <typename T, int Q, int TM, int TN, bool GATED = false>
 __global__ void __launch_bounds__(TM / 2 * TN, Fill2Occ<T>::value)
     fill2_kernel(const double *__restrict__ rec_t, const double *__restrict__ rec_s,
                  const FillJob *__restrict__ jobs, const int *__restrict__ tile_prefix,
                  int njobs, int total_tiles, T k, T kinv, double kturn, T scale,
-                 double r_near2, int *flags) {
+                 double r_near2, int *flags, const int *const *__restrict__ gates) {
     constexpr int NP = 2 * Q;
     constexpr int RS = (7 * NP) | 1;
     constexpr int PS = (3 * NP) | 1;
@@ -301,6 +305,9 @@ __global__ void __launch_bounds__(TM / 2 * TN, Fill2Occ<T>::value)
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const int jb = find_job(tile_prefix, njobs, tile);
+        if constexpr (GATED) {
+            if (*gates[jb] == 0) continue;  // uniform over the CTA
+        }
         const FillJob job = jobs[jb];
         const int local = tile - tile_prefix[jb];
         const int tiles_r = (job.nr + TM - 1) / TM;
@@ -434,7 +441,7 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     constexpr int NT = TM / 2 * TN;
     const size_t smem = (sizeof(double2) + sizeof(double) + 4 * sizeof(T)) * (size_t)TN * NP +
                         (sizeof(double) * PS + sizeof(T) * VS) * (size_t)TM + 16;
-    auto kern = fill2_kernel<T, Q, TM, TN>;
+    auto kern = p.gates ? fill2_kernel<T, Q, TM, TN, true> : fill2_kernel<T, Q, TM, TN, false>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -445,7 +452,7 @@ static int launch2_t(const double *rec, const FillParams &p, const FillJob *d_jo
     const double pi = 3.14159265358979323846;
     kern<<<(int)grid, NT, smem, stream>>>(rec, rec, d_jobs, d_prefix, njobs, total_tiles, (T)p.k,
                                           (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)),
-                                          p.r_near > 0 ? p.r_near * p.r_near : 0.0, d_flags);
+                                          p.r_near > 0 ? p.r_near * p.r_near : 0.0, d_flags, p.gates);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
@@ -459,7 +466,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     constexpr int VS = (4 * NP) | 1;
     constexpr int NT = TM * TN * SPLIT;
     const size_t smem = (sizeof(double) * PS + sizeof(T) * VS) * (size_t)(TM + TN) + 16;
-    auto kern = fill_kernel<T, Q, TM, TN, SPLIT>;
+    auto kern = p.gates ? fill_kernel<T, Q, TM, TN, SPLIT, true> : fill_kernel<T, Q, TM, TN, SPLIT, false>;
     PSKEL_TRY(ensure_smem_attr(kern, smem));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, NT, smem));
@@ -474,7 +481,7 @@ static int launch_t(const double *rec_t, const double *rec_s, const FillParams &
     const T scale = (T)(p.eta / (4.0 * pi));
     const double rn2 = p.r_near > 0 ? p.r_near * p.r_near : 0.0;
     kern<<<(int)grid, NT, smem, stream>>>(rec_t, rec_s, d_jobs, d_prefix, njobs, total_tiles, k,
-                                          kinv, kphase, scale, rn2, d_flags);
+                                          kinv, kphase, scale, rn2, d_flags, p.gates);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }
@@ -575,13 +582,13 @@ struct TriWeights {
 // and the phase of |D| reduced to a fraction of a turn are FP64; per pair, with e = x'_p - (y_q - y_0)
 // (both small), R^2 = |D|^2 + u with u = e . (2 D + e), and R - |D| = u / (R + |D|), all FP32:
 // the phase keeps an absolute error of ~1e-7 turn without FP64 arithmetic in the pair loop.
-template <typename T, int Q, int TN, bool OFS = false>
+template <typename T, int Q, int TN, bool OFS = false, bool GATED = false>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
     tri_fill_kernel(const double *__restrict__ tri_rec, const double *__restrict__ rec_s,
                     const double *__restrict__ edges, const double *__restrict__ vertex,
                     const double *__restrict__ ln, const GroupFillJob *__restrict__ jobs,
                     const int *__restrict__ tile_prefix, int njobs, int total_tiles, T k,
-                    T kinv, double kturn, T scale, TriWeights wq) {
+                    T kinv, double kturn, T scale, TriWeights wq, const int *const *__restrict__ gates) {
     constexpr int NP = 2 * Q;
     constexpr int RS = (7 * NP) | 1;
     constexpr int TS = tri_stride(Q);
@@ -596,6 +603,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
 
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const int jb = find_job(tile_prefix, njobs, tile);
+        if constexpr (GATED) {
+            if (*gates[jb] == 0) continue;  // uniform over the CTA
+        }
         const GroupFillJob job = jobs[jb];
         const int tcols = job.tc > 0 && job.tc < TN ? job.tc : TN;  // this job's tile width
         const int j0 = (tile - tile_prefix[jb]) * tcols;
@@ -776,7 +786,7 @@ static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillP
         (sizeof(double2) + sizeof(double) + 4 * sizeof(T) + (OFS ? sizeof(float4) : 0)) * (size_t)TN * NP;
     const int rows = p.max_rows > 0 && p.max_rows < kTriFillMaxRows ? p.max_rows : kTriFillMaxRows;
     const size_t smem = rec_bytes + 2 * sizeof(T) * (size_t)rows * TN + 16;
-    auto kern = tri_fill_kernel<T, Q, TN, OFS>;
+    auto kern = p.gates ? tri_fill_kernel<T, Q, TN, OFS, true> : tri_fill_kernel<T, Q, TN, OFS, false>;
     PSKEL_TRY(ensure_smem_attr(kern, rec_bytes + 2 * sizeof(T) * (size_t)kTriFillMaxRows * TN + 16));
     int per_sm = 0;
     PSKEL_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, smem));
@@ -791,7 +801,7 @@ static int launch_tri_t(const DevMesh &mesh, const MeshRecords &rec, const FillP
     kern<<<(int)grid, 256, smem, stream>>>(
         rec.tri.as<double>(), rec.f64.as<double>(), mesh.edges.as<double>(),
         mesh.vertex.as<double>(), mesh.ln.as<double>(), d_jobs, d_prefix, njobs, total_tiles,
-        (T)p.k, (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)), w);
+        (T)p.k, (T)(1.0 / p.k), p.k / (2.0 * pi), (T)(p.eta / (4.0 * pi)), w, p.gates);
     PSKEL_LAUNCHED(1);
     return PSKEL_OK;
 }

@@ -149,6 +149,9 @@ struct FillParams {
     bool persistent = true;  // grid of SM count x occupancy striding over the tiles; false: one
                              // CTA per tile (CTAs retire continually, so kernels on other streams
                              // can take their place)
+    const int *const *gates = nullptr;  // non-null: per job, a device flag; the tiles of a job
+                                        // whose flag is 0 do nothing (jobs planned ahead whose
+                                        // use is decided on the device)
 };
 
 // Launch the batched fill over jobs (device array) with tile prefix offsets computed on the
