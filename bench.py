@@ -834,12 +834,13 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
 #   python bench.py --profile-case store --calls 5
 #   python bench.py --profile-case extras
 #   python bench.py --profile-case recompress --calls 2 [--subdiv 5]
-def fill_case(prec, calls, split, geom32):
+def fill_case(prec, calls, split, geom32, tri_cols=8):
     """CALLS single-round compressions of every far block of the 7,680-RWG sphere at a fixed
     sample count of 24 with the given precision (c128 or c64) and fill variant (8: triangle
     moments, the default; 0: two rows per thread; 1, 2, 4: lanes per entry; geom32 = 1:
-    complex-FP32 fill with FP32 pair geometry), printing the fill time and point-pair rate of
-    each call. Under a profiler the fill launch of call i is the i-th launch of the fill kernel."""
+    complex-FP32 fill with FP32 pair geometry; tri_cols: columns per triangle-moment tile, 0 =
+    balanced per job), printing the fill time and point-pair rate of each call. Under a profiler
+    the fill launch of call i is the i-th launch of the fill kernel."""
     from pskel import mesh as pmesh
     from pskel import octree
     from pskel.engine import Engine
@@ -853,6 +854,7 @@ def fill_case(prec, calls, split, geom32):
         else:
             eng.set_fill_split(split_c64=split)
             eng.set_fill_geometry(bool(geom32))
+        eng.set_tri_cols(tri_cols)
         for i in range(calls):
             eng.compress(1.0, precision=prec, r0=np.full(part.n_blocks, 24), oversample=0,
                          max_rounds=1, seed=i)
@@ -997,12 +999,14 @@ def main():
     ap.add_argument("--calls", type=int, default=3, help="profiling cases: calls of the kernel")
     ap.add_argument("--split", type=int, default=8, help="profiling case fill: fill variant")
     ap.add_argument("--geom32", type=int, default=0, help="profiling case fill: FP32 pair geometry")
+    ap.add_argument("--tri-cols", type=int, default=8,
+                    help="profiling case fill: columns per triangle-moment tile (0: balanced per job)")
     ap.add_argument("--subdiv", type=int, default=4,
                     help="profiling case recompress: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
     args = ap.parse_args()
     if args.profile_case:
         if args.profile_case == "fill":
-            fill_case(args.precision, args.calls, args.split, args.geom32)
+            fill_case(args.precision, args.calls, args.split, args.geom32, args.tri_cols)
         elif args.profile_case == "store":
             store_case(args.calls)
         elif args.profile_case == "recompress":

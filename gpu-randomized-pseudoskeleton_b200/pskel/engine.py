@@ -372,7 +372,8 @@ class Engine:
         _lib.check(self._lib.pskel_set_fill_split(self._h, int(split_c128), int(split_c64)))
 
     def set_tri_cols(self, cols: int):
-        """Columns per CTA tile of the triangle-moment fill (4, 8 or 16)."""
+        """Columns per CTA tile of the triangle-moment fill (4, 8 or 16; 0: per job, the width
+        up to 16 that fills the CTA best)."""
         _lib.check(self._lib.pskel_set_tri_cols(self._h, int(cols)))
 
     def set_round_growth(self, factor: float):
