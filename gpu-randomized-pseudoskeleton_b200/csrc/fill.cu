@@ -216,26 +216,23 @@ __device__ __forceinline__ void sincos_2pi(float g, int q, float *s, float *c) {
     rotate_quadrant(q, sn, cs, s, c);
 }
 
-// sin/cos(2 pi g) for |g| <= 1/4 turn (|theta| <= pi/2), no quadrant rotation: the Taylor series
-// in g itself, coefficients (-1)^j (2 pi)^n / n!, truncated where the first omitted term is below
-// FP32 rounding at pi/2 (sin: theta^13/13! ~ 6e-8, cos: theta^14/14! ~ 6e-9). Used with a
-// half-turn reduction t = n/2 + g, where sin and cos of 2 pi t both take the sign (-1)^n.
-__host__ __device__ constexpr double two_pi_pow(int n) { return n == 0 ? 1.0 : 6.28318530717958647692 * two_pi_pow(n - 1); }
-__host__ __device__ constexpr double taylor_2pi(int n) { return two_pi_pow(n) * inv_fact(n); }
-
+// sin/cos(2 pi g) for |g| <= 1/4 turn (|theta| <= pi/2), no quadrant rotation, as polynomials in
+// s = g^2 on [0, 1/16]: sin(2 pi g) = g P(s), cos(2 pi g) = 1 + s Q(s), P and Q of degree 4 that
+// interpolate sin(2 pi g) / g and (cos(2 pi g) - 1) / g^2 at the five Chebyshev nodes of the
+// interval (near-minimax: 7e-9 and 9e-10 before rounding, below FP32's own rounding; evaluated
+// in FP32 both stay within 1.3 ulp of 1, as the degree-5 and -6 Taylor series in g did). Used
+// with a half-turn reduction t = n/2 + g, where sin and cos of 2 pi t both take the sign (-1)^n.
 __device__ __forceinline__ void sincos_2pi_half(float g, float *s, float *c) {
     const float t2 = g * g;
-    float ps = fmaf(t2, -(float)taylor_2pi(11), (float)taylor_2pi(9));
-    ps = fmaf(t2, ps, -(float)taylor_2pi(7));
-    ps = fmaf(t2, ps, (float)taylor_2pi(5));
-    ps = fmaf(t2, ps, -(float)taylor_2pi(3));
-    ps = fmaf(t2, ps, (float)taylor_2pi(1));
+    float ps = fmaf(t2, 39.759827f, -76.58117f);
+    ps = fmaf(t2, ps, 81.60248f);
+    ps = fmaf(t2, ps, -41.341682f);
+    ps = fmaf(t2, ps, 6.2831855f);
     *s = g * ps;
-    float pc = fmaf(t2, (float)taylor_2pi(12), -(float)taylor_2pi(10));
-    pc = fmaf(t2, pc, (float)taylor_2pi(8));
-    pc = fmaf(t2, pc, -(float)taylor_2pi(6));
-    pc = fmaf(t2, pc, (float)taylor_2pi(4));
-    pc = fmaf(t2, pc, -(float)taylor_2pi(2));
+    float pc = fmaf(t2, -25.218163f, 60.17904f);
+    pc = fmaf(t2, pc, -85.45536f);
+    pc = fmaf(t2, pc, 64.939384f);
+    pc = fmaf(t2, pc, -19.739208f);
     *c = fmaf(t2, pc, 1.0f);
 }
 
@@ -668,7 +665,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 3)
                 // pair u = |R|^2 - |D|^2 = c_p + |d_q|^2 - 2 A_p . d_q (d_q = y_q - y_0)
                 const float Ax = fmaf(0.5f, D2x, ex0), Ay = fmaf(0.5f, D2y, ey0), Az = fmaf(0.5f, D2z, ez0);
                 const float cp = fmaf(ex0, fmaf(1.0f, D2x, ex0), fmaf(ey0, D2y + ey0, ez0 * (D2z + ez0)));
-#pragma unroll 2
+#pragma unroll(OFS ? 7 : 2)
                 for (int q = 0; q < NP; ++q) {
                     T rinv, sn, cs;
                     int quad;
@@ -854,7 +851,9 @@ int launch_tri_fill(const DevMesh &mesh, const FillParams &p, const GroupFillJob
 }
 
 // ---------------------------------------------------------------- diagnostics
-// The fill's sin/cos of 2 pi t next to CUDA's sincospi(2 t), for tests of the polynomial.
+// The fill's sin/cos of 2 pi t next to CUDA's sincospi(2 t), for tests of the polynomials: the
+// quarter-turn forms in FP64 and FP32, CUDA's values, then the half-turn FP32 form of the
+// complex-FP32 fill with FP32 pair geometry (t = n/2 + g, sign (-1)^n).
 __global__ void diag_sincos_kernel(const double *t, int n, double *out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -866,12 +865,18 @@ __global__ void diag_sincos_kernel(const double *t, int n, double *out) {
     sincos_2pi((float)g, q, &sf, &cf);
     double rs, rc;
     sincospi(2.0 * t[i], &rs, &rc);
-    out[6 * i + 0] = s;
-    out[6 * i + 1] = c;
-    out[6 * i + 2] = sf;
-    out[6 * i + 3] = cf;
-    out[6 * i + 4] = rs;
-    out[6 * i + 5] = rc;
+    const double nh = rint(2.0 * t[i]);
+    float sh, ch;
+    sincos_2pi_half((float)(t[i] - 0.5 * nh), &sh, &ch);
+    const float sg = ((long long)nh & 1) ? -1.0f : 1.0f;
+    out[8 * i + 0] = s;
+    out[8 * i + 1] = c;
+    out[8 * i + 2] = sf;
+    out[8 * i + 3] = cf;
+    out[8 * i + 4] = rs;
+    out[8 * i + 5] = rc;
+    out[8 * i + 6] = sg * sh;
+    out[8 * i + 7] = sg * ch;
 }
 
 }  // namespace pskel

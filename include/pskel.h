@@ -500,9 +500,10 @@ int pskel_mlp_adam(float *params, const float *grad, float *m, float *v, int t, 
 int pskel_pinv_noalloc(const pskel_c128 *A, int M, int N, double tau, int relative,
                        pskel_c128 *P, double *sigma, int *rank, void *stream);
 
-/* Diagnostics: for n phases t (DEVICE array, in wavelengths) writes 6 values per phase to
-   out: the fill kernels' own sin(2 pi t), cos(2 pi t) in FP64, the same in FP32, and CUDA's
-   sincospi(2 t) for comparison. Runs on the legacy default stream. No reference counterpart. */
+/* Diagnostics: for n phases t (DEVICE array, in wavelengths) writes 8 values per phase to
+   out: the fill kernels' own sin(2 pi t), cos(2 pi t) in FP64, the same in FP32, CUDA's
+   sincospi(2 t) for comparison, then the half-turn FP32 form of the complex-FP32 fill with FP32
+   pair geometry. Runs on the legacy default stream. No reference counterpart. */
 int pskel_diag_sincos(const double *t, int n, double *out);
 
 /* Device kernels launched by this library since load (graph replays count their kernel

@@ -95,17 +95,19 @@ def test_q7_device_fill_matches_oracle(prec, bar):
 
 
 def test_fill_sincos_against_cuda_sincospi():
-    """The fill kernels' own quarter-turn Taylor sin/cos against CUDA's sincospi: FP64 within
-    a few ulp, FP32 within a few FP32 ulp, over phases of 0 to 40 wavelengths."""
+    """The fill kernels' own sin/cos against CUDA's sincospi: the quarter-turn Taylor forms in
+    FP64 within a few ulp and in FP32 within a few FP32 ulp, the half-turn near-minimax FP32 form
+    within a few FP32 ulp, over phases of 0 to 40 wavelengths."""
     import ctypes
     import torch
     rng = np.random.default_rng(0)
     t = np.concatenate([rng.uniform(0, 40, 200000), np.arange(0, 40, 0.125),
                         np.arange(0, 40, 0.125) + 1e-9, [1e-12, 0.0625, 0.1875]])
     td = torch.from_numpy(t).cuda()
-    out = torch.empty(6 * len(t), dtype=torch.float64, device="cuda")
+    out = torch.empty(8 * len(t), dtype=torch.float64, device="cuda")
     _lib.check(_lib.lib().pskel_diag_sincos(ctypes.c_void_p(td.data_ptr()), len(t),
                                            ctypes.c_void_p(out.data_ptr())))
-    o = out.cpu().numpy().reshape(-1, 6)
+    o = out.cpu().numpy().reshape(-1, 8)
     assert np.abs(o[:, 0] - o[:, 4]).max() < 4e-16 and np.abs(o[:, 1] - o[:, 5]).max() < 4e-16
     assert np.abs(o[:, 2] - o[:, 4]).max() < 3e-7 and np.abs(o[:, 3] - o[:, 5]).max() < 3e-7
+    assert np.abs(o[:, 6] - o[:, 4]).max() < 3e-7 and np.abs(o[:, 7] - o[:, 5]).max() < 3e-7
