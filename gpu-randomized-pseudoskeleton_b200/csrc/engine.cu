@@ -581,6 +581,9 @@ struct RoundPlan {
 constexpr int kPipeMinBlocks = 2048;  // smaller rounds run as one chunk
 
 // Lay out the round's storage, build all job tables on the host and upload them in one copy.
+// A first pass sizes everything (storage, fill tiles, pipeline chunks, re-check extents), so
+// that the second writes every table once, straight into the context's page-locked staging
+// buffer, from which one asynchronous copy uploads them.
 int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     const int nb = (int)p.blocks.size();
     p.nb = nb;
@@ -589,13 +592,31 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     const size_t es = o.precision == PSKEL_C64 ? sizeof(float2) : sizeof(double2);
     const int nv = (int)p.vcand.size();
     p.nv = nv;
-    // ---- keep arena
+    p.tri = tri_for(c, o.precision);
+    int tm, tn;
+    fill_tile_shape(o.precision, c->em.q_test, entry_split_for(c, o.precision), &tm, &tn);
+    auto rows_of = [&](int g) { return c->gptr[g + 1] - c->gptr[g]; };
+    auto tris_of = [&](int g) { return c->gtri_ptr[g + 1] - c->gtri_ptr[g]; };
+    // triangle-moment tile width of each group's jobs
+    std::vector<int> gtc;
+    if (p.tri) {
+        gtc.resize(c->gptr.size() - 1);
+        for (size_t g = 0; g < gtc.size(); ++g) gtc[g] = tri_cols_for(c, tris_of((int)g));
+    }
+    // tiles of a fill job of nr rows (group g) and nc columns
+    auto job_tiles = [&](int g, int nr, int nc) {
+        if (p.tri) return (nc + gtc[g] - 1) / gtc[g];
+        return ((nr + tm - 1) / tm) * ((nc + tn - 1) / tn);
+    };
+    // ---- first pass: keep arena, scratch, fill tiles (C, then Rx, of each block)
     std::vector<size_t> off(nb + 1, 0);
+    std::vector<int> prefix(2 * (size_t)nb + 1, 0);
     size_t scratch_total = 0;
+    int max_pinv_tiles = 0;
+    p.tri_rows = 0;
     for (int i = 0; i < nb; ++i) {
-        const int b = p.blocks[i];
-        const size_t m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
-        const size_t n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
+        const int b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
+        const size_t m = rows_of(gt), n = rows_of(gs);
         const size_t r = p.r[i], pe = p.pe[i], pc = p.pc[i];
         size_t s = 0;
         s += al16(m * (r + pc) * es);       // C (+ extra columns)
@@ -611,45 +632,112 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         s += 16 + 64;                       // rank; est and its four sums
         off[i + 1] = off[i] + ((s + 255) & ~size_t(255));
         scratch_total += 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
+        prefix[2 * i + 1] = prefix[2 * i] + job_tiles(gt, (int)m, (int)(r + pc));
+        prefix[2 * i + 2] = prefix[2 * i + 1] + job_tiles(gs, (int)n, (int)(r + pe));
+        if (p.tri) p.tri_rows = std::max(p.tri_rows, (int)std::max(m, n));
+        max_pinv_tiles = std::max(max_pinv_tiles, (int)(((r + 31) / 32) * ((r + 31) / 32)));
     }
     // re-check storage of every candidate after the blocks' scratch: the fresh extra columns
-    // (m x pc2) and rows (pe2 x n), their local and global ids, the estimate's scratch
-    std::vector<int> vpe2(nv), vpc2(nv);
+    // (m x pc2) and rows (pe2 x n), their local and global ids, the estimate's scratch; its fill
+    // jobs (extra columns, then extra rows, where there are any) and their tiles
+    std::vector<int> vpe2(nv), vpc2(nv), vjob0(nv + 1, 0);
     std::vector<size_t> voff(nv + 1, 0);
+    std::vector<int> vprefix(1, 0);
+    vprefix.reserve(2 * (size_t)nv + 1);
+    p.vrmax = p.vpemax = p.vpcmax = p.vtri_rows = 0;
     for (int v = 0; v < nv; ++v) {
-        const int i = p.vcand[v], b = p.blocks[i];
-        const int m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
-        const int n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
+        const int i = p.vcand[v], b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
+        const int m = rows_of(gt), n = rows_of(gs);
         verify_extent(m, n, p.r[i], p.pe[i], p.pc[i], o, &vpe2[v], &vpc2[v]);
         size_t q = al16((size_t)m * vpc2[v] * es) + al16((size_t)vpe2[v] * n * es);
         q += 4 * al16(sizeof(int) * (kMaxExtra + 1));
         q += al16(sizeof(double2) * (size_t)(vpe2[v] + vpc2[v]) * p.r[i]);
         voff[v + 1] = voff[v] + al256(q);
+        vjob0[v] = (int)vprefix.size() - 1;
+        if (vpc2[v] > 0) {
+            vprefix.push_back(vprefix.back() + job_tiles(gt, m, vpc2[v]));
+            if (p.tri) p.vtri_rows = std::max(p.vtri_rows, m);
+        }
+        if (vpe2[v] > 0) {
+            vprefix.push_back(vprefix.back() + job_tiles(gs, n, vpe2[v]));
+            if (p.tri) p.vtri_rows = std::max(p.vtri_rows, n);
+        }
+        p.vrmax = std::max(p.vrmax, p.r[i]);
+        p.vpemax = std::max(p.vpemax, vpe2[v]);
+        p.vpcmax = std::max(p.vpcmax, vpc2[v]);
     }
+    const int nvf = (int)vprefix.size() - 1;
+    vjob0[nv] = nvf;
     scratch_total = al256(scratch_total);
     PSKEL_TRY(ar.keep.reserve(off[nb] + 256));
     PSKEL_TRY(ar.work.reserve(scratch_total + voff[nv] + 256));
     PSKEL_TRY(ar.outs.reserve(outs_bytes(nb, nv) + 256));
-    std::vector<BlockWork> works(nb);
-    std::vector<FillJob> fills;
-    fills.reserve(2 * nb);
-    std::vector<GroupFillJob> gfills;
-    if (tri_for(c, o.precision)) gfills.reserve(2 * nb);
-    std::vector<SvdJob> svds(nb);
-    std::vector<PinvJob> pinvs(nb);
-    std::vector<EstJob> ests(nb);
+    // pipeline chunks, each with its own tables, of decreasing fill work: chunk k ends at the
+    // fraction 1 - (1 - k/K)^2 of the tiles, so the early chunks' pinv and estimate run beside
+    // the many later fills and the last chunk, whose pinv and estimate run alone, is small
+    const int K = (nb >= kPipeMinBlocks && c->pipe_chunks > 1) ? std::min(c->pipe_chunks, pskel_ctx::kMaxChunks) : 1;
+    p.cb.assign(1, 0);
+    {
+        const long long total = prefix.back();
+        int b = 0;
+        for (int k = 1; k < K; ++k) {
+            const double left = 1.0 - (double)k / K;
+            const long long want = (long long)((1.0 - left * left) * (double)total);
+            while (b < nb && prefix[2 * (size_t)b] < want) ++b;
+            if (b > p.cb.back()) p.cb.push_back(b);
+        }
+        p.cb.push_back(nb);
+    }
+    const int nch = (int)p.cb.size() - 1;
+    // the re-checks by pipeline chunk (candidates are in round order, so each chunk's candidates
+    // and their fill jobs are contiguous)
+    p.vc.assign(nch + 1, nv);
+    p.vj.assign(nch + 1, nvf);
+    p.vch_tiles.assign(nch, 0);
+    for (int k = 0; k < nch; ++k) {
+        p.vc[k] = (int)(std::lower_bound(p.vcand.begin(), p.vcand.end(), p.cb[k]) - p.vcand.begin());
+        p.vj[k] = vjob0[p.vc[k]];
+    }
+    // ---- table layout in the staging buffer (and, at the same offsets, on the device)
+    size_t t = 0;
+    auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
+    const size_t o_works = slot(sizeof(BlockWork) * nb);
+    const size_t o_fill = p.tri ? slot(sizeof(GroupFillJob) * 2 * (size_t)nb) : slot(sizeof(FillJob) * 2 * (size_t)nb);
+    const size_t o_pref = slot(sizeof(int) * prefix.size());
+    const size_t o_svd = slot(sizeof(SvdJob) * nb);
+    const size_t o_idx = slot(sizeof(int) * nb);
+    const size_t o_pinv = slot(sizeof(PinvJob) * nb);
+    const size_t o_est = slot(sizeof(EstJob) * nb);
+    const size_t o_cpref = slot(sizeof(int) * (2 * (size_t)nb + nch));
+    const size_t o_cidx = slot(sizeof(int) * (nb + 1));
+    const size_t o_vw = slot(sizeof(VerifyWork) * nv);
+    const size_t o_vf = p.tri ? slot(sizeof(GroupFillJob) * (nvf + 1)) : slot(sizeof(FillJob) * (nvf + 1));
+    const size_t o_vp = slot(sizeof(int) * (nvf + nch));
+    const size_t o_ve = slot(sizeof(EstJob) * nv);
+    const size_t o_vi = slot(sizeof(int) * (nv + 1));
+    const size_t o_vg = slot(sizeof(const int *) * (nvf + 1));
+    PSKEL_TRY(c->plan_host.reserve(t + 256));
+    char *h = c->plan_host.as<char>();
+    BlockWork *works = reinterpret_cast<BlockWork *>(h + o_works);
+    FillJob *fills = reinterpret_cast<FillJob *>(h + o_fill);
+    GroupFillJob *gfills = reinterpret_cast<GroupFillJob *>(h + o_fill);
+    SvdJob *svds = reinterpret_cast<SvdJob *>(h + o_svd);
+    PinvJob *pinvs = reinterpret_cast<PinvJob *>(h + o_pinv);
+    EstJob *ests = reinterpret_cast<EstJob *>(h + o_est);
+    std::memcpy(h + o_pref, prefix.data(), sizeof(int) * prefix.size());
+    // ---- second pass: every block's storage pointers and jobs
     char *kb = ar.keep.as<char>();
     char *sb = ar.work.as<char>();
+    const int *tri_ids = c->d_gtri.as<int>(), *tri_adj = c->d_gadj.as<int>();
     size_t soff = 0;
-    int max_pinv_tiles = 0;
     for (int i = 0; i < nb; ++i) {
         const int b = p.blocks[i];
-        BlockWork &w = works[i];
+        BlockWork w{};
         BlockResult &res = c->results[b];
         w.rows_g = c->d_gids.as<int>() + c->gptr[c->gt[b]];
         w.cols_g = c->d_gids.as<int>() + c->gptr[c->gs[b]];
-        w.m = c->gptr[c->gt[b] + 1] - c->gptr[c->gt[b]];
-        w.n = c->gptr[c->gs[b] + 1] - c->gptr[c->gs[b]];
+        w.m = rows_of(c->gt[b]);
+        w.n = rows_of(c->gs[b]);
         w.r = p.r[i];
         w.pe = p.pe[i];
         w.pc = p.pc[i];
@@ -677,20 +765,21 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         soff += al16(r * r * sizeof(double2));
         w.T = reinterpret_cast<double2 *>(sb + soff);
         soff += al16((pe + pc) * r * sizeof(double2));
-        fills.push_back(FillJob{w.rows_g, w.Jg, w.C, w.m, w.r + w.pc, w.m, 0});
-        // Rx = Z([I; Ix], group_s) filled as the transpose of Z(group_s, [I; Ix]) (the Galerkin
-        // block is symmetric for equal test and source rules), so the long side is on rows
-        fills.push_back(FillJob{w.cols_g, w.Ig, w.Rx, w.n, w.r + w.pe, w.r + w.pe, 1});
-        if (tri_for(c, o.precision)) {
+        works[i] = w;
+        // C = Z(group_t, [J; Jx]); Rx = Z([I; Ix], group_s) filled as the transpose of
+        // Z(group_s, [I; Ix]) (the Galerkin block is symmetric for equal test and source rules),
+        // so the long side is on rows
+        if (p.tri) {
             const int gt = c->gt[b], gs = c->gs[b];
-            const int *tri = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
-            const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
-            gfills.push_back(GroupFillJob{w.rows_g, tri + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                          w.Jg, w.C, w.m, ntt, w.r + w.pc, w.m, 0, tri_cols_for(c, ntt),
-                                          guse_of(c, gt)});
-            gfills.push_back(GroupFillJob{w.cols_g, tri + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                          w.Ig, w.Rx, w.n, nts, w.r + w.pe, w.r + w.pe, 1, tri_cols_for(c, nts),
-                                          guse_of(c, gs)});
+            gfills[2 * i] = GroupFillJob{w.rows_g, tri_ids + c->gtri_ptr[gt], tri_adj + 3 * (size_t)c->gtri_ptr[gt],
+                                         w.Jg, w.C, w.m, tris_of(gt), w.r + w.pc, w.m, 0,
+                                         gtc[gt], guse_of(c, gt)};
+            gfills[2 * i + 1] = GroupFillJob{w.cols_g, tri_ids + c->gtri_ptr[gs], tri_adj + 3 * (size_t)c->gtri_ptr[gs],
+                                             w.Ig, w.Rx, w.n, tris_of(gs), w.r + w.pe, w.r + w.pe, 1,
+                                             gtc[gs], guse_of(c, gs)};
+        } else {
+            fills[2 * i] = FillJob{w.rows_g, w.Jg, w.C, w.m, w.r + w.pc, w.m, 0};
+            fills[2 * i + 1] = FillJob{w.cols_g, w.Ig, w.Rx, w.n, w.r + w.pe, w.r + w.pe, 1};
         }
         svds[i] = SvdJob{w.AV, w.V, w.sigma, w.perm, w.r, w.r, 0, 0};
         // a block sampled on every row or every column of its smaller side cannot gain from more
@@ -705,7 +794,6 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         pinvs[i] = PinvJob{w.AV, w.V, w.sigma, w.U, w.rank, w.r, w.r, tau_i, rel_i};
         ests[i] = EstJob{w.C, w.Rx, w.U, (const char *)w.Rx + r * es, (const char *)w.C + m * r * es,
                          w.Ix, w.Jx, w.m, w.n, w.r, w.r + w.pe, w.r + w.pe, w.pe, w.pc, w.T, w.est};
-        max_pinv_tiles = std::max(max_pinv_tiles, ((w.r + 31) / 32) * ((w.r + 31) / 32));
         res.m = w.m;
         res.n = w.n;
         res.r = w.r;
@@ -723,80 +811,51 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         res.offSig = (char *)w.sigma - kb;
         res.offPerm = (char *)w.perm - kb;
     }
-    // fill tile prefix
-    int tm, tn;
-    fill_tile_shape(o.precision, c->em.q_test, entry_split_for(c, o.precision), &tm, &tn);
-    p.tri = tri_for(c, o.precision);
-    std::vector<int> prefix(fills.size() + 1, 0);
-    if (p.tri) {
-        p.tri_rows = 0;
-        for (size_t i = 0; i < gfills.size(); ++i) {
-            prefix[i + 1] = prefix[i] + (gfills[i].nc + gfills[i].tc - 1) / gfills[i].tc;
-            p.tri_rows = std::max(p.tri_rows, gfills[i].m);
-        }
-    } else {
-        for (size_t i = 0; i < fills.size(); ++i)
-            prefix[i + 1] = prefix[i] + ((fills[i].nr + tm - 1) / tm) * ((fills[i].nc + tn - 1) / tn);
-    }
-    PSKEL_TRY(svd_plan(svds, p.svd));
-    const std::vector<int> &svd_idx = p.svd.idx;
-    // pipeline chunks, each with its own tables, of decreasing fill work: chunk k ends at the
-    // fraction 1 - (1 - k/K)^2 of the tiles, so the early chunks' pinv and estimate run beside
-    // the many later fills and the last chunk, whose pinv and estimate run alone, is small
-    const int K = (nb >= kPipeMinBlocks && c->pipe_chunks > 1) ? std::min(c->pipe_chunks, pskel_ctx::kMaxChunks) : 1;
-    p.cb.assign(1, 0);
-    {
-        const long long total = prefix.back();
-        int b = 0;
-        for (int k = 1; k < K; ++k) {
-            const double left = 1.0 - (double)k / K;
-            const long long want = (long long)((1.0 - left * left) * (double)total);
-            while (b < nb && prefix[2 * (size_t)b] < want) ++b;
-            if (b > p.cb.back()) p.cb.push_back(b);
-        }
-        p.cb.push_back(nb);
-    }
-    const int nch = (int)p.cb.size() - 1;
-    std::vector<int> ch_prefix_all, ch_idx_all;
+    // SVD plans of the round and of each chunk (index maps into the round's SvdJob table)
+    PSKEL_TRY(svd_plan(svds, nb, p.svd));
+    std::memcpy(h + o_idx, p.svd.idx.data(), sizeof(int) * nb);
     std::vector<size_t> ch_pref_off(nch), ch_idx_off(nch);
     p.ch_svd.assign(nch, SvdPlan());
     p.ch_tiles.assign(nch, 0);
     p.ch_pinv_tiles.assign(nch, 0);
-    for (int k = 0; k < nch; ++k) {
-        const int b0 = p.cb[k], b1 = p.cb[k + 1];
-        ch_pref_off[k] = ch_prefix_all.size();
-        for (int j = 2 * b0; j <= 2 * b1; ++j) ch_prefix_all.push_back(prefix[j] - prefix[2 * b0]);
-        p.ch_tiles[k] = prefix[2 * b1] - prefix[2 * b0];
-        std::vector<SvdJob> sub(svds.begin() + b0, svds.begin() + b1);
-        PSKEL_TRY(svd_plan(sub, p.ch_svd[k]));
-        for (int &x : p.ch_svd[k].idx) x += b0;  // into the round's SvdJob table
-        ch_idx_off[k] = ch_idx_all.size();
-        ch_idx_all.insert(ch_idx_all.end(), p.ch_svd[k].idx.begin(), p.ch_svd[k].idx.end());
-        for (int i = b0; i < b1; ++i)
-            p.ch_pinv_tiles[k] = std::max(p.ch_pinv_tiles[k], ((p.r[i] + 31) / 32) * ((p.r[i] + 31) / 32));
-    }
-    // re-check tables of every candidate; the gates and outputs live in the outcome buffer
-    std::vector<VerifyWork> vws(nv);
-    std::vector<EstJob> vests(nv);
-    std::vector<FillJob> vfills;
-    std::vector<GroupFillJob> vgfills;
-    std::vector<const int *> vjgate;  // each re-check fill job's gate
-    std::vector<int> vjob0(nv + 1, 0);  // each candidate's first fill job
     {
+        int *cpref = reinterpret_cast<int *>(h + o_cpref);
+        int *cidx = reinterpret_cast<int *>(h + o_cidx);
+        size_t np = 0, ni = 0;
+        for (int k = 0; k < nch; ++k) {
+            const int b0 = p.cb[k], b1 = p.cb[k + 1];
+            ch_pref_off[k] = np;
+            for (int j = 2 * b0; j <= 2 * b1; ++j) cpref[np++] = prefix[j] - prefix[2 * b0];
+            p.ch_tiles[k] = prefix[2 * b1] - prefix[2 * b0];
+            PSKEL_TRY(svd_plan(svds + b0, b1 - b0, p.ch_svd[k]));
+            for (int &x : p.ch_svd[k].idx) x += b0;  // into the round's SvdJob table
+            ch_idx_off[k] = ni;
+            for (int x : p.ch_svd[k].idx) cidx[ni++] = x;
+            for (int i = b0; i < b1; ++i)
+                p.ch_pinv_tiles[k] = std::max(p.ch_pinv_tiles[k], ((p.r[i] + 31) / 32) * ((p.r[i] + 31) / 32));
+        }
+    }
+    // ---- re-check tables of every candidate; the gates and outputs live in the outcome buffer
+    {
+        VerifyWork *vws = reinterpret_cast<VerifyWork *>(h + o_vw);
+        EstJob *vests = reinterpret_cast<EstJob *>(h + o_ve);
+        FillJob *vfills = reinterpret_cast<FillJob *>(h + o_vf);
+        GroupFillJob *vgfills = reinterpret_cast<GroupFillJob *>(h + o_vf);
+        const int **vjgate = reinterpret_cast<const int **>(h + o_vg);
+        std::memcpy(h + o_vi, p.vcand.data(), sizeof(int) * nv);
         char *vb = sb + scratch_total;
         char *ob = ar.outs.as<char>();
         double *vouts = reinterpret_cast<double *>(ob + outs_vouts_offset(nb));
         int *gates = reinterpret_cast<int *>(ob + outs_gates_offset(nb, nv));
         p.d_gates = gates;
-        p.vrmax = p.vpemax = p.vpcmax = p.vtri_rows = 0;
+        int f = 0;  // next re-check fill job
         for (int v = 0; v < nv; ++v) {
             const int i = p.vcand[v];
             const BlockWork &w = works[i];
             const int b = w.block_id, pe2 = vpe2[v], pc2 = vpc2[v];
-            vjob0[v] = (int)vjgate.size();
             char *q = vb + voff[v];
             auto take = [&](size_t bytes) { char *x = q; q += al16(bytes); return x; };
-            VerifyWork &x = vws[v];
+            VerifyWork x{};
             x.rows_g = w.rows_g;
             x.cols_g = w.cols_g;
             x.I = w.I;
@@ -820,112 +879,50 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
             x.Ig2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
             x.Jg2 = reinterpret_cast<int *>(take(sizeof(int) * (kMaxExtra + 1)));
             double2 *T = reinterpret_cast<double2 *>(take(sizeof(double2) * (size_t)(pe2 + pc2) * w.r));
+            vws[v] = x;
             vests[v] = EstJob{w.C, w.Rx, w.U, Xr, Xc, x.Ix2, x.Jx2, w.m, w.n, w.r, w.r + w.pe,
                               std::max(pe2, 1), pe2, pc2, T, vouts + 8 * (size_t)v, gates + v};
-            p.vrmax = std::max(p.vrmax, w.r);
-            p.vpemax = std::max(p.vpemax, pe2);
-            p.vpcmax = std::max(p.vpcmax, pc2);
             const int gt = c->gt[b], gs = c->gs[b];
-            if (p.tri) {
-                const int *tr = c->d_gtri.as<int>(), *adj = c->d_gadj.as<int>();
-                const int ntt = c->gtri_ptr[gt + 1] - c->gtri_ptr[gt], nts = c->gtri_ptr[gs + 1] - c->gtri_ptr[gs];
-                if (pc2 > 0) {
-                    vgfills.push_back(GroupFillJob{w.rows_g, tr + c->gtri_ptr[gt], adj + 3 * (size_t)c->gtri_ptr[gt],
-                                                   x.Jg2, Xc, w.m, ntt, pc2, w.m, 0, tri_cols_for(c, ntt),
-                                                   guse_of(c, gt)});
-                    vjgate.push_back(gates + v);
-                    p.vtri_rows = std::max(p.vtri_rows, w.m);
-                }
-                if (pe2 > 0) {
-                    vgfills.push_back(GroupFillJob{w.cols_g, tr + c->gtri_ptr[gs], adj + 3 * (size_t)c->gtri_ptr[gs],
-                                                   x.Ig2, Xr, w.n, nts, pe2, pe2, 1, tri_cols_for(c, nts),
-                                                   guse_of(c, gs)});
-                    vjgate.push_back(gates + v);
-                    p.vtri_rows = std::max(p.vtri_rows, w.n);
-                }
-            } else {
-                if (pc2 > 0) {
-                    vfills.push_back(FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2, w.m, 0});
-                    vjgate.push_back(gates + v);
-                }
-                if (pe2 > 0) {
-                    vfills.push_back(FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2, pe2, 1});
-                    vjgate.push_back(gates + v);
-                }
+            if (pc2 > 0) {
+                if (p.tri)
+                    vgfills[f] = GroupFillJob{w.rows_g, tri_ids + c->gtri_ptr[gt], tri_adj + 3 * (size_t)c->gtri_ptr[gt],
+                                              x.Jg2, Xc, w.m, tris_of(gt), pc2, w.m, 0,
+                                              gtc[gt], guse_of(c, gt)};
+                else
+                    vfills[f] = FillJob{w.rows_g, x.Jg2, Xc, w.m, pc2, w.m, 0};
+                vjgate[f++] = gates + v;
+            }
+            if (pe2 > 0) {
+                if (p.tri)
+                    vgfills[f] = GroupFillJob{w.cols_g, tri_ids + c->gtri_ptr[gs], tri_adj + 3 * (size_t)c->gtri_ptr[gs],
+                                              x.Ig2, Xr, w.n, tris_of(gs), pe2, pe2, 1,
+                                              gtc[gs], guse_of(c, gs)};
+                else
+                    vfills[f] = FillJob{w.cols_g, x.Ig2, Xr, w.n, pe2, pe2, 1};
+                vjgate[f++] = gates + v;
             }
         }
     }
-    const size_t nvf = p.tri ? vgfills.size() : vfills.size();
-    std::vector<int> vprefix(nvf + 1, 0);
-    for (size_t f = 0; f < nvf; ++f)
-        vprefix[f + 1] = vprefix[f] + (p.tri ? (vgfills[f].nc + vgfills[f].tc - 1) / vgfills[f].tc
-                                             : ((vfills[f].nr + tm - 1) / tm) * ((vfills[f].nc + tn - 1) / tn));
-    // the re-checks by pipeline chunk (candidates are in round order, so each chunk's candidates
-    // and their fill jobs are contiguous)
-    vjob0[nv] = (int)nvf;
-    const int nchv = (int)p.cb.size() - 1;
-    p.vc.assign(nchv + 1, nv);
-    p.vj.assign(nchv + 1, (int)nvf);
-    p.vch_tiles.assign(nchv, 0);
-    std::vector<int> vch_prefix_all;
-    std::vector<size_t> vch_off(nchv);
-    for (int k = 0; k < nchv; ++k) {
-        p.vc[k] = (int)(std::lower_bound(p.vcand.begin(), p.vcand.end(), p.cb[k]) - p.vcand.begin());
-        p.vj[k] = vjob0[p.vc[k]];
+    std::vector<size_t> vch_off(nch);
+    {
+        int *vp = reinterpret_cast<int *>(h + o_vp);
+        size_t np = 0;
+        for (int k = 0; k < nch; ++k) {
+            vch_off[k] = np;
+            for (int j = p.vj[k]; j <= p.vj[k + 1]; ++j) vp[np++] = vprefix[j] - vprefix[p.vj[k]];
+            p.vch_tiles[k] = vprefix[p.vj[k + 1]] - vprefix[p.vj[k]];
+        }
     }
-    for (int k = 0; k < nchv; ++k) {
-        vch_off[k] = vch_prefix_all.size();
-        for (int j = p.vj[k]; j <= p.vj[k + 1]; ++j) vch_prefix_all.push_back(vprefix[j] - vprefix[p.vj[k]]);
-        p.vch_tiles[k] = vprefix[p.vj[k + 1]] - vprefix[p.vj[k]];
-    }
-    // pack tables
-    size_t t = 0;
-    auto slot = [&](size_t bytes) { size_t x = t; t += (bytes + 255) & ~size_t(255); return x; };
-    const size_t o_works = slot(sizeof(BlockWork) * nb);
-    const size_t o_fill = p.tri ? slot(sizeof(GroupFillJob) * gfills.size())
-                                : slot(sizeof(FillJob) * fills.size());
-    const size_t o_pref = slot(sizeof(int) * prefix.size());
-    const size_t o_svd = slot(sizeof(SvdJob) * nb);
-    const size_t o_idx = slot(sizeof(int) * nb);
-    const size_t o_pinv = slot(sizeof(PinvJob) * nb);
-    const size_t o_est = slot(sizeof(EstJob) * nb);
-    const size_t o_cpref = slot(sizeof(int) * ch_prefix_all.size());
-    const size_t o_cidx = slot(sizeof(int) * (ch_idx_all.size() + 1));
-    const size_t o_vw = slot(sizeof(VerifyWork) * nv);
-    const size_t o_vf = p.tri ? slot(sizeof(GroupFillJob) * (nvf + 1)) : slot(sizeof(FillJob) * (nvf + 1));
-    const size_t o_vp = slot(sizeof(int) * vch_prefix_all.size());
-    const size_t o_ve = slot(sizeof(EstJob) * nv);
-    const size_t o_vi = slot(sizeof(int) * (nv + 1));
-    const size_t o_vg = slot(sizeof(const int *) * (nvf + 1));
-    ar.h_tables.assign(t, 0);
-    std::memcpy(ar.h_tables.data() + o_works, works.data(), sizeof(BlockWork) * nb);
-    if (p.tri)
-        std::memcpy(ar.h_tables.data() + o_fill, gfills.data(), sizeof(GroupFillJob) * gfills.size());
-    else
-        std::memcpy(ar.h_tables.data() + o_fill, fills.data(), sizeof(FillJob) * fills.size());
-    std::memcpy(ar.h_tables.data() + o_pref, prefix.data(), sizeof(int) * prefix.size());
-    std::memcpy(ar.h_tables.data() + o_svd, svds.data(), sizeof(SvdJob) * nb);
-    std::memcpy(ar.h_tables.data() + o_idx, svd_idx.data(), sizeof(int) * nb);
-    std::memcpy(ar.h_tables.data() + o_pinv, pinvs.data(), sizeof(PinvJob) * nb);
-    std::memcpy(ar.h_tables.data() + o_est, ests.data(), sizeof(EstJob) * nb);
-    std::memcpy(ar.h_tables.data() + o_cpref, ch_prefix_all.data(), sizeof(int) * ch_prefix_all.size());
-    std::memcpy(ar.h_tables.data() + o_cidx, ch_idx_all.data(), sizeof(int) * ch_idx_all.size());
-    std::memcpy(ar.h_tables.data() + o_vw, vws.data(), sizeof(VerifyWork) * nv);
-    if (p.tri) std::memcpy(ar.h_tables.data() + o_vf, vgfills.data(), sizeof(GroupFillJob) * nvf);
-    else std::memcpy(ar.h_tables.data() + o_vf, vfills.data(), sizeof(FillJob) * nvf);
-    std::memcpy(ar.h_tables.data() + o_vp, vch_prefix_all.data(), sizeof(int) * vch_prefix_all.size());
-    std::memcpy(ar.h_tables.data() + o_ve, vests.data(), sizeof(EstJob) * nv);
-    std::memcpy(ar.h_tables.data() + o_vi, p.vcand.data(), sizeof(int) * nv);
-    std::memcpy(ar.h_tables.data() + o_vg, vjgate.data(), sizeof(const int *) * nvf);
+    // ---- one asynchronous upload from the staging buffer (the previous round's upload from it
+    // completed before that round's outcome was read)
     PSKEL_TRY(ar.tables.reserve(t + 256));
-    PSKEL_CUDA(cudaMemcpyAsync(ar.tables.ptr, ar.h_tables.data(), t, cudaMemcpyHostToDevice,
-                               c->stream));
+    PSKEL_CUDA(cudaMemcpyAsync(ar.tables.ptr, h, t, cudaMemcpyHostToDevice, c->stream));
     char *d = ar.tables.as<char>();
     p.d_works = reinterpret_cast<BlockWork *>(d + o_works);
     p.d_fill = reinterpret_cast<FillJob *>(d + o_fill);
     p.d_gfill = reinterpret_cast<GroupFillJob *>(d + o_fill);
     p.d_fill_prefix = reinterpret_cast<int *>(d + o_pref);
-    p.fill_jobs = (int)fills.size();
+    p.fill_jobs = 2 * nb;
     p.fill_tiles = prefix.back();
     p.d_svd = reinterpret_cast<SvdJob *>(d + o_svd);
     p.d_svd_idx = reinterpret_cast<int *>(d + o_idx);
@@ -934,11 +931,11 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     p.d_vworks = reinterpret_cast<VerifyWork *>(d + o_vw);
     p.d_vfill = reinterpret_cast<FillJob *>(d + o_vf);
     p.d_vgfill = reinterpret_cast<GroupFillJob *>(d + o_vf);
-    p.vch_prefix.assign(nchv, nullptr);
-    for (int k = 0; k < nchv; ++k) p.vch_prefix[k] = reinterpret_cast<int *>(d + o_vp) + vch_off[k];
     p.d_vest = reinterpret_cast<EstJob *>(d + o_ve);
     p.d_vidx = reinterpret_cast<int *>(d + o_vi);
     p.d_vjgate = reinterpret_cast<const int *const *>(d + o_vg);
+    p.vch_prefix.assign(nch, nullptr);
+    for (int k = 0; k < nch; ++k) p.vch_prefix[k] = reinterpret_cast<int *>(d + o_vp) + vch_off[k];
     p.ch_prefix.assign(nch, nullptr);
     p.ch_idx.assign(nch, nullptr);
     for (int k = 0; k < nch; ++k) {
@@ -1132,7 +1129,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec1.f64.release();
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
-    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->recomp64b.release(); c->rc_work.release(); c->rc_tab.release(); c->rc_idx.release(); c->rc_host.release(); c->mv_table.release();
+    c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->recomp64b.release(); c->rc_work.release(); c->rc_tab.release(); c->rc_idx.release(); c->rc_host.release(); c->plan_host.release(); c->mv_table.release();
     for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     svd_streams_destroy(c->svd_par);

@@ -68,7 +68,6 @@ struct RoundArena {
                      // rounds grow their own)
     DevBuf tables;   // device copies of the job tables
     DevBuf outs;     // RoundOut per block of the round, then its re-checks' sums and gates
-    std::vector<char> h_tables;
 };
 
 struct RecompSlot {
@@ -152,6 +151,7 @@ struct pskel_ctx {
     DevBuf recomp64, recomp64b;             // FP64 path: recompressed factors and workspace
     DevBuf rc_work, rc_tab, rc_idx;         // split path: workspace, job tables, SVD order
     pskel::PinnedBuf rc_host;               // split path: host copy of the job tables
+    pskel::PinnedBuf plan_host;             // a compression round's job tables, staged for upload
     std::vector<pskel::SvdJob> rc_hs;       // split path: host SVD jobs (kept: no per-call allocation)
     int recomp_path = 0;                    // 0 auto, 1 FP64 only, 2 split whenever eligible
     int recomp_split_blocks = 0;            // blocks of the last recompression on the split path

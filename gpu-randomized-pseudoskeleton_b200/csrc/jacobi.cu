@@ -568,7 +568,10 @@ static int resident_threads_for(int n) {
 }
 
 int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
-    const int nj = (int)h_jobs.size();
+    return svd_plan(h_jobs.data(), (int)h_jobs.size(), plan);
+}
+
+int svd_plan(const SvdJob *h_jobs, int nj, SvdPlan &plan) {
     plan.idx.clear();
     plan.idx.reserve(nj);
     plan.res.clear();

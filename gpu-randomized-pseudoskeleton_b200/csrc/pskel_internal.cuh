@@ -258,6 +258,7 @@ struct SvdPlan {
     int blk_off = 0, blk_count = 0;
 };
 int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan);
+int svd_plan(const SvdJob *h_jobs, int nj, SvdPlan &plan);
 // Side streams for the size-class launches of one SVD plan: the classes are independent, so
 // they run concurrently (fork on `fork`, join through `join`); graph capture follows the events.
 constexpr int kSvdAux = 4;
