@@ -865,19 +865,28 @@ def fill_case(prec, calls, split, geom32, tri_cols=8):
                   f"max {t['sweeps_max']:.0f}", flush=True)
 
 
-def store_case(calls):
-    """Compress the same sphere at tol 1e-4 (c64), recompress to 1e-4, build the compressed
-    store and run CALLS tensor-core matvecs with 16 right-hand sides."""
+def store_case(calls, subdiv=4):
+    """Compress the sphere (SUBDIV 4: 7,680 RWG, every block compressed; 5: the bench workload,
+    30,720 RWG, symmetric mode with the learned first sample counts) at tol 1e-4 (c64),
+    recompress to 1e-4, build the compressed store and run CALLS tensor-core matvecs with 16
+    right-hand sides. Under a profiler each matvec is build_b1_kernel, store_gemm_kernel (phase
+    1), build_b2_kernel, store_gemm_kernel (phase 2) after two memsets."""
     import torch
     from pskel import mesh as pmesh
     from pskel import octree
     from pskel.engine import Engine
-    m = pmesh.icosphere(2.0, 4)
-    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30)
+    from pskel.predictor import Predictor
+    m = pmesh.icosphere(2.0, subdiv)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30 if subdiv <= 4 else 40)
     with Engine() as eng:
         eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
         eng.set_blocks(part)
-        eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        if subdiv <= 4:
+            eng.compress(1e-4, precision="c64", tau=1e-7, seed=0)
+        else:
+            eng.set_symmetric(True)
+            r0 = Predictor.load().sample_counts(part, 2 * np.pi, 1e-4)
+            eng.compress(1e-4, precision="c64", tau=1e-7, r0=r0, oversample=0, seed=0)
         eng.recompress(1e-4)
         nbytes = eng.build_store()
         X = torch.randn((m.N, 16), dtype=torch.complex64, device="cuda")
@@ -1002,13 +1011,13 @@ def main():
     ap.add_argument("--tri-cols", type=int, default=8,
                     help="profiling case fill: columns per triangle-moment tile (0: balanced per job)")
     ap.add_argument("--subdiv", type=int, default=4,
-                    help="profiling case recompress: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
+                    help="profiling cases recompress and store: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
     args = ap.parse_args()
     if args.profile_case:
         if args.profile_case == "fill":
             fill_case(args.precision, args.calls, args.split, args.geom32, args.tri_cols)
         elif args.profile_case == "store":
-            store_case(args.calls)
+            store_case(args.calls, args.subdiv)
         elif args.profile_case == "recompress":
             recompress_case(args.calls, args.subdiv)
         else:

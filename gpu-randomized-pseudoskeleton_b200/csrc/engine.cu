@@ -1130,7 +1130,7 @@ extern "C" int pskel_destroy(pskel_ctx *c) {
     c->mesh.rec7.f64.release();
     c->flags.release(); c->d_gids.release();
     c->tmp.release(); c->tmp2.release(); c->tmp3.release(); c->recomp.release(); c->recomp64.release(); c->recomp64b.release(); c->rc_work.release(); c->rc_tab.release(); c->rc_idx.release(); c->rc_host.release(); c->plan_host.release(); c->mv_table.release();
-    for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_map, &c->st_tiles, &c->st_err}) d->release();
+    for (DevBuf *d : {&c->st_ah, &c->st_al, &c->st_bh, &c->st_bl, &c->st_t, &c->st_tab, &c->st_tiles, &c->st_err}) d->release();
     for (auto &a : c->arenas) { a.keep.release(); a.work.release(); a.tables.release(); a.outs.release(); }
     svd_streams_destroy(c->svd_par);
     octree_release(c->octree);

@@ -82,23 +82,24 @@ struct RecompSlot {
 // Compressed store of the recompressed blocks (csrc/store.cu): host copy of its layout.
 struct StoreTile {
     long long a_off, b_off;  // A and B offsets (bf16 elements) within the phase's region
-    int kc, rows, out0;      // K chunks, valid rows, first T row (phase 1) or first group row
+    int kc, rows, out0;      // K chunks, valid rows, first T row (phase 1) or first row of the
+                             // test group's 2m-row stack (phase 2)
     int phase;
+    int ids0 = 0, m = 0;     // phase 2: the test group's first id and its rows
 };
 struct StoreGroup {
     long long b_base;  // B offset within the phase's region
     int kc, K;         // chunks, real K
-    int ids0;          // phase 1: offset of the group's ids in the group id list
-    int map0;          // phase 2: offset of the group's T-row map
+    int ids0;          // offset of the group's ids in the group id list
 };
 struct StoreLayout {
     std::vector<StoreTile> tiles1, tiles2;
-    std::vector<StoreGroup> groups1, groups2;
-    std::vector<int> trow_map;
+    std::vector<StoreGroup> groups1;  // source groups (phase-1 B operands, built per matvec)
     long long a1 = 0, a2 = 0, b1 = 0, b2 = 0;
     int trows = 0;
     int n_items1 = 0, n_items2 = 0;  // GEMM work items per phase
-    void *d_t1 = nullptr, *d_t2 = nullptr, *d_g1 = nullptr, *d_g2 = nullptr;
+    int n_bitems1 = 0;  // phase-1 B-builder work items (8-chunk blocks)
+    void *d_t1 = nullptr, *d_t2 = nullptr, *d_g1 = nullptr, *d_bi1 = nullptr;
     bool ready = false;
     long long generation = -1;
     int mode = PSKEL_STORE_BF16X3;  // operand format of the planes
@@ -162,7 +163,7 @@ struct pskel_ctx {
     int mv_max_r = 0, mv_max_m = 0, mv_max_n = 0, mv_chunks = 0;  // largest rank / groups, chunks
     size_t mv_chunk_off = 0;                        // byte offset of the chunk table in mv_table
     StoreLayout store;                      // compressed store (bf16 hi/lo planes, tiled)
-    DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_map, st_tiles, st_err;
+    DevBuf st_ah, st_al, st_bh, st_bl, st_t, st_tab, st_tiles, st_err;  // st_t: phase-1 row places
     pskel::OctreeState octree;              // device octree partition (pskel_octree_build)
     DevBuf near_jobs, near_mom;             // near-field fill: job table, same-triangle moments
     DevBuf near_data, near_tab;             // near blocks (dense complex FP64) and their table

@@ -9,8 +9,13 @@
 // 1929-1960, for all blocks and 16 vectors, on the recompressed form of
 // codes/ACA_vs_CUR/seed/svd_compress.m:19-33).
 //
-// Complex products run as real GEMMs: A' = [Re A | Im A] (K doubled) times
-// B' = [[Re X, Im X]; [-Im X, Re X]] gives [Re(AX) | Im(AX)] (N = 2 x 16 = 32).
+// Complex products run as real GEMMs. Phase 1: A' = [Re A | Im A] (K doubled) times
+// B' = [[Re X, Im X]; [-Im X, Re X]] gives [Re(AX) | Im(AX)] (N = 2 x 16 = 32). Phase 2: the
+// rows are doubled instead, A' = [Re C' ; Im C'] times B' = [Re T | Im T], and each output row
+// combines its two rows (Re Y = Re C' Re T - Im C' Im T, Im Y = Re C' Im T + Im C' Re T) in the
+// FP32 atomics that write Y: a test group of m rows pads 2m rows to the 128-row tile (154 -> 256
+// instead of 154 -> 128 x 2 on a doubled K), and B' is half the size. The phase-1 epilogue
+// writes its rows straight into B' (no separate T and no builder kernel).
 // Operand formats (pskel_store_build_mode), all accumulated in FP32 in TMEM:
 //   BF16X3 (default): every real operand split into bf16 hi + lo (hi = bf16(x), lo = bf16(x -
 //            hi)), hi*hi + hi*lo + lo*hi with tcgen05.mma kind::f16 (relative error ~1e-5);
@@ -103,8 +108,8 @@ struct PackBlock {
     int trans, ldcp;    // trans: mirror block, Cp and Rp are its primary's (C' = R'_p^T, R' = C'_p^T)
     long long a1_base;  // phase-1 group base (elements) and the block's first row in it
     int a1_kc, a1_row0;
-    long long a2_base;  // phase-2 group base and the block's first K column (real part)
-    int a2_kc, a2_col0, a2_K;  // a2_K: real K of the test group (imag parts start there)
+    long long a2_base;  // phase-2 group base and the block's first K column
+    int a2_kc, a2_col0, a2_m;  // a2_m: rows of the test group (imaginary parts start there)
 };
 
 template <int MODE>
@@ -132,7 +137,7 @@ __global__ void __launch_bounds__(256) pack_kernel(const PackBlock *__restrict__
         const int i = e % w.m, j = e / w.m;
         const double2 v = w.trans ? w.Rp[j + (size_t)i * w.r] : w.Cp[i + (size_t)j * w.ldcp];
         const long long o_re = st_a_off<EPC>(w.a2_base, w.a2_kc, i, w.a2_col0 + j);
-        const long long o_im = st_a_off<EPC>(w.a2_base, w.a2_kc, i, w.a2_K + w.a2_col0 + j);
+        const long long o_im = st_a_off<EPC>(w.a2_base, w.a2_kc, w.a2_m + i, w.a2_col0 + j);
         st_split((float)v.x, A2h + o_re, two ? A2l + o_re : nullptr);
         st_split((float)v.y, A2h + o_im, two ? A2l + o_im : nullptr);
     }
@@ -146,73 +151,77 @@ struct StGroupB {
     const int *src;    // phase 1: RWG ids of the group; phase 2: T row of each real K index
 };
 
-// phase 1: B'(k, c) from X (complex64, column-major, ldx), columns >= nrhs are zero. One thread
-// per K index writes its 32 columns: eight consecutive K indices fill one 16-byte chunk row.
+// One work item of a B-operand builder: 8 chunks (8 x EPC consecutive K values) of a group.
+struct StBItem {
+    int g;   // group (index into the phase's StGroupB table)
+    int kb;  // 8-chunk block within the group's K
+};
+
+// the hi (and lo) plane values of v in a thread's chunk slot e
 template <int MODE>
-__global__ void __launch_bounds__(256) build_b1_kernel(const StGroupB *__restrict__ groups,
-                                                       const float2 *__restrict__ X, int ldx,
-                                                       int nrhs, typename StFmt<MODE>::E *Bh,
-                                                       typename StFmt<MODE>::E *Bl) {
-    constexpr int EPC = StFmt<MODE>::kEpc;
-    const bool two = StFmt<MODE>::kPlanes == 2;
-    const StGroupB g = groups[blockIdx.x];
-    const int kpad = g.kc * EPC;
-    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
-        const bool in = k < 2 * g.K;
-        const bool re_half = k < g.K;
-        const int id = in ? g.src[re_half ? k : k - g.K] : 0;
-#pragma unroll 4
-        for (int rhs = 0; rhs < kStRhs; ++rhs) {
-            float2 x = make_float2(0.f, 0.f);
-            if (in && rhs < nrhs) x = X[id + (size_t)rhs * ldx];
-            const float v0 = re_half ? x.x : -x.y;  // column rhs:      [re X; -im X]
-            const float v1 = re_half ? x.y : x.x;   // column 16 + rhs: [im X;  re X]
-            const long long o0 = st_b_off<EPC>(g.b_base, rhs, k);
-            const long long o1 = st_b_off<EPC>(g.b_base, rhs + kStRhs, k);
-            st_split(v0, Bh + o0, two ? Bl + o0 : nullptr);
-            st_split(v1, Bh + o1, two ? Bl + o1 : nullptr);
-        }
-    }
+__device__ __forceinline__ void st_split_at(float v, typename StFmt<MODE>::E (&hi)[StFmt<MODE>::kEpc],
+                                            typename StFmt<MODE>::E (&lo)[StFmt<MODE>::kEpc], int e) {
+    st_split(v, &hi[e], StFmt<MODE>::kPlanes == 2 ? &lo[e] : nullptr);
 }
 
-// phase 2: B'(k, c) from the phase-1 rows T (32 floats per row: re of the 16 sides, then im);
-// one thread per K index reads its T row once
+// one 16-byte chunk of each plane at element offset o
 template <int MODE>
-__global__ void __launch_bounds__(256) build_b2_kernel(const StGroupB *__restrict__ groups,
-                                                       const float *__restrict__ T,
-                                                       typename StFmt<MODE>::E *Bh,
-                                                       typename StFmt<MODE>::E *Bl) {
-    constexpr int EPC = StFmt<MODE>::kEpc;
-    const bool two = StFmt<MODE>::kPlanes == 2;
-    const StGroupB g = groups[blockIdx.x];
-    const int kpad = g.kc * EPC;
-    for (int k = threadIdx.x; k < kpad; k += blockDim.x) {
-        const bool in = k < 2 * g.K;
-        const bool re_half = k < g.K;
-        float t[kStN];
-        if (in) {
-            const float4 *row = reinterpret_cast<const float4 *>(T + (size_t)g.src[re_half ? k : k - g.K] * kStN);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const float4 a = row[q];
-                t[4 * q] = a.x;
-                t[4 * q + 1] = a.y;
-                t[4 * q + 2] = a.z;
-                t[4 * q + 3] = a.w;
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < kStN; ++c) t[c] = 0.f;
-        }
-#pragma unroll
-        for (int c = 0; c < kStN; ++c) {
-            // [re T | im T] on the first K rows, [-im T | re T] on the second
-            const float v = re_half ? t[c] : (c < kStRhs ? -t[c + kStRhs] : t[c - kStRhs]);
-            const long long o = st_b_off<EPC>(g.b_base, c, k);
-            st_split(v, Bh + o, two ? Bl + o : nullptr);
-        }
-    }
+__device__ __forceinline__ void st_store_chunk(typename StFmt<MODE>::E *Bh, typename StFmt<MODE>::E *Bl,
+                                               long long o, const typename StFmt<MODE>::E (&hi)[StFmt<MODE>::kEpc],
+                                               const typename StFmt<MODE>::E (&lo)[StFmt<MODE>::kEpc]) {
+    *reinterpret_cast<uint4 *>(Bh + o) = *reinterpret_cast<const uint4 *>(hi);
+    if (StFmt<MODE>::kPlanes == 2) *reinterpret_cast<uint4 *>(Bl + o) = *reinterpret_cast<const uint4 *>(lo);
 }
+
+// phase 1: B'(k, c) from X (complex64, column-major, ldx), columns >= nrhs are zero. A CTA stages
+// the X rows of its 8 x EPC K values in shared memory; thread (q, c) then writes chunk q of column
+// c: EPC consecutive K values, 16 bytes per plane, each warp one contiguous 512-byte row. The
+// grid also clears Y (ny float2, the phase-2 atomics' target) and the error word.
+template <int MODE>
+__global__ void __launch_bounds__(256) build_b1_kernel(const StBItem *__restrict__ items,
+                                                       const StGroupB *__restrict__ groups,
+                                                       const float2 *__restrict__ X, int ldx,
+                                                       int nrhs, typename StFmt<MODE>::E *Bh,
+                                                       typename StFmt<MODE>::E *Bl, float2 *Y,
+                                                       long long ny, int *err) {
+    using E = typename StFmt<MODE>::E;
+    constexpr int EPC = StFmt<MODE>::kEpc, KB = 8 * EPC;
+    __shared__ float2 xs[KB][kStRhs + 1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ny; e += (long long)gridDim.x * blockDim.x)
+        Y[e] = make_float2(0.f, 0.f);
+    const StBItem it = items[blockIdx.x];
+    const StGroupB g = groups[it.g];
+    const int k0 = it.kb * KB;
+    for (int e = threadIdx.x; e < KB * kStRhs; e += blockDim.x) {
+        const int kk = e % KB, rhs = e / KB, k = k0 + kk;
+        float2 x = make_float2(0.f, 0.f);
+        if (k < 2 * g.K && rhs < nrhs) x = X[g.src[k < g.K ? k : k - g.K] + (size_t)rhs * ldx];
+        xs[kk][rhs] = x;
+    }
+    __syncthreads();
+    const int q = threadIdx.x >> 5, c = threadIdx.x & 31, rhs = c & (kStRhs - 1);
+    alignas(16) E hi[EPC];
+    alignas(16) E lo[EPC];
+#pragma unroll
+    for (int e = 0; e < EPC; ++e) {
+        const int kk = q * EPC + e;
+        const bool re_half = k0 + kk < g.K;
+        const float2 x = xs[kk][rhs];
+        // column rhs: [re X; -im X], column 16 + rhs: [im X; re X]
+        const float v = c < kStRhs ? (re_half ? x.x : -x.y) : (re_half ? x.y : x.x);
+        st_split_at<MODE>(v, hi, lo, e);
+    }
+    st_store_chunk<MODE>(Bh, Bl, st_b_off<EPC>(g.b_base, c, k0 + q * EPC), hi, lo);
+}
+
+// Place of a phase-1 output row (block b's i-th rank row of T_s) in the phase-2 B operand
+// [Re T | Im T] of its test group t = gt(b): row k, the row's position in the test group's
+// stack of ranks.
+struct StT2 {
+    long long b_base;  // the test group's B region (elements, phase-2 region included)
+    int k, pad;
+};
 
 // ---------------------------------------------------------------- tcgen05 grouped GEMM
 // One work item of the grouped GEMM: a 128-row output tile and a range of its K stages.
@@ -221,8 +230,9 @@ struct StItem {
     long long b_off;  // first B chunk of the item
     int nst;          // stages (64 K values each)
     int rows;         // valid rows of the tile
-    int out0;         // phase 1: first T row of the tile
-    const int *ids;   // phase 2: RWG ids of the tile's rows (null in phase 1)
+    int out0;         // phase 1: first T row of the tile; phase 2: first row of the 2m stack
+    const int *ids;   // phase 2: RWG ids of the test group (null in phase 1)
+    int m;            // phase 2: rows of the test group (stack rows m + i: imaginary parts)
 };
 
 // instruction descriptors, FP32 D, both operands K-major, M = 128, N = 32:
@@ -242,8 +252,9 @@ __device__ __forceinline__ void umma_st(uint32_t tmem_d, uint64_t adesc, uint64_
 //   warp 0 lane 0   producer: bulk copies of the A and B planes into a 4-stage ring;
 //   warp 1 lane 0   MMA issuer: 3 x 4 tcgen05.mma per stage into one of two TMEM accumulators;
 //   warps 2-5       epilogue: tcgen05.ld of their TMEM lane quadrant, then the rows go out
-//                   (phase 1: stores into T; phase 2: FP32 atomics into Y, the items of a tile
-//                   being K slices of it).
+//                   (phase 1: each row T(b, i) straight into the phase-2 B operand, as its
+//                   format's planes, at rows k and K + k of its test group; phase 2: FP32
+//                   atomics into Y, the items of a tile being K slices of it).
 // The two accumulators let the epilogue of one item overlap the MMAs of the next.
 template <int MODE>
 __global__ void __launch_bounds__(192, 1)
@@ -252,7 +263,8 @@ __global__ void __launch_bounds__(192, 1)
                       const typename StFmt<MODE>::E *__restrict__ Al,
                       const typename StFmt<MODE>::E *__restrict__ Bh,
                       const typename StFmt<MODE>::E *__restrict__ Bl,
-                      float *T, float *Y, int ldy, int nrhs, int *err) {
+                      const StT2 *__restrict__ t2, typename StFmt<MODE>::E *B2h,
+                      typename StFmt<MODE>::E *B2l, float *Y, int ldy, int nrhs, int *err) {
     constexpr int EPC = StFmt<MODE>::kEpc;
     constexpr bool kTwo = StFmt<MODE>::kPlanes == 2;
     constexpr int kChunkA = kStTileM * EPC, kChunkB = kStN * EPC;  // elements per chunk block
@@ -390,19 +402,29 @@ __global__ void __launch_bounds__(192, 1)
             const int row = quad * 32 + lane;
             if (row < w.rows) {
                 if (!w.ids) {
-                    float4 *t = reinterpret_cast<float4 *>(T + (size_t)(w.out0 + row) * kStN);
+                    // T(b, i) = [re of the 16 sides | im] is row k of its test group's B'
+                    const StT2 d = t2[w.out0 + row];
 #pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        t[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                           __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+                    for (int c = 0; c < kStN; ++c) {
+                        typename StFmt<MODE>::E h, l;
+                        const long long o = st_b_off<EPC>(d.b_base, c, d.k);
+                        st_split(__uint_as_float(v[c]), &h, kTwo ? &l : nullptr);
+                        B2h[o] = h;
+                        if (kTwo) B2l[o] = l;
+                    }
                 } else {
-                    const int id = w.ids[row];
+                    // stack row rho: Re C'(i, :) [Re T | Im T] (rho = i) or Im C'(i, :) [Re T | Im T]
+                    // (rho = m + i)
+                    const int rho = w.out0 + row;
+                    const bool im = rho >= w.m;
+                    const int id = w.ids[im ? rho - w.m : rho];
 #pragma unroll
                     for (int c = 0; c < kStRhs; ++c)
                         if (c < nrhs) {
                             float *y = Y + 2 * ((size_t)id + (size_t)c * ldy);
-                            atomicAdd(y, __uint_as_float(v[c]));
-                            atomicAdd(y + 1, __uint_as_float(v[c + kStRhs]));
+                            const float a = __uint_as_float(v[c]), b = __uint_as_float(v[c + kStRhs]);
+                            atomicAdd(y, im ? -b : a);
+                            atomicAdd(y + 1, im ? a : b);
                         }
                 }
             }
@@ -479,12 +501,13 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
         for (int mt = 0; mt < mpad / kStTileM; ++mt)
             L.tiles1.push_back(StoreTile{a1 + (long long)mt * kc * chunkA, b1, kc,
                                          std::min(kStTileM, K - mt * kStTileM), trow + mt * kStTileM, -1});
-        L.groups1.push_back(StoreGroup{b1, kc, n, c->gptr[g], -1});
+        L.groups1.push_back(StoreGroup{b1, kc, n, c->gptr[g]});
         a1 += (long long)mpad * kc * epc;
         b1 += (long long)kc * chunkB;
         trow += mpad;
     }
-    // phase 2: per test group; the T row of every real K index
+    // phase 2: per test group; the place of every phase-1 output row in its B operand
+    std::vector<StT2> tplace(std::max(trow, 1), StT2{0, 0, 0});
     long long a2 = 0, b2 = 0;
     for (int g = 0; g < ng; ++g) {
         if (by_test[g].empty()) continue;
@@ -492,23 +515,22 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
         for (int b : by_test[g]) K += c->recomp_slots[b].k;
         if (K == 0) continue;
         const int m = gsize(g);
-        const int kc = (int)(pad(2 * (long long)K, stageK) / epc);
-        const int mpad = (int)pad(m, kStTileM);
-        const int map0 = (int)L.trow_map.size();
+        const int kc = (int)(pad((long long)K, stageK) / epc);
+        const int mpad = (int)pad(2 * (long long)m, kStTileM);  // Re C' rows, then Im C' rows
         int col = 0;
         for (int b : by_test[g]) {
             PackBlock &w = pb[b];
             w.a2_base = a2;
             w.a2_kc = kc;
             w.a2_col0 = col;
-            w.a2_K = K;
-            for (int i = 0; i < c->recomp_slots[b].k; ++i) L.trow_map.push_back(t_row0[b] + i);
+            w.a2_m = m;
+            for (int i = 0; i < c->recomp_slots[b].k; ++i) tplace[t_row0[b] + i] = StT2{b1 + b2, col + i, 0};
             col += c->recomp_slots[b].k;
         }
         for (int mt = 0; mt < mpad / kStTileM; ++mt)
             L.tiles2.push_back(StoreTile{a2 + (long long)mt * kc * chunkA, b2, kc,
-                                         std::min(kStTileM, m - mt * kStTileM), c->gptr[g] + mt * kStTileM, 1});
-        L.groups2.push_back(StoreGroup{b2, kc, K, -1, map0});
+                                         std::min(kStTileM, 2 * m - mt * kStTileM), mt * kStTileM, 1,
+                                         c->gptr[g], m});
         a2 += (long long)mpad * kc * epc;
         b2 += (long long)kc * chunkB;
     }
@@ -539,9 +561,15 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
         PSKEL_TRY(c->st_al.reserve(abytes));
         PSKEL_TRY(c->st_bl.reserve((size_t)(b1 + b2) * esize + 256));
     }
-    PSKEL_TRY(c->st_t.reserve((size_t)std::max(trow, 1) * kStN * sizeof(float)));
+    PSKEL_TRY(c->st_t.reserve(sizeof(StT2) * tplace.size()));
+    PSKEL_CUDA(cudaMemcpyAsync(c->st_t.ptr, tplace.data(), sizeof(StT2) * tplace.size(), cudaMemcpyHostToDevice,
+                               c->stream));
     PSKEL_CUDA(cudaMemsetAsync(c->st_ah.ptr, 0, abytes, c->stream));
     if (planes == 2) PSKEL_CUDA(cudaMemsetAsync(c->st_al.ptr, 0, abytes, c->stream));
+    // the B planes' K padding stays zero: every matvec rewrites the phase-1 region whole and
+    // the phase-2 rows k < 2K of each test group
+    PSKEL_CUDA(cudaMemsetAsync(c->st_bh.ptr, 0, (size_t)(b1 + b2) * esize, c->stream));
+    if (planes == 2) PSKEL_CUDA(cudaMemsetAsync(c->st_bl.ptr, 0, (size_t)(b1 + b2) * esize, c->stream));
     PSKEL_TRY(c->st_tab.reserve(sizeof(PackBlock) * nb + 256));
     PSKEL_CUDA(cudaMemcpyAsync(c->st_tab.ptr, pb.data(), sizeof(PackBlock) * nb, cudaMemcpyHostToDevice,
                                c->stream));
@@ -551,39 +579,38 @@ extern "C" int pskel_store_build_mode(pskel_ctx *c, int mode, long long *bytes) 
     PSKEL_LAUNCHED(1);
     // device tile and group tables (pointers resolved here)
     const int *gids = c->d_gids.as<int>();
-    PSKEL_TRY(c->st_map.reserve(sizeof(int) * std::max<size_t>(L.trow_map.size(), 1)));
-    if (!L.trow_map.empty())
-        PSKEL_CUDA(cudaMemcpyAsync(c->st_map.ptr, L.trow_map.data(), sizeof(int) * L.trow_map.size(),
-                                   cudaMemcpyHostToDevice, c->stream));
     // work items: phase-1 tiles whole (their K is one source group); phase-2 tiles cut into K
     // slices of at most kStSliceStages stages, accumulated with atomics
     std::vector<StItem> t1, t2;
     for (const StoreTile &t : L.tiles1)
-        t1.push_back(StItem{t.a_off, t.b_off, t.kc / 8, t.rows, t.out0, nullptr});
+        t1.push_back(StItem{t.a_off, t.b_off, t.kc / 8, t.rows, t.out0, nullptr, 0});
     for (const StoreTile &t : L.tiles2)
         for (int s0 = 0; s0 < t.kc / 8; s0 += kStSliceStages)
             t2.push_back(StItem{a1 + t.a_off + (long long)s0 * 8 * chunkA,
                                 b1 + t.b_off + (long long)s0 * 8 * chunkB,
-                                std::min(kStSliceStages, t.kc / 8 - s0), t.rows, 0, gids + t.out0});
+                                std::min(kStSliceStages, t.kc / 8 - s0), t.rows, t.out0, gids + t.ids0, t.m});
     L.n_items1 = (int)t1.size();
     L.n_items2 = (int)t2.size();
-    std::vector<StGroupB> g1, g2;
+    std::vector<StGroupB> g1;
     for (const StoreGroup &g : L.groups1) g1.push_back(StGroupB{g.b_base, g.kc, g.K, gids + g.ids0});
-    for (const StoreGroup &g : L.groups2)
-        g2.push_back(StGroupB{b1 + g.b_base, g.kc, g.K, c->st_map.as<int>() + g.map0});
+    // phase-1 B-builder items: every 8-chunk block of every source group (kc is a multiple of 8)
+    std::vector<StBItem> bi1;
+    for (size_t g = 0; g < g1.size(); ++g)
+        for (int kb = 0; kb < g1[g].kc / 8; ++kb) bi1.push_back(StBItem{(int)g, kb});
+    L.n_bitems1 = (int)bi1.size();
     const size_t s1 = sizeof(StItem) * t1.size(), s2 = sizeof(StItem) * t2.size();
-    const size_t s3 = sizeof(StGroupB) * g1.size(), s4 = sizeof(StGroupB) * g2.size();
+    const size_t s3 = sizeof(StGroupB) * g1.size(), s5 = sizeof(StBItem) * bi1.size();
     auto al256 = [](size_t x) { return (x + 255) & ~size_t(255); };
-    PSKEL_TRY(c->st_tiles.reserve(al256(s1) + al256(s2) + al256(s3) + al256(s4) + 256));
+    PSKEL_TRY(c->st_tiles.reserve(al256(s1) + al256(s2) + al256(s3) + al256(s5) + 256));
     char *d = c->st_tiles.as<char>();
     L.d_t1 = d;
     L.d_t2 = d + al256(s1);
     L.d_g1 = d + al256(s1) + al256(s2);
-    L.d_g2 = d + al256(s1) + al256(s2) + al256(s3);
+    L.d_bi1 = d + al256(s1) + al256(s2) + al256(s3);
     if (s1) PSKEL_CUDA(cudaMemcpyAsync(L.d_t1, t1.data(), s1, cudaMemcpyHostToDevice, c->stream));
     if (s2) PSKEL_CUDA(cudaMemcpyAsync(L.d_t2, t2.data(), s2, cudaMemcpyHostToDevice, c->stream));
     if (s3) PSKEL_CUDA(cudaMemcpyAsync(L.d_g1, g1.data(), s3, cudaMemcpyHostToDevice, c->stream));
-    if (s4) PSKEL_CUDA(cudaMemcpyAsync(L.d_g2, g2.data(), s4, cudaMemcpyHostToDevice, c->stream));
+    if (s5) PSKEL_CUDA(cudaMemcpyAsync(L.d_bi1, bi1.data(), s5, cudaMemcpyHostToDevice, c->stream));
     PSKEL_CUDA(cudaStreamSynchronize(c->stream));
     L.ready = true;
     L.generation = c->generation;
@@ -596,7 +623,9 @@ extern "C" int pskel_store_build(pskel_ctx *c, long long *bytes) {
 }
 
 namespace {
-// The four launches of one matvec over a store of format MODE (Y cleared by the caller).
+// The three launches of one matvec over a store of format MODE: the phase-1 B operand (with the
+// clear of Y and of the error word), the phase-1 GEMM (writing the phase-2 B operand), the
+// phase-2 GEMM (atomics into Y).
 template <int MODE>
 int store_matvec_t(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
                    cudaStream_t st) {
@@ -608,27 +637,24 @@ int store_matvec_t(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int n
     E *bh = c->st_bh.as<E>(), *bl = two ? c->st_bl.as<E>() : nullptr;
     int *err = c->st_err.as<int>();
     const int n1 = L.n_items1, n2 = L.n_items2;
-    const int ng1 = (int)L.groups1.size(), ng2 = (int)L.groups2.size();
+    const int nb1 = L.n_bitems1;
     const int sms = sm_count();
-    if (ng1 > 0) {
-        build_b1_kernel<MODE><<<ng1, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g1),
-                                                   reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl);
+    if (nb1 > 0) {
+        build_b1_kernel<MODE><<<nb1, 256, 0, st>>>(reinterpret_cast<const StBItem *>(L.d_bi1),
+                                                   reinterpret_cast<const StGroupB *>(L.d_g1),
+                                                   reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl,
+                                                   reinterpret_cast<float2 *>(Y), (long long)ldy * nrhs, err);
         PSKEL_LAUNCHED(1);
     }
     if (n1 > 0) {
         store_gemm_kernel<MODE><<<std::min(n1, sms), 192, kStSmem, st>>>(
-            reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<float>(), nullptr, 0,
-            kStRhs, err);
-        PSKEL_LAUNCHED(1);
-    }
-    if (ng2 > 0) {
-        build_b2_kernel<MODE><<<ng2, 256, 0, st>>>(reinterpret_cast<const StGroupB *>(L.d_g2),
-                                                   c->st_t.as<float>(), bh, bl);
+            reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<StT2>(), bh, bl,
+            nullptr, 0, kStRhs, err);
         PSKEL_LAUNCHED(1);
     }
     if (n2 > 0) {
         store_gemm_kernel<MODE><<<std::min(n2, sms), 192, kStSmem, st>>>(
-            reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr,
+            reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr, nullptr, nullptr,
             reinterpret_cast<float *>(Y), ldy, nrhs, err);
         PSKEL_LAUNCHED(1);
     }
@@ -650,8 +676,10 @@ extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y,
     PSKEL_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     PSKEL_TRY(c->st_err.reserve(256));
-    PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
-    PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));
+    if (L.n_bitems1 == 0) {  // no phase-1 work: Y and the error word are cleared here
+        PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
+        PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));
+    }
     if (L.mode == PSKEL_STORE_BF16X3) return store_matvec_t<PSKEL_STORE_BF16X3>(c, X, ldx, Y, ldy, nrhs, st);
     if (L.mode == PSKEL_STORE_TF32) return store_matvec_t<PSKEL_STORE_TF32>(c, X, ldx, Y, ldy, nrhs, st);
     return store_matvec_t<PSKEL_STORE_TF32X3>(c, X, ldx, Y, ldy, nrhs, st);
