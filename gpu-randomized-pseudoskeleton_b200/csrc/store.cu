@@ -30,13 +30,15 @@
 // one contiguous range of global memory, fetched with one bulk copy (cp.async.bulk, the TMA
 // engine's linear mode) per plane. The hi and lo planes are two arrays of the same shape.
 //
-// Kernel: one CTA of 128 threads per 128-row output tile. Warp 0 allocates 32 TMEM columns
-// (the 128 x 32 FP32 accumulator) and its lane 0 issues the bulk copies of a 4-stage ring;
-// lane 0 of warp 1 issues tcgen05.mma (kind::f16, bf16 in, FP32 accumulate, M = 128, N = 32,
-// K = 16) and commits each stage back to the producer through an mbarrier; after the last
-// stage all four warps read their 32 TMEM lanes (tcgen05.ld 32x32b) and write the rows. Every
-// mbarrier wait is bounded: a wait that runs out sets the error word, the CTA stops issuing,
-// waits (bounded) for what it issued, frees its TMEM and returns.
+// Kernels of one matvec: build_b1_kernel (phase-1 B' from X; also clears Y), then the grouped
+// GEMM store_gemm_kernel twice (phase 1, phase 2): persistent, one CTA of 192 threads per SM
+// over 128-row work items. Warp 0 allocates two 32-column TMEM accumulators (128 x 32 FP32
+// each) and its lane 0 issues the bulk copies of a 4-stage ring; lane 0 of warp 1 issues
+// tcgen05.mma (M = 128, N = 32) and commits each stage back to the producer through an
+// mbarrier; warps 2-5 read their 32 TMEM lanes (tcgen05.ld 32x32b) and write the rows while the
+// next item accumulates into the other accumulator. Every mbarrier wait is bounded: a wait that
+// runs out sets the error word, the CTA stops issuing, waits (bounded) for what it issued,
+// frees its TMEM and returns.
 #include <algorithm>
 #include <cstring>
 #include <vector>
