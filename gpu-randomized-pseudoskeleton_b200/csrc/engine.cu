@@ -18,7 +18,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <numeric>
+#include <thread>
 
 #include "pskel_internal.cuh"
 #include "zgemm.cuh"
@@ -580,6 +582,25 @@ struct RoundPlan {
 
 constexpr int kPipeMinBlocks = 2048;  // smaller rounds run as one chunk
 
+// f(lo, hi) over [0, n) split into contiguous ranges run on up to kPlanThreads host threads
+// (one range per thread of at least min_each items; the calling thread takes the first)
+constexpr int kPlanThreads = 8;
+template <typename F>
+void parallel_ranges(int n, int min_each, F f) {
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int nt = std::max(1, std::min({kPlanThreads, hw, n / std::max(1, min_each)}));
+    if (nt <= 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    for (int t = 1; t < nt; ++t)
+        th.emplace_back(f, (int)((long long)n * t / nt), (int)((long long)n * (t + 1) / nt));
+    f(0, (int)((long long)n / nt));
+    for (std::thread &x : th) x.join();
+}
+
 // Lay out the round's storage, build all job tables on the host and upload them in one copy.
 // A first pass sizes everything (storage, fill tiles, pipeline chunks, re-check extents), so
 // that the second writes every table once, straight into the context's page-locked staging
@@ -608,63 +629,87 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         if (p.tri) return (nc + gtc[g] - 1) / gtc[g];
         return ((nr + tm - 1) / tm) * ((nc + tn - 1) / tn);
     };
-    // ---- first pass: keep arena, scratch, fill tiles (C, then Rx, of each block)
-    std::vector<size_t> off(nb + 1, 0);
+    // ---- first pass: keep arena, scratch, fill tiles (C, then Rx, of each block): sizes per
+    // block on the planning threads, then the running offsets
+    std::vector<size_t> off(nb + 1, 0), soffs(nb + 1, 0);
     std::vector<int> prefix(2 * (size_t)nb + 1, 0);
-    size_t scratch_total = 0;
     int max_pinv_tiles = 0;
     p.tri_rows = 0;
+    std::mutex red;  // the per-range maxima
+    parallel_ranges(nb, 2048, [&](int lo, int hi) {
+        int pt = 0, rm = 0;
+        for (int i = lo; i < hi; ++i) {
+            const int b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
+            const size_t m = rows_of(gt), n = rows_of(gs);
+            const size_t r = p.r[i], pe = p.pe[i], pc = p.pc[i];
+            size_t sz = 0;
+            sz += al16(m * (r + pc) * es);       // C (+ extra columns)
+            sz += al16((r + pe) * n * es);       // Rx
+            sz += al16(r * r * sizeof(double2)); // U
+            sz += al16(sizeof(int) * r) * 2;     // I, J
+            sz += al16(sizeof(int) * (pe + 1));  // Ix
+            sz += al16(sizeof(int) * (pc + 1));  // Jx
+            sz += al16(sizeof(int) * (r + pe));  // Ig
+            sz += al16(sizeof(int) * (r + pc));  // Jg
+            sz += al16(sizeof(double) * r);      // sigma
+            sz += al16(sizeof(int) * r);         // perm
+            sz += 16 + 64;                       // rank; est and its four sums
+            off[i + 1] = (sz + 255) & ~size_t(255);
+            soffs[i + 1] = 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
+            prefix[2 * i + 1] = job_tiles(gt, (int)m, (int)(r + pc));
+            prefix[2 * i + 2] = job_tiles(gs, (int)n, (int)(r + pe));
+            if (p.tri) rm = std::max(rm, (int)std::max(m, n));
+            pt = std::max(pt, (int)(((r + 31) / 32) * ((r + 31) / 32)));
+        }
+        std::lock_guard<std::mutex> lk(red);
+        max_pinv_tiles = std::max(max_pinv_tiles, pt);
+        p.tri_rows = std::max(p.tri_rows, rm);
+    });
     for (int i = 0; i < nb; ++i) {
-        const int b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
-        const size_t m = rows_of(gt), n = rows_of(gs);
-        const size_t r = p.r[i], pe = p.pe[i], pc = p.pc[i];
-        size_t s = 0;
-        s += al16(m * (r + pc) * es);       // C (+ extra columns)
-        s += al16((r + pe) * n * es);       // Rx
-        s += al16(r * r * sizeof(double2)); // U
-        s += al16(sizeof(int) * r) * 2;     // I, J
-        s += al16(sizeof(int) * (pe + 1));  // Ix
-        s += al16(sizeof(int) * (pc + 1));  // Jx
-        s += al16(sizeof(int) * (r + pe));  // Ig
-        s += al16(sizeof(int) * (r + pc));  // Jg
-        s += al16(sizeof(double) * r);      // sigma
-        s += al16(sizeof(int) * r);         // perm
-        s += 16 + 64;                       // rank; est and its four sums
-        off[i + 1] = off[i] + ((s + 255) & ~size_t(255));
-        scratch_total += 2 * al16(r * r * sizeof(double2)) + al16((pe + pc) * r * sizeof(double2));
-        prefix[2 * i + 1] = prefix[2 * i] + job_tiles(gt, (int)m, (int)(r + pc));
-        prefix[2 * i + 2] = prefix[2 * i + 1] + job_tiles(gs, (int)n, (int)(r + pe));
-        if (p.tri) p.tri_rows = std::max(p.tri_rows, (int)std::max(m, n));
-        max_pinv_tiles = std::max(max_pinv_tiles, (int)(((r + 31) / 32) * ((r + 31) / 32)));
+        off[i + 1] += off[i];
+        soffs[i + 1] += soffs[i];
     }
+    for (size_t j = 1; j < prefix.size(); ++j) prefix[j] += prefix[j - 1];
+    size_t scratch_total = soffs[nb];
     // re-check storage of every candidate after the blocks' scratch: the fresh extra columns
     // (m x pc2) and rows (pe2 x n), their local and global ids, the estimate's scratch; its fill
     // jobs (extra columns, then extra rows, where there are any) and their tiles
-    std::vector<int> vpe2(nv), vpc2(nv), vjob0(nv + 1, 0);
+    std::vector<int> vpe2(nv), vpc2(nv), vjob0(nv + 1, 0), vtc(nv), vtr(nv);
     std::vector<size_t> voff(nv + 1, 0);
+    p.vrmax = p.vpemax = p.vpcmax = p.vtri_rows = 0;
+    parallel_ranges(nv, 2048, [&](int lo, int hi) {
+        int rmax = 0, pemax = 0, pcmax = 0, trows = 0;
+        for (int v = lo; v < hi; ++v) {
+            const int i = p.vcand[v], b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
+            const int m = rows_of(gt), n = rows_of(gs);
+            verify_extent(m, n, p.r[i], p.pe[i], p.pc[i], o, &vpe2[v], &vpc2[v]);
+            size_t q = al16((size_t)m * vpc2[v] * es) + al16((size_t)vpe2[v] * n * es);
+            q += 4 * al16(sizeof(int) * (kMaxExtra + 1));
+            q += al16(sizeof(double2) * (size_t)(vpe2[v] + vpc2[v]) * p.r[i]);
+            voff[v + 1] = al256(q);
+            vtc[v] = vpc2[v] > 0 ? job_tiles(gt, m, vpc2[v]) : -1;  // -1: no job
+            vtr[v] = vpe2[v] > 0 ? job_tiles(gs, n, vpe2[v]) : -1;
+            if (p.tri && vpc2[v] > 0) trows = std::max(trows, m);
+            if (p.tri && vpe2[v] > 0) trows = std::max(trows, n);
+            rmax = std::max(rmax, p.r[i]);
+            pemax = std::max(pemax, vpe2[v]);
+            pcmax = std::max(pcmax, vpc2[v]);
+        }
+        std::lock_guard<std::mutex> lk(red);
+        p.vrmax = std::max(p.vrmax, rmax);
+        p.vpemax = std::max(p.vpemax, pemax);
+        p.vpcmax = std::max(p.vpcmax, pcmax);
+        p.vtri_rows = std::max(p.vtri_rows, trows);
+    });
+    // running offsets; each candidate's fill jobs (extra columns, then extra rows, where there
+    // are any) and their tiles
     std::vector<int> vprefix(1, 0);
     vprefix.reserve(2 * (size_t)nv + 1);
-    p.vrmax = p.vpemax = p.vpcmax = p.vtri_rows = 0;
     for (int v = 0; v < nv; ++v) {
-        const int i = p.vcand[v], b = p.blocks[i], gt = c->gt[b], gs = c->gs[b];
-        const int m = rows_of(gt), n = rows_of(gs);
-        verify_extent(m, n, p.r[i], p.pe[i], p.pc[i], o, &vpe2[v], &vpc2[v]);
-        size_t q = al16((size_t)m * vpc2[v] * es) + al16((size_t)vpe2[v] * n * es);
-        q += 4 * al16(sizeof(int) * (kMaxExtra + 1));
-        q += al16(sizeof(double2) * (size_t)(vpe2[v] + vpc2[v]) * p.r[i]);
-        voff[v + 1] = voff[v] + al256(q);
+        voff[v + 1] += voff[v];
         vjob0[v] = (int)vprefix.size() - 1;
-        if (vpc2[v] > 0) {
-            vprefix.push_back(vprefix.back() + job_tiles(gt, m, vpc2[v]));
-            if (p.tri) p.vtri_rows = std::max(p.vtri_rows, m);
-        }
-        if (vpe2[v] > 0) {
-            vprefix.push_back(vprefix.back() + job_tiles(gs, n, vpe2[v]));
-            if (p.tri) p.vtri_rows = std::max(p.vtri_rows, n);
-        }
-        p.vrmax = std::max(p.vrmax, p.r[i]);
-        p.vpemax = std::max(p.vpemax, vpe2[v]);
-        p.vpcmax = std::max(p.vpcmax, vpc2[v]);
+        if (vtc[v] >= 0) vprefix.push_back(vprefix.back() + vtc[v]);
+        if (vtr[v] >= 0) vprefix.push_back(vprefix.back() + vtr[v]);
     }
     const int nvf = (int)vprefix.size() - 1;
     vjob0[nv] = nvf;
@@ -729,8 +774,8 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
     char *kb = ar.keep.as<char>();
     char *sb = ar.work.as<char>();
     const int *tri_ids = c->d_gtri.as<int>(), *tri_adj = c->d_gadj.as<int>();
-    size_t soff = 0;
-    for (int i = 0; i < nb; ++i) {
+    parallel_ranges(nb, 2048, [&](int lo, int hi) {
+    for (int i = lo; i < hi; ++i) {
         const int b = p.blocks[i];
         BlockWork w{};
         BlockResult &res = c->results[b];
@@ -759,12 +804,12 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         w.perm = reinterpret_cast<int *>(take(sizeof(int) * r));
         w.rank = reinterpret_cast<int *>(take(16));
         w.est = reinterpret_cast<double *>(take(64));
+        size_t soff = soffs[i];
         w.AV = reinterpret_cast<double2 *>(sb + soff);
         soff += al16(r * r * sizeof(double2));
         w.V = reinterpret_cast<double2 *>(sb + soff);
         soff += al16(r * r * sizeof(double2));
         w.T = reinterpret_cast<double2 *>(sb + soff);
-        soff += al16((pe + pc) * r * sizeof(double2));
         works[i] = w;
         // C = Z(group_t, [J; Jx]); Rx = Z([I; Ix], group_s) filled as the transpose of
         // Z(group_s, [I; Ix]) (the Galerkin block is symmetric for equal test and source rules),
@@ -811,6 +856,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         res.offSig = (char *)w.sigma - kb;
         res.offPerm = (char *)w.perm - kb;
     }
+    });
     // SVD plans of the round and of each chunk (index maps into the round's SvdJob table)
     PSKEL_TRY(svd_plan(svds, nb, p.svd));
     std::memcpy(h + o_idx, p.svd.idx.data(), sizeof(int) * nb);
@@ -848,8 +894,9 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
         double *vouts = reinterpret_cast<double *>(ob + outs_vouts_offset(nb));
         int *gates = reinterpret_cast<int *>(ob + outs_gates_offset(nb, nv));
         p.d_gates = gates;
-        int f = 0;  // next re-check fill job
-        for (int v = 0; v < nv; ++v) {
+        parallel_ranges(nv, 2048, [&](int lo, int hi) {
+        for (int v = lo; v < hi; ++v) {
+            int f = vjob0[v];  // the candidate's first re-check fill job
             const int i = p.vcand[v];
             const BlockWork &w = works[i];
             const int b = w.block_id, pe2 = vpe2[v], pc2 = vpc2[v];
@@ -902,6 +949,7 @@ int plan_round(pskel_ctx *c, RoundPlan &p, const pskel_opts_t &o) {
                 vjgate[f++] = gates + v;
             }
         }
+        });
     }
     std::vector<size_t> vch_off(nch);
     {
