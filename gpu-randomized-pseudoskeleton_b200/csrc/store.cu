@@ -175,30 +175,35 @@ __device__ __forceinline__ void st_store_chunk(typename StFmt<MODE>::E *Bh, type
     if (StFmt<MODE>::kPlanes == 2) *reinterpret_cast<uint4 *>(Bl + o) = *reinterpret_cast<const uint4 *>(lo);
 }
 
-// phase 1: B'(k, c) from X (complex64, column-major, ldx), columns >= nrhs are zero. A CTA stages
-// the X rows of its 8 x EPC K values in shared memory; thread (q, c) then writes chunk q of column
-// c: EPC consecutive K values, 16 bytes per plane, each warp one contiguous 512-byte row. The
-// grid also clears Y (ny float2, the phase-2 atomics' target) and the error word.
+// phase 1: B'(k, c) from X (complex64, entry (i, rhs) at X[i xr + rhs xc]), columns >= nrhs
+// are zero. A CTA stages the X rows of its 8 x EPC K values in shared memory; thread (q, c) then
+// writes chunk q of column c: EPC consecutive K values, 16 bytes per plane, each warp one
+// contiguous 512-byte row. The grid also clears Y (ne x nrhs entries at Y[i yr + rhs yc], the
+// phase-2 atomics' target; the unit stride runs fastest) and the error word.
 template <int MODE>
 __global__ void __launch_bounds__(256) build_b1_kernel(const StBItem *__restrict__ items,
                                                        const StGroupB *__restrict__ groups,
-                                                       const float2 *__restrict__ X, int ldx,
-                                                       int nrhs, typename StFmt<MODE>::E *Bh,
-                                                       typename StFmt<MODE>::E *Bl, float2 *Y,
-                                                       long long ny, int *err) {
+                                                       const float2 *__restrict__ X, long long xr,
+                                                       long long xc, int nrhs, typename StFmt<MODE>::E *Bh,
+                                                       typename StFmt<MODE>::E *Bl, float2 *Y, int ne,
+                                                       long long yr, long long yc, int *err) {
     using E = typename StFmt<MODE>::E;
     constexpr int EPC = StFmt<MODE>::kEpc, KB = 8 * EPC;
     __shared__ float2 xs[KB][kStRhs + 1];
     if (blockIdx.x == 0 && threadIdx.x == 0) *err = 0;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ny; e += (long long)gridDim.x * blockDim.x)
-        Y[e] = make_float2(0.f, 0.f);
+    const long long ny = (long long)ne * nrhs;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ny; e += (long long)gridDim.x * blockDim.x) {
+        const long long i = yr == 1 ? e % ne : e / nrhs, rhs = yr == 1 ? e / ne : e % nrhs;
+        Y[i * yr + rhs * yc] = make_float2(0.f, 0.f);
+    }
     const StBItem it = items[blockIdx.x];
     const StGroupB g = groups[it.g];
     const int k0 = it.kb * KB;
     for (int e = threadIdx.x; e < KB * kStRhs; e += blockDim.x) {
-        const int kk = e % KB, rhs = e / KB, k = k0 + kk;
+        // the unit stride of X runs fastest across the threads
+        const int kk = xc == 1 ? e / kStRhs : e % KB, rhs = xc == 1 ? e % kStRhs : e / KB, k = k0 + kk;
         float2 x = make_float2(0.f, 0.f);
-        if (k < 2 * g.K && rhs < nrhs) x = X[g.src[k < g.K ? k : k - g.K] + (size_t)rhs * ldx];
+        if (k < 2 * g.K && rhs < nrhs) x = X[(long long)g.src[k < g.K ? k : k - g.K] * xr + rhs * xc];
         xs[kk][rhs] = x;
     }
     __syncthreads();
@@ -266,7 +271,8 @@ __global__ void __launch_bounds__(192, 1)
                       const typename StFmt<MODE>::E *__restrict__ Bh,
                       const typename StFmt<MODE>::E *__restrict__ Bl,
                       const StT2 *__restrict__ t2, typename StFmt<MODE>::E *B2h,
-                      typename StFmt<MODE>::E *B2l, float *Y, int ldy, int nrhs, int *err) {
+                      typename StFmt<MODE>::E *B2l, float *Y, long long yr, long long yc, int nrhs,
+                      int *err) {
     constexpr int EPC = StFmt<MODE>::kEpc;
     constexpr bool kTwo = StFmt<MODE>::kPlanes == 2;
     constexpr int kChunkA = kStTileM * EPC, kChunkB = kStN * EPC;  // elements per chunk block
@@ -423,7 +429,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
                     for (int c = 0; c < kStRhs; ++c)
                         if (c < nrhs) {
-                            float *y = Y + 2 * ((size_t)id + (size_t)c * ldy);
+                            float *y = Y + 2 * ((long long)id * yr + (long long)c * yc);
                             const float a = __uint_as_float(v[c]), b = __uint_as_float(v[c + kStRhs]);
                             atomicAdd(y, im ? -b : a);
                             atomicAdd(y + 1, im ? a : b);
@@ -629,8 +635,8 @@ namespace {
 // clear of Y and of the error word), the phase-1 GEMM (writing the phase-2 B operand), the
 // phase-2 GEMM (atomics into Y).
 template <int MODE>
-int store_matvec_t(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
-                   cudaStream_t st) {
+int store_matvec_t(pskel_ctx *c, const void *X, long long xr, long long xc, void *Y, long long yr,
+                   long long yc, int nrhs, cudaStream_t st) {
     using E = typename StFmt<MODE>::E;
     const bool two = StFmt<MODE>::kPlanes == 2;
     const StoreLayout &L = c->store;
@@ -644,30 +650,33 @@ int store_matvec_t(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int n
     if (nb1 > 0) {
         build_b1_kernel<MODE><<<nb1, 256, 0, st>>>(reinterpret_cast<const StBItem *>(L.d_bi1),
                                                    reinterpret_cast<const StGroupB *>(L.d_g1),
-                                                   reinterpret_cast<const float2 *>(X), ldx, nrhs, bh, bl,
-                                                   reinterpret_cast<float2 *>(Y), (long long)ldy * nrhs, err);
+                                                   reinterpret_cast<const float2 *>(X), xr, xc, nrhs, bh, bl,
+                                                   reinterpret_cast<float2 *>(Y), c->mesh.ne, yr, yc, err);
         PSKEL_LAUNCHED(1);
     }
     if (n1 > 0) {
         store_gemm_kernel<MODE><<<std::min(n1, sms), 192, kStSmem, st>>>(
             reinterpret_cast<const StItem *>(L.d_t1), n1, ah, al, bh, bl, c->st_t.as<StT2>(), bh, bl,
-            nullptr, 0, kStRhs, err);
+            nullptr, 0, 0, kStRhs, err);
         PSKEL_LAUNCHED(1);
     }
     if (n2 > 0) {
         store_gemm_kernel<MODE><<<std::min(n2, sms), 192, kStSmem, st>>>(
             reinterpret_cast<const StItem *>(L.d_t2), n2, ah, al, bh, bl, nullptr, nullptr, nullptr,
-            reinterpret_cast<float *>(Y), ldy, nrhs, err);
+            reinterpret_cast<float *>(Y), yr, yc, nrhs, err);
         PSKEL_LAUNCHED(1);
     }
     return PSKEL_OK;
 }
 }  // namespace
 
-extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
-                                  void *stream) {
-    if (!c || !X || !Y || nrhs <= 0 || nrhs > kStRhs || ldx < c->mesh.ne || ldy < c->mesh.ne) {
-        set_error(PSKEL_ERR_ARG, "store_matvec: bad arguments (nrhs=%d, at most %d)", nrhs, kStRhs);
+extern "C" int pskel_store_matvec_strided(pskel_ctx *c, const void *X, long long x_row_stride,
+                                          long long x_col_stride, void *Y, long long y_row_stride,
+                                          long long y_col_stride, int nrhs, void *stream) {
+    if (!c || !X || !Y || nrhs <= 0 || nrhs > kStRhs || x_row_stride <= 0 || x_col_stride <= 0 ||
+        !((y_row_stride == 1 && y_col_stride >= c->mesh.ne) || (y_col_stride == 1 && y_row_stride >= nrhs))) {
+        set_error(PSKEL_ERR_ARG, "store_matvec: bad arguments (nrhs=%d, at most %d; positive X strides; Y "
+                                 "column-major or row-major without overlap)", nrhs, kStRhs);
         return PSKEL_ERR_ARG;
     }
     const StoreLayout &L = c->store;
@@ -680,11 +689,24 @@ extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y,
     PSKEL_TRY(c->st_err.reserve(256));
     if (L.n_bitems1 == 0) {  // no phase-1 work: Y and the error word are cleared here
         PSKEL_CUDA(cudaMemsetAsync(c->st_err.ptr, 0, sizeof(int), st));
-        PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)ldy * nrhs, st));
+        if (y_row_stride == 1)
+            PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)y_col_stride * nrhs, st));
+        else
+            PSKEL_CUDA(cudaMemsetAsync(Y, 0, sizeof(float2) * (size_t)y_row_stride * c->mesh.ne, st));
     }
-    if (L.mode == PSKEL_STORE_BF16X3) return store_matvec_t<PSKEL_STORE_BF16X3>(c, X, ldx, Y, ldy, nrhs, st);
-    if (L.mode == PSKEL_STORE_TF32) return store_matvec_t<PSKEL_STORE_TF32>(c, X, ldx, Y, ldy, nrhs, st);
-    return store_matvec_t<PSKEL_STORE_TF32X3>(c, X, ldx, Y, ldy, nrhs, st);
+    const long long xr = x_row_stride, xc = x_col_stride, yr = y_row_stride, yc = y_col_stride;
+    if (L.mode == PSKEL_STORE_BF16X3) return store_matvec_t<PSKEL_STORE_BF16X3>(c, X, xr, xc, Y, yr, yc, nrhs, st);
+    if (L.mode == PSKEL_STORE_TF32) return store_matvec_t<PSKEL_STORE_TF32>(c, X, xr, xc, Y, yr, yc, nrhs, st);
+    return store_matvec_t<PSKEL_STORE_TF32X3>(c, X, xr, xc, Y, yr, yc, nrhs, st);
+}
+
+extern "C" int pskel_store_matvec(pskel_ctx *c, const void *X, int ldx, void *Y, int ldy, int nrhs,
+                                  void *stream) {
+    if (!c || ldx < c->mesh.ne || ldy < c->mesh.ne) {
+        set_error(PSKEL_ERR_ARG, "store_matvec: bad arguments (ldx=%d, ldy=%d)", ldx, ldy);
+        return PSKEL_ERR_ARG;
+    }
+    return pskel_store_matvec_strided(c, X, 1, ldx, Y, 1, ldy, nrhs, stream);
 }
 
 extern "C" int pskel_store_status(pskel_ctx *c, int *error_word) {

@@ -106,6 +106,8 @@ SIGNATURES = {
     "pskel_store_build": (ci, [VP, ctypes.POINTER(ctypes.c_longlong)]),
     "pskel_store_build_mode": (ci, [VP, ci, ctypes.POINTER(ctypes.c_longlong)]),
     "pskel_store_matvec": (ci, [VP, VP, ci, VP, ci, ci, VP]),
+    "pskel_store_matvec_strided": (ci, [VP, VP, ctypes.c_longlong, ctypes.c_longlong, VP,
+                                        ctypes.c_longlong, ctypes.c_longlong, ci, VP]),
     "pskel_store_status": (ci, [VP, I32]),
     "pskel_mlp_num_params": (ci, []),
     "pskel_mlp_forward": (ci, [VP, VP, ci, VP, VP]),

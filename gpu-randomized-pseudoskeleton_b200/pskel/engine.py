@@ -307,13 +307,16 @@ class Engine:
         if X.dtype != torch.complex64 or not X.is_cuda:
             raise ValueError("X must be a complex64 CUDA tensor")
         ne, nrhs = X.shape
-        Xc = X.t().contiguous()
-        Y = torch.empty_like(Xc)
+        if X.stride(0) <= 0 or X.stride(1) <= 0:
+            X = X.contiguous()
+        # X as it is laid out (no transposed copy); Y column-major (the phase-2 atomics of one
+        # right-hand side then land on consecutive RWG ids), returned as its transposed view
+        Yt = torch.empty((nrhs, ne), dtype=torch.complex64, device=X.device)
         s = torch.cuda.current_stream(X.device).cuda_stream
-        _lib.check(self._lib.pskel_store_matvec(self._h, ctypes.c_void_p(Xc.data_ptr()), ne,
-                                                ctypes.c_void_p(Y.data_ptr()), ne, nrhs,
-                                                ctypes.c_void_p(s)))
-        return Y.t()
+        _lib.check(self._lib.pskel_store_matvec_strided(
+            self._h, ctypes.c_void_p(X.data_ptr()), X.stride(0), X.stride(1),
+            ctypes.c_void_p(Yt.data_ptr()), 1, ne, nrhs, ctypes.c_void_p(s)))
+        return Yt.t()
 
     def aca_compress(self, tol: float, kmax: int = 128) -> dict:
         """Adaptive cross approximation of every far block (see pskel_aca_compress); returns

@@ -465,6 +465,14 @@ int pskel_store_build(pskel_ctx *ctx, long long *bytes);
    user_impedance_for_julia_cuda.cu:1929-1960. */
 int pskel_store_matvec(pskel_ctx *ctx, const void *X, int ldx, void *Y, int ldy, int nrhs,
                        void *stream);
+/* pskel_store_matvec with general strides, in pskel_c64 elements: X(i, j) at
+   X[i x_row_stride + j x_col_stride], Y(i, j) at Y[i y_row_stride + j y_col_stride]; Y is
+   column-major (y_row_stride 1, y_col_stride >= RWG count) or row-major (y_col_stride 1,
+   y_row_stride >= nrhs). A row-major (RWG count, nrhs) tensor is passed without a transposed
+   copy. No reference counterpart (the reference's matvec takes one vector). */
+int pskel_store_matvec_strided(pskel_ctx *ctx, const void *X, long long x_row_stride,
+                               long long x_col_stride, void *Y, long long y_row_stride,
+                               long long y_col_stride, int nrhs, void *stream);
 
 /* Error word of the last pskel_store_matvec (0: every pipeline wait completed; 1: a bounded
    wait ran out and the affected tiles were skipped). Waits for the device. */

@@ -112,3 +112,32 @@ def test_store_formats_match_fp64_product(compressed, mode, bar):
     Yo = _recompressed_product(eng, X.astype(np.complex128))
     err = np.linalg.norm(Y - Yo) / np.linalg.norm(Yo)
     assert err < bar, (mode, err)
+
+
+def test_store_matvec_layouts_agree(compressed):
+    """The strided entry point: X row-major (the tensor as it is) and column-major (through
+    pskel_store_matvec with ldx), Y column-major and row-major, give the same products; Y strides
+    that overlap are refused."""
+    import ctypes
+
+    from pskel import _lib
+    m, eng, st, ks, nbytes = compressed
+    rng = np.random.default_rng(21)
+    X = (rng.standard_normal((m.N, 7)) + 1j * rng.standard_normal((m.N, 7))).astype(np.complex64)
+    Xd = torch.as_tensor(X, device="cuda:0")  # row-major
+    Y1 = eng.store_matvec(Xd).cpu().numpy()
+    L = _lib.lib()
+    vp = lambda t: ctypes.c_void_p(t.data_ptr())
+    ldx = m.N + 3
+    Xc = torch.zeros((7, ldx), dtype=torch.complex64, device="cuda:0")
+    Xc[:, :m.N] = Xd.t()
+    Yc = torch.zeros((7, ldx), dtype=torch.complex64, device="cuda:0")
+    _lib.check(L.pskel_store_matvec(eng._h, vp(Xc), ldx, vp(Yc), ldx, 7, None))
+    Yr = torch.zeros((m.N, 7), dtype=torch.complex64, device="cuda:0")
+    _lib.check(L.pskel_store_matvec_strided(eng._h, vp(Xd), 7, 1, vp(Yr), 7, 1, 7, None))
+    torch.cuda.synchronize()
+    # the same products; the phase-2 FP32 atomics add K slices in run-dependent order
+    for Y2 in (Yc[:, :m.N].t().cpu().numpy(), Yr.cpu().numpy()):
+        assert np.linalg.norm(Y2 - Y1) <= 1e-6 * np.linalg.norm(Y1)
+    with pytest.raises(_lib.PskelError):  # Y rows overlapping
+        _lib.check(L.pskel_store_matvec_strided(eng._h, vp(Xd), 7, 1, vp(Yr), 3, 1, 7, None))
