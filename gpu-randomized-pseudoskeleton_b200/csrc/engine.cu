@@ -595,8 +595,14 @@ void parallel_ranges(int n, int min_each, F f) {
     }
     std::vector<std::thread> th;
     th.reserve(nt - 1);
-    for (int t = 1; t < nt; ++t)
-        th.emplace_back(f, (int)((long long)n * t / nt), (int)((long long)n * (t + 1) / nt));
+    for (int t = 1; t < nt; ++t) {
+        const int lo = (int)((long long)n * t / nt), hi = (int)((long long)n * (t + 1) / nt);
+        try {
+            th.emplace_back(f, lo, hi);
+        } catch (...) {  // no thread to be had: the range runs here
+            f(lo, hi);
+        }
+    }
     f(0, (int)((long long)n / nt));
     for (std::thread &x : th) x.join();
 }
