@@ -148,11 +148,13 @@ __device__ double zero_column_norm2(const double2 *A, size_t count, int m) {
 }
 
 // Lanes per column pair in a Jacobi round over w columns of m rows: as many as keep at least
-// two rows per lane while all w/2 pairs of a round still run at once in the CTA.
+// two rows per lane while all w/2 pairs of a round still run at once in the CTA, at most 8 (16
+// lanes per pair made the cores of 32-63 columns take 512-thread CTAs, two per SM; with 8 they
+// take the five-CTA instantiation: pinv of the 30,720-RWG round 14.8 -> 13.3 ms).
 __device__ int jacobi_team(int m, int w, int threads) {
     const int npairs = (w + 1) / 2;
     int t = 1;
-    while (t < 32 && 2 * t * 2 <= m && 2 * t * npairs <= threads) t <<= 1;
+    while (t < 8 && 2 * t * 2 <= m && 2 * t * npairs <= threads) t <<= 1;
     return t;
 }
 
@@ -561,7 +563,7 @@ static int size_class(int n) { return n <= 16 ? 0 : n <= 32 ? 1 : n <= 48 ? 2 : 
 
 static int resident_threads_for(int n) {
     int team = 1;
-    while (team < 32 && 4 * team <= n) team <<= 1;  // jacobi_team without the thread cap
+    while (team < 8 && 4 * team <= n) team <<= 1;  // jacobi_team without the thread cap
     int want = team * ((n + 1) / 2);
     want = (want + 31) / 32 * 32;
     return want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
