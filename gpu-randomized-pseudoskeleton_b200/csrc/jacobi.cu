@@ -150,7 +150,7 @@ __device__ double zero_column_norm2(const double2 *A, size_t count, int m) {
 // Lanes per column pair in a Jacobi round over w columns of m rows: as many as keep at least
 // two rows per lane while all w/2 pairs of a round still run at once in the CTA, at most 8 (16
 // lanes per pair made the cores of 32-63 columns take 512-thread CTAs, two per SM; with 8 they
-// take the five-CTA instantiation: pinv of the 30,720-RWG round 14.8 -> 13.3 ms).
+// take the 256-thread instantiation: pinv of the 30,720-RWG round 14.8 -> 13.3 ms).
 __device__ int jacobi_team(int m, int w, int threads) {
     const int npairs = (w + 1) / 2;
     int t = 1;
@@ -200,11 +200,11 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 //      singular value amplifies).
 // Columns of B whose norm is zero give zero columns of V.
 // Two instantiations: up to 512 threads with at most 64 registers (one 512-thread CTA per 32 k
-// registers), and up to 256 threads with five CTAs per SM (at most 48 registers, a few spilled)
-// for the classes of small cores: more resident cores per SM hide the latency of the rotation
-// rounds (pinv of the 30,720-RWG round 13.4 -> 12.8 ms, recompression cores 6.2 -> 5.7 ms).
-// Without the register cap the compiler takes 104 registers and the 512-thread classes drop to
-// one CTA per SM.
+// registers), and up to 256 threads with at least four CTAs per SM (64 registers; the smaller
+// classes launch 64-128 threads and fit more) for the classes of small cores: more resident
+// cores per SM hide the latency of the rotation rounds (pinv of the 30,720-RWG round: 13.3 ms
+// with a five-CTA cap of 48 registers and spills, 12.8 ms with four). Without the register cap
+// the compiler takes 104 registers and the 512-thread classes drop to one CTA per SM.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
@@ -610,7 +610,7 @@ int svd_plan(const SvdJob *h_jobs, int nj, SvdPlan &plan) {
 
 int svd_resident_attr() {
     PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<kSvdThreads, 2>, kSmemBudget));
-    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<256, 5>, kSmemBudget));
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<256, 4>, kSmemBudget));
     return ensure_smem_attr(svd_blocked_kernel, kSmemBudget);
 }
 
@@ -660,7 +660,7 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
         const SvdPlan::Cls &c = plan.res[ci];
         cudaStream_t s = lane(l++);
         if (c.threads <= 256)
-            svd_resident_kernel<256, 5><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
+            svd_resident_kernel<256, 4><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         else
             svd_resident_kernel<kSvdThreads, 2><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
