@@ -148,13 +148,16 @@ __device__ double zero_column_norm2(const double2 *A, size_t count, int m) {
 }
 
 // Lanes per column pair in a Jacobi round over w columns of m rows: as many as keep at least
-// two rows per lane while all w/2 pairs of a round still run at once in the CTA, at most 8 (16
-// lanes per pair made the cores of 32-63 columns take 512-thread CTAs, two per SM; with 8 they
-// take the 256-thread instantiation: pinv of the 30,720-RWG round 14.8 -> 13.3 ms).
+// two rows per lane while all w/2 pairs of a round still run at once in the CTA, at most 8 up
+// to 64 columns (16 lanes per pair made the cores of 32-63 columns take 512-thread CTAs, two
+// per SM; with 8 they take the 256-thread instantiation: pinv of the 30,720-RWG round 14.8 ->
+// 13.3 ms) and 16 above (the few large cores of a second round, whose latency sets the round's:
+// one 1024-thread CTA per core).
 __device__ int jacobi_team(int m, int w, int threads) {
     const int npairs = (w + 1) / 2;
     int t = 1;
-    while (t < 8 && 2 * t * 2 <= m && 2 * t * npairs <= threads) t <<= 1;
+    const int cap = w > 64 ? 16 : 8;
+    while (t < cap && 2 * t * 2 <= m && 2 * t * npairs <= threads) t <<= 1;
     return t;
 }
 
@@ -199,12 +202,12 @@ __device__ void finish_sigma(const double2 *A, int lda, int m, int n, double *si
 //      product of A and V would carry eps |A| in every column, which the inverse of a small
 //      singular value amplifies).
 // Columns of B whose norm is zero give zero columns of V.
-// Two instantiations: up to 512 threads with at most 64 registers (one 512-thread CTA per 32 k
-// registers), and up to 256 threads with at least four CTAs per SM (64 registers; the smaller
+// Two instantiations: up to 1024 threads with at most 64 registers (the cores of more than 64
+// columns), and up to 256 threads with at least four CTAs per SM (64 registers; the smaller
 // classes launch 64-128 threads and fit more) for the classes of small cores: more resident
 // cores per SM hide the latency of the rotation rounds (pinv of the 30,720-RWG round: 13.3 ms
-// with a five-CTA cap of 48 registers and spills, 12.8 ms with four). Without the register cap
-// the compiler takes 104 registers and the 512-thread classes drop to one CTA per SM.
+// with a five-CTA cap of 48 registers and spills, 12.8 ms with four). Without a register cap
+// the compiler takes 104 registers.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB)
     svd_resident_kernel(SvdJob *jobs, const int *idx_map, int max_sweeps) {
@@ -564,10 +567,11 @@ static int size_class(int n) { return n <= 16 ? 0 : n <= 24 ? 1 : n <= 32 ? 2 : 
 
 static int resident_threads_for(int n) {
     int team = 1;
-    while (team < 8 && 4 * team <= n) team <<= 1;  // jacobi_team without the thread cap
+    const int cap = n > 64 ? 16 : 8;
+    while (team < cap && 4 * team <= n) team <<= 1;  // jacobi_team without the thread cap
     int want = team * ((n + 1) / 2);
     want = (want + 31) / 32 * 32;
-    return want < 64 ? 64 : (want > kSvdThreads ? kSvdThreads : want);
+    return want < 64 ? 64 : (want > 1024 ? 1024 : want);
 }
 
 int svd_plan(const std::vector<SvdJob> &h_jobs, SvdPlan &plan) {
@@ -610,7 +614,7 @@ int svd_plan(const SvdJob *h_jobs, int nj, SvdPlan &plan) {
 }
 
 int svd_resident_attr() {
-    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<kSvdThreads, 2>, kSmemBudget));
+    PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<1024, 1>, kSmemBudget));
     PSKEL_TRY(ensure_smem_attr(svd_resident_kernel<256, 4>, kSmemBudget));
     return ensure_smem_attr(svd_blocked_kernel, kSmemBudget);
 }
@@ -663,7 +667,7 @@ int svd_launch(SvdJob *d_jobs, const int *d_idx, const SvdPlan &plan, int max_sw
         if (c.threads <= 256)
             svd_resident_kernel<256, 4><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         else
-            svd_resident_kernel<kSvdThreads, 2><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
+            svd_resident_kernel<1024, 1><<<c.count, c.threads, c.smem, s>>>(d_jobs, d_idx + c.off, max_sweeps);
         PSKEL_LAUNCHED(1);
     }
     if (plan.blk_count > 0) {
