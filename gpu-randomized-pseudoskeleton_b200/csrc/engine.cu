@@ -1047,10 +1047,11 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
         return launch_estimate(p.d_est + b0, cnt, o.precision, rmax, pemax, pcmax, st);
     };
     const RoundOut *outs = c->arenas[p.round].outs.as<RoundOut>();
-    auto collect = [&](int b0, int cnt, cudaStream_t st) {
+    auto collect = [&](int b0, int cnt, cudaStream_t st) -> int {
         collect_kernel<<<(cnt + 255) / 256, 256, 0, st>>>(p.d_works + b0, p.d_svd + b0, cnt,
                                                           c->arenas[p.round].outs.as<RoundOut>() + b0);
         PSKEL_LAUNCHED(1);
+        return PSKEL_OK;
     };
     // the re-check of chunk k's blocks accepted with little margin, selected on the device from
     // their estimates: every candidate's launches are planned, the unselected return at once
@@ -1080,7 +1081,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
         PSKEL_TRY(fill(0, p.d_fill_prefix, p.fill_jobs, p.fill_tiles, s));
         if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));
         PSKEL_TRY(pinv_est(0, p.nb, p.svd, p.d_svd_idx, p.pinv_tiles, s, events ? c->ev[3] : nullptr));
-        collect(0, p.nb, s);
+        PSKEL_TRY(collect(0, p.nb, s));
         if (p.nv > 0) PSKEL_TRY(verify(0, s));
     } else {
         cudaStream_t s2 = c->pipe_stream;
@@ -1091,7 +1092,7 @@ int launch_round(pskel_ctx *c, const RoundPlan &p, const pskel_opts_t &o, bool e
             PSKEL_CUDA(cudaEventRecord(c->pipe_ev[k], s));
             PSKEL_CUDA(cudaStreamWaitEvent(s2, c->pipe_ev[k], 0));
             PSKEL_TRY(pinv_est(b0, cnt, p.ch_svd[k], p.ch_idx[k], p.ch_pinv_tiles[k], s2, nullptr));
-            collect(b0, cnt, s2);
+            PSKEL_TRY(collect(b0, cnt, s2));
             PSKEL_CUDA(cudaEventRecord(c->chunk_ev[k], s2));
         }
         if (events) PSKEL_CUDA(cudaEventRecord(c->ev[2], s));  // the last fill
@@ -1665,7 +1666,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
         set_error(PSKEL_ERR_RANGE, "an id was out of range during the fill");
         return PSKEL_ERR_RANGE;
     }
-    int worst = PSKEL_OK;
+    // per-block statuses are reported in stats (the call itself succeeds)
     for (int b = 0; b < nb; ++b) {
         const BlockResult &res = c->results[b];
         if (stats) {
@@ -1679,9 +1680,7 @@ extern "C" int pskel_compress_blocks(pskel_ctx *c, const pskel_opts_t *opts, con
             s.status = res.status;
             s.est = res.est;
         }
-        if (res.status != PSKEL_OK) worst = res.status;
     }
-    (void)worst;
     return PSKEL_OK;
 }
 

@@ -96,7 +96,7 @@ __global__ void noalloc_setup_kernel(unsigned char *base, const double2 *A, int 
 __global__ void noalloc_finish_kernel(const unsigned char *base, int M, int N, double2 *P,
                                       double *sigma_out, int *rank_out) {
     const bool tr = M < N;
-    const int m = tr ? N : M, n = tr ? M : N;  // working matrix m x n, its pinv Pt is n x m
+    const int n = tr ? M : N;  // working matrix (tr ? N : M) x n, its pinv Pt has n rows
     const double2 *Pt = reinterpret_cast<const double2 *>(base + NoAllocLayout::Pt);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < M * N; idx += gridDim.x * blockDim.x) {
         const int a = idx % N, b = idx / N;  // P(a, b), a < N, b < M
