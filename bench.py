@@ -851,6 +851,7 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
 #   python bench.py --profile-case store --calls 5
 #   python bench.py --profile-case extras
 #   python bench.py --profile-case recompress --calls 2 [--subdiv 5]
+#   python bench.py --profile-case matvec --calls 5 [--subdiv 5]
 def fill_case(prec, calls, split, geom32, tri_cols=8):
     """CALLS single-round compressions of every far block of the 7,680-RWG sphere at a fixed
     sample count of 24 with the given precision (c128 or c64) and fill variant (8: triangle
@@ -916,6 +917,36 @@ def store_case(calls, subdiv=4):
             torch.cuda.synchronize()
             print(f"store matvec call {i}: {e0.elapsed_time(e1):.4f} ms, store {nbytes / 1e6:.1f} MB, "
                   f"status {eng.store_status()}", flush=True)
+
+
+def matvec_case(calls, subdiv=4):
+    """Compress the sphere (SUBDIV 4: 7,680 RWG, 5: 30,720 RWG, the bench workload) as the
+    product does (learned first sample counts, complex64, symmetric mode) and run CALLS CUR-form
+    matvecs (pskel_matvec) with 16 complex64 right-hand sides, printing the device time of each.
+    Under a profiler each call is one matvec_group_kernel launch after a memset."""
+    import torch
+    from pskel import mesh as pmesh
+    from pskel import octree
+    from pskel.engine import Engine
+    from pskel.predictor import Predictor
+    m = pmesh.icosphere(2.0, subdiv)
+    part = octree.partition(m, 0.5, origin=(0, 0, 0), min_group=30 if subdiv <= 4 else 40)
+    r0 = Predictor.load().sample_counts(part, 2 * np.pi, 1e-4)
+    with Engine() as eng:
+        eng.upload_mesh(m, 2 * np.pi, 376.73, q=7)
+        eng.set_blocks(part)
+        eng.set_symmetric(True)
+        eng.compress(1e-4, **dict(PRODUCT, r0=r0))
+        g = torch.Generator(device="cuda").manual_seed(0)
+        X = torch.randn((m.N, 16), dtype=torch.complex64, device="cuda", generator=g)
+        for i in range(calls):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            eng.matvec(X)
+            e1.record()
+            torch.cuda.synchronize()
+            print(f"matvec call {i}: {e0.elapsed_time(e1):.4f} ms", flush=True)
 
 
 def recompress_case(calls, subdiv=4):
@@ -1018,7 +1049,7 @@ def main():
     ap.add_argument("--product-only", action="store_true",
                     help="time the product steps only (no baselines, ablations, checks): the "
                          "command the kernel launch list is captured from")
-    ap.add_argument("--profile-case", choices=("fill", "store", "extras", "recompress"), default=None,
+    ap.add_argument("--profile-case", choices=("fill", "store", "extras", "recompress", "matvec"), default=None,
                     help="run one small profiling workload on the 7,680-RWG sphere instead of the "
                          "benchmark (the cases the kernel profiles are captured from)")
     ap.add_argument("--precision", default="c64", help="profiling case fill: c64 or c128")
@@ -1028,13 +1059,15 @@ def main():
     ap.add_argument("--tri-cols", type=int, default=8,
                     help="profiling case fill: columns per triangle-moment tile (0: balanced per job)")
     ap.add_argument("--subdiv", type=int, default=4,
-                    help="profiling cases recompress and store: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
+                    help="profiling cases recompress, store and matvec: sphere subdivisions (4: 7,680 RWG, 5: 30,720)")
     args = ap.parse_args()
     if args.profile_case:
         if args.profile_case == "fill":
             fill_case(args.precision, args.calls, args.split, args.geom32, args.tri_cols)
         elif args.profile_case == "store":
             store_case(args.calls, args.subdiv)
+        elif args.profile_case == "matvec":
+            matvec_case(args.calls, args.subdiv)
         elif args.profile_case == "recompress":
             recompress_case(args.calls, args.subdiv)
         else:
