@@ -529,8 +529,11 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10, fp64_recompress=True):
     mv_launches = (L.pskel_kernel_launches() - l0) // reps
     mv_ms = float(np.mean(times))
     mm, nn, rr = (st[k].astype(np.float64) for k in ("m", "n", "r"))
-    factor_bytes = roofline.matvec_bytes(mm, nn, rr, 0, 8.0, 16.0)
-    vec_bytes = roofline.matvec_bytes(mm, nn, 0 * rr, nrhs, 0.0)
+    mirror = eng.mirror_of()
+    own = np.array([p < 0 or b < p for b, p in enumerate(mirror)]) if eng_symmetric(eng) else \
+        np.ones(len(mirror), dtype=bool)
+    factor_bytes = roofline.matvec_bytes(mm[own], nn[own], rr[own], 0, 8.0, 16.0)
+    vec_bytes = 2.0 * nrhs * m.N * 8.0
     flops = roofline.matvec_flops(mm, nn, rr, nrhs)
     peak = _hbm_peak()
     gbs = (factor_bytes + vec_bytes) / (mv_ms * 1e-3) / 1e9
@@ -538,8 +541,9 @@ def run_blockops(eng, st, m, flush, nrhs=16, reps=10, fp64_recompress=True):
                       factor_bytes=factor_bytes, vector_bytes=vec_bytes,
                       achieved_gbs=round(gbs, 1), peak_gbs=peak, frac=round(gbs / peak, 4),
                       gflops=round(flops / (mv_ms * 1e-3) / 1e9, 1),
-                      bytes="C and R in complex64 + U in complex128 + gathered X and scattered Y, "
-                            "once each per call (algorithmic)")
+                      bytes="C and R in complex64 + U in complex128 of the blocks that keep factors "
+                            "(a mirrored block reads its partner's), X read and Y written once "
+                            "(algorithmic)")
     # recompression to the compression tolerance (device time of its launches, from the
     # library's own events on its stream): the default path (split tensor-core path for these
     # complex-FP32 factors) and, where its workspace fits, the FP64 path on the same blocks
