@@ -419,12 +419,13 @@ def run_ours(args, rank, world, dev):
         st = eng.compress(TOL, r0=r0, use_graph=True, **PRODUCT)
     octree_t = run_octree(args, m, part, dev) if rank == 0 else None
     aca_t = run_aca(m, part, dev) if (rank == 0 and not args.product_only and not large) else None
-    # e2e: the public call path from host buffers: mesh + groups + features up, stats down (its
+    # e2e: the public call path from host buffers: mesh up, octree partition and far list built on
+    # the device and copied out, features on the host, block lists + features up, stats down (its
     # own engine; this one's device memory is released first, which the 122,880-RWG workload
     # needs)
     mirror = eng.mirror_of()
     eng.close()
-    e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush,
+    e2e_ms, h2d, d2h = run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, rank, world, flush,
                                    fill_choice=tune["choice"], pipeline=pipe["choice"])
     if args.save and rank == 0:
         np.savez(args.save, m=st["m"], n=st["n"], r=st["r"], rounds=st["rounds"], est=st["est"],
@@ -490,7 +491,10 @@ def run_ours(args, rank, world, dev):
                       fill_ms=round(tph["fill"], 3), fill_launches=int(tph["fill_launches"])),
         phases_nograph_ms={k: round(tph[k], 3) for k in ("sample", "fill", "pinv", "estimate", "total")},
         e2e=dict(value=round(e2e_ms, 3), unit="ms", h2d_bytes_per_step=int(h2d),
-                 d2h_bytes_per_step=int(d2h)),
+                 d2h_bytes_per_step=int(d2h),
+                 scope="mesh upload, device octree partition and far list (copied out), host "
+                       "features, block lists and features up, rank prediction, compression, "
+                       "per-block stats down"),
         clocks=clocks, gpu_launches=int(launches),
         blockops=blockops,
         footprint=footprint,
@@ -788,8 +792,11 @@ def run_aca(m, part, dev, reps=3):
                      "one CTA per block, symmetric mode; wall time of the call")
 
 
-def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=None, pipeline=None):
-    """Host data in, compressed blocks resident on the GPU, per-block stats out."""
+def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, rank, world, flush, fill_choice=None, pipeline=None):
+    """Host data in, compressed blocks resident on the GPU, per-block stats out. Every step
+    uploads the mesh, builds the octree partition and far list on the device (copied out to the
+    host), takes this rank's blocks, computes the predictor features on the host, uploads the
+    block lists and features, predicts the first sample counts and compresses."""
     import torch
 
     from pskel import _lib, autotune
@@ -799,7 +806,6 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
     class Sub:
         pass
     sp = Sub()
-    sp.gt, sp.gs, sp.sizes, sp.extents, sp.centres = sub_gt, sub_gs, part.sizes, part.extents, part.centres
     a = m.as_f64()
     eng = Engine(dev)
     if fill_choice is not None:  # the fill variant the autotuner picked for this GPU and workload
@@ -808,19 +814,24 @@ def run_e2e(args, m, part, sub_gt, sub_gs, pred, dev, world, flush, fill_choice=
         eng.set_pipeline(pipeline)
     eng.set_symmetric(True)
     L = _lib.lib()
-    feats_host = features(sp, K_WAVE, TOL)
-    x_pin = torch.from_numpy(((feats_host - pred.mean) / pred.std).astype(np.float32)).pin_memory()
+    w = WORKLOADS[args.workload]
+    x_pin = torch.empty((len(sub_gt), 8), dtype=torch.float32).pin_memory()
     p_dev = torch.from_numpy(pred.params).cuda()
-    Dmin = np.minimum(part.sizes()[sub_gt], part.sizes()[sub_gs])
     vp = lambda t: ctypes.c_void_p(t.data_ptr())
     h2d = sum(a[k].nbytes for k in ("vertex", "topol", "edges", "ln", "cent"))
     h2d += part.group_ptr.nbytes + part.group_ids.nbytes + sub_gt.nbytes + sub_gs.nbytes
     h2d += x_pin.numel() * 4 + p_dev.numel() * 4
     d2h = len(sub_gt) * 40 + len(sub_gt) * 4
+    d2h += sum(getattr(part, k).nbytes for k in ("group_ptr", "group_ids", "gt", "gs", "centres", "extents"))
 
     def one():
         eng.upload_mesh(m, K_WAVE, ETA, q=7)
-        eng.set_blocks(group_ptr=part.group_ptr, group_ids=part.group_ids, gt=sub_gt, gs=sub_gs)
+        p = eng.octree(w["leaf"], origin=(0, 0, 0), min_group=w["min_group"])
+        mine = shard_blocks(p.gt, p.gs, rank, world) if world > 1 else slice(None)
+        sp.gt, sp.gs, sp.sizes, sp.extents, sp.centres = p.gt[mine], p.gs[mine], p.sizes, p.extents, p.centres
+        x_pin.copy_(torch.from_numpy(((features(sp, K_WAVE, TOL) - pred.mean) / pred.std).astype(np.float32)))
+        eng.set_blocks(group_ptr=p.group_ptr, group_ids=p.group_ids, gt=sp.gt, gs=sp.gs)
+        Dmin = np.minimum(p.sizes()[sp.gt], p.sizes()[sp.gs])
         x = x_pin.cuda(non_blocking=True)
         y = torch.empty(len(sub_gt), dtype=torch.float32, device="cuda")
         _lib.check(L.pskel_mlp_forward(vp(p_dev), vp(x), len(sub_gt), vp(y), None))
