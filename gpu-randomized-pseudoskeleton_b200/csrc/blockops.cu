@@ -170,37 +170,45 @@ __global__ void __launch_bounds__(256) matvec_group_kernel(const MatvecBlock *__
                 }
             }
         } else {
-            // several right-hand sides: X(cols, :) staged once, each warp takes JB / kMvWarps of
-            // them over the whole k range (lane = row of R); no cross-warp reduction
-            constexpr int RPW = JB / kMvWarps > 0 ? JB / kMvWarps : 1;
+            // several right-hand sides: X(cols, j0 : j0 + JB) staged once (xs[k][jj]); the k range
+            // split over the warps (lane = row of R, all JB right-hand sides in registers), so that
+            // the CTA reads R once; the warps' partial sums are added into T1 by shared-memory
+            // atomics
             for (int j0 = 0; j0 < nrhs; j0 += JB) {
                 __syncthreads();  // xs is free
                 for (int e = threadIdx.x; e < w.n * JB; e += blockDim.x) {
-                    const int jj = e / w.n, k = e - jj * w.n;  // xs[jj][k]: one row of X per jj
+                    const int k = e / JB, jj = e - k * JB;
                     xs[e] = j0 + jj < nrhs ? X[w.cols[k] + (size_t)(j0 + jj) * ldx] : mk<A>(0.0, 0.0);
                 }
+                for (int e = threadIdx.x; e < w.r * JB; e += blockDim.x) {
+                    const int i = e % w.r, j = j0 + e / w.r;
+                    if (j < nrhs) t1[i + j * w.r] = mk<A>(0.0, 0.0);
+                }
                 __syncthreads();
-                for (int g = wid; g * RPW < JB; g += kMvWarps) {
-                    for (int ib = 0; ib < w.r; ib += 32) {
-                        const int i = ib + lane;
-                        if (i >= w.r) continue;
-                        A ar[RPW], ai[RPW];
+                for (int ib = 0; ib < w.r; ib += 32) {
+                    const int i = ib + lane;
+                    if (i >= w.r || k0 >= k1) continue;
+                    A ar[JB], ai[JB];
 #pragma unroll
-                        for (int q = 0; q < RPW; ++q) ar[q] = ai[q] = 0;
-                        for (int k = 0; k < w.n; ++k) {
-                            const double2 rv = r_op(w, R, Cm, i, k);
-                            const A rx = (A)rv.x, ry = (A)rv.y;
+                    for (int q = 0; q < JB; ++q) ar[q] = ai[q] = 0;
+                    for (int k = k0; k < k1; ++k) {
+                        const double2 rv = r_op(w, R, Cm, i, k);
+                        const A rx = (A)rv.x, ry = (A)rv.y;
+                        const C2 *xk = xs + k * JB;
 #pragma unroll
-                            for (int q = 0; q < RPW; ++q) {
-                                const C2 x = xs[(g * RPW + q) * w.n + k];
-                                ar[q] += rx * x.x - ry * x.y;
-                                ai[q] += rx * x.y + ry * x.x;
-                            }
+                        for (int q = 0; q < JB; ++q) {
+                            const C2 x = xk[q];
+                            ar[q] += rx * x.x - ry * x.y;
+                            ai[q] += rx * x.y + ry * x.x;
                         }
+                    }
 #pragma unroll
-                        for (int q = 0; q < RPW; ++q) {
-                            const int j = j0 + g * RPW + q;
-                            if (j < nrhs) t1[i + j * w.r] = mk<A>(ar[q], ai[q]);
+                    for (int q = 0; q < JB; ++q) {
+                        const int j = j0 + q;
+                        if (j < nrhs) {
+                            A *t = reinterpret_cast<A *>(t1 + i + j * w.r);
+                            atomicAdd(t, ar[q]);
+                            atomicAdd(t + 1, ai[q]);
                         }
                     }
                 }
